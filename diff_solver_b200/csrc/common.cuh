@@ -1,0 +1,342 @@
+// Shared device helpers of the smoke kernels: MAC-grid indexing, boundary
+// handling, trilinear sampling and the RK2 backtrace.
+//
+// The semantics follow the reference helpers in solvers/smoke/operators.cu
+// (cited per function); boundary modes and packing are the reference's
+// (data.ixx:14-25, operators.cpp:85-105).  Everything here is header-only
+// and __forceinline__ so each kernel specialises it.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "diff_smoke.h"
+
+namespace xs {
+
+constexpr int kBlock = 256;
+
+// Launch accounting (read through xs_launch_count).
+void count_launch();
+
+struct Grid {
+    int nx, ny, nz;
+    float h, dt;
+};
+
+__host__ __device__ __forceinline__ Grid make_grid(const XsGrid& g) {
+    return Grid{static_cast<int>(g.nx), static_cast<int>(g.ny), static_cast<int>(g.nz), g.cell_size, g.time_step};
+}
+
+struct Vec3 {
+    float x, y, z;
+};
+
+struct Sample {
+    float value;
+    Vec3 gradient;
+};
+
+struct Trace {
+    Vec3 position;
+    Vec3 derivative;
+};
+
+__host__ __device__ __forceinline__ uint64_t cell_count(const Grid& g) {
+    return static_cast<uint64_t>(g.nx) * g.ny * g.nz;
+}
+
+// operators.cu:36-39
+__host__ __device__ __forceinline__ int extent(const Grid& g, int axis, int dim) {
+    const int base = dim == 0 ? g.nx : (dim == 1 ? g.ny : g.nz);
+    return base + (axis == dim ? 1 : 0);
+}
+
+// operators.cu:41-43
+__host__ __device__ __forceinline__ uint64_t face_count(const Grid& g, int axis) {
+    return static_cast<uint64_t>(extent(g, axis, 0)) * extent(g, axis, 1) * extent(g, axis, 2);
+}
+
+// operators.cu:45-47
+__host__ __device__ __forceinline__ uint64_t idx3(int x, int y, int z, int nx, int ny) {
+    return static_cast<uint64_t>(x) + static_cast<uint64_t>(nx) * (static_cast<uint64_t>(y) + static_cast<uint64_t>(ny) * z);
+}
+
+// operators.cu:49-54
+__device__ __forceinline__ void decode(uint64_t i, int nx, int ny, int& x, int& y, int& z) {
+    const uint64_t yz = i / static_cast<uint64_t>(nx);
+    x = static_cast<int>(i - yz * nx);
+    const uint64_t zz = yz / static_cast<uint64_t>(ny);
+    y = static_cast<int>(yz - zz * ny);
+    z = static_cast<int>(zz);
+}
+
+__device__ __forceinline__ bool in_grid(const Grid& g, int x, int y, int z) {
+    return x >= 0 && x < g.nx && y >= 0 && y < g.ny && z >= 0 && z < g.nz;
+}
+
+template <class T>
+__host__ __device__ __forceinline__ T* component(T* x, T* y, T* z, int axis) {
+    return axis == 0 ? x : (axis == 1 ? y : z);
+}
+
+// operators.cu:80-86
+__device__ __forceinline__ bool periodic(const XsVelocityBoundary& b, int d) {
+    return b.modes[2 * d] == 3u && b.modes[2 * d + 1] == 3u;
+}
+__device__ __forceinline__ bool periodic(const XsScalarBoundary& b, int d) {
+    return b.modes[2 * d] == 2u && b.modes[2 * d + 1] == 2u;
+}
+
+// operators.cu:88-96
+__device__ __forceinline__ int wrap(int v, int p) {
+    const int r = v % p;
+    return r < 0 ? r + p : r;
+}
+__device__ __forceinline__ int map_coordinate(int v, int size, bool per, int period) {
+    return per ? wrap(v, period) : max(0, min(size - 1, v));
+}
+
+__device__ __forceinline__ bool is_solid(const uint32_t* mask, uint64_t i) {
+    return mask != nullptr && __ldg(mask + i) != 0u;
+}
+
+// operators.cu:98-103
+__device__ __forceinline__ uint64_t mapped_cell(int x, int y, int z, const Grid& g, bool px, bool py, bool pz) {
+    return idx3(map_coordinate(x, g.nx, px, g.nx), map_coordinate(y, g.ny, py, g.ny), map_coordinate(z, g.nz, pz, g.nz), g.nx, g.ny);
+}
+
+// operators.cu:105-113
+__device__ __forceinline__ uint64_t mapped_face(int x, int y, int z, const Grid& g, int axis, const XsVelocityBoundary& b) {
+    const int ex = extent(g, axis, 0), ey = extent(g, axis, 1), ez = extent(g, axis, 2);
+    return idx3(map_coordinate(x, ex, periodic(b, 0), g.nx), map_coordinate(y, ey, periodic(b, 1), g.ny),
+                map_coordinate(z, ez, periodic(b, 2), g.nz), ex, ey);
+}
+
+// operators.cu:115-123: value of a cell-centred field, boundary aware.
+__device__ __forceinline__ float load_scalar(const float* __restrict__ v, int x, int y, int z, const Grid& g, const XsScalarBoundary& b) {
+    if (x < 0 && b.modes[0] == 0u) return b.values[0];
+    if (x >= g.nx && b.modes[1] == 0u) return b.values[1];
+    if (y < 0 && b.modes[2] == 0u) return b.values[2];
+    if (y >= g.ny && b.modes[3] == 0u) return b.values[3];
+    if (z < 0 && b.modes[4] == 0u) return b.values[4];
+    if (z >= g.nz && b.modes[5] == 0u) return b.values[5];
+    return __ldg(v + mapped_cell(x, y, z, g, periodic(b, 0), periodic(b, 1), periodic(b, 2)));
+}
+
+// operators.cu:125-134: value of one face component, boundary aware.  A face
+// outside the grid along a fixed-value face (or the normal component at a
+// normal-fixed face) reads the boundary value of the first such dimension.
+__device__ __forceinline__ bool face_constant(int axis, int x, int y, int z, const Grid& g, const XsVelocityBoundary& b, float& value) {
+    const int c[3] = {x, y, z};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+        const int size = extent(g, axis, d);
+        if (c[d] >= 0 && c[d] < size) continue;
+        const int face = 2 * d + (c[d] >= size);
+        if (b.modes[face] == 0u || (b.modes[face] == 2u && axis == d)) {
+            value = b.values[3 * face + axis];
+            return true;
+        }
+    }
+    return false;
+}
+
+__device__ __forceinline__ float load_face(const float* __restrict__ v, int axis, int x, int y, int z, const Grid& g,
+                                           const XsVelocityBoundary& b) {
+    float value;
+    if (face_constant(axis, x, y, z, g, b, value)) return value;
+    return __ldg(v + mapped_face(x, y, z, g, axis, b));
+}
+
+// Trilinear value and gradient of an 8-value cell (operators.cu:150-163).
+__device__ __forceinline__ Sample trilinear(const float v[2][2][2], float tx, float ty, float tz, float h) {
+    const float wx[2] = {1.0f - tx, tx}, wy[2] = {1.0f - ty, ty}, wz[2] = {1.0f - tz, tz};
+    Sample s{0.0f, {0.0f, 0.0f, 0.0f}};
+#pragma unroll
+    for (int dz = 0; dz < 2; ++dz) {
+#pragma unroll
+        for (int dy = 0; dy < 2; ++dy) {
+#pragma unroll
+            for (int dx = 0; dx < 2; ++dx) s.value += wx[dx] * wy[dy] * wz[dz] * v[dz][dy][dx];
+            s.gradient.x += wy[dy] * wz[dz] * (v[dz][dy][1] - v[dz][dy][0]) / h;
+        }
+#pragma unroll
+        for (int dx = 0; dx < 2; ++dx) s.gradient.y += wx[dx] * wz[dz] * (v[dz][1][dx] - v[dz][0][dx]) / h;
+    }
+#pragma unroll
+    for (int dy = 0; dy < 2; ++dy)
+#pragma unroll
+        for (int dx = 0; dx < 2; ++dx) s.gradient.z += wx[dx] * wy[dy] * (v[1][dy][dx] - v[0][dy][dx]) / h;
+    return s;
+}
+
+__device__ __forceinline__ float trilinear_value(const float v[2][2][2], float tx, float ty, float tz) {
+    const float x00 = v[0][0][0] + tx * (v[0][0][1] - v[0][0][0]);
+    const float x01 = v[0][1][0] + tx * (v[0][1][1] - v[0][1][0]);
+    const float x10 = v[1][0][0] + tx * (v[1][0][1] - v[1][0][0]);
+    const float x11 = v[1][1][0] + tx * (v[1][1][1] - v[1][1][0]);
+    const float y0 = x00 + ty * (x01 - x00);
+    const float y1 = x10 + ty * (x11 - x10);
+    return y0 + tz * (y1 - y0);
+}
+
+// Grid coordinates of a sample point for a cell-centred field (offset 0.5
+// on every axis) or face component `axis` (offset 0 along axis).
+__device__ __forceinline__ void grid_coordinates(const Vec3& p, float h, int axis, float& gx, float& gy, float& gz) {
+    gx = p.x / h - (axis == 0 ? 0.0f : 0.5f);
+    gy = p.y / h - (axis == 1 ? 0.0f : 0.5f);
+    gz = p.z / h - (axis == 2 ? 0.0f : 0.5f);
+}
+
+// operators.cu:136-164
+template <bool kGradient>
+__device__ __forceinline__ Sample sample_scalar(const float* __restrict__ v, const Vec3& p, const Grid& g, const XsScalarBoundary& b) {
+    float gx, gy, gz;
+    grid_coordinates(p, g.h, -1, gx, gy, gz);
+    const int x0 = static_cast<int>(floorf(gx)), y0 = static_cast<int>(floorf(gy)), z0 = static_cast<int>(floorf(gz));
+    float v8[2][2][2];
+#pragma unroll
+    for (int dz = 0; dz < 2; ++dz)
+#pragma unroll
+        for (int dy = 0; dy < 2; ++dy)
+#pragma unroll
+            for (int dx = 0; dx < 2; ++dx) v8[dz][dy][dx] = load_scalar(v, x0 + dx, y0 + dy, z0 + dz, g, b);
+    if (kGradient) return trilinear(v8, gx - x0, gy - y0, gz - z0, g.h);
+    return Sample{trilinear(v8, gx - x0, gy - y0, gz - z0, g.h).value, {0.0f, 0.0f, 0.0f}};
+}
+
+// operators.cu:166-194
+template <bool kGradient>
+__device__ __forceinline__ Sample sample_face(const float* __restrict__ v, int axis, const Vec3& p, const Grid& g,
+                                              const XsVelocityBoundary& b) {
+    float gx, gy, gz;
+    grid_coordinates(p, g.h, axis, gx, gy, gz);
+    const int x0 = static_cast<int>(floorf(gx)), y0 = static_cast<int>(floorf(gy)), z0 = static_cast<int>(floorf(gz));
+    float v8[2][2][2];
+#pragma unroll
+    for (int dz = 0; dz < 2; ++dz)
+#pragma unroll
+        for (int dy = 0; dy < 2; ++dy)
+#pragma unroll
+            for (int dx = 0; dx < 2; ++dx) v8[dz][dy][dx] = load_face(v, axis, x0 + dx, y0 + dy, z0 + dz, g, b);
+    if (kGradient) return trilinear(v8, gx - x0, gy - y0, gz - z0, g.h);
+    return Sample{trilinear(v8, gx - x0, gy - y0, gz - z0, g.h).value, {0.0f, 0.0f, 0.0f}};
+}
+
+// operators.cu:242-244
+__device__ __forceinline__ Vec3 sample_velocity(const float* __restrict__ ux, const float* __restrict__ uy, const float* __restrict__ uz,
+                                                const Vec3& p, const Grid& g, const XsVelocityBoundary& b) {
+    return Vec3{sample_face<false>(ux, 0, p, g, b).value, sample_face<false>(uy, 1, p, g, b).value,
+                sample_face<false>(uz, 2, p, g, b).value};
+}
+
+// operators.cu:246-254
+__device__ __forceinline__ bool solid_at(Vec3 p, const uint32_t* mask, const Grid& g, const XsVelocityBoundary& b) {
+    if (mask == nullptr) return false;
+    if (periodic(b, 0)) p.x -= floorf(p.x / (g.nx * g.h)) * g.nx * g.h;
+    if (periodic(b, 1)) p.y -= floorf(p.y / (g.ny * g.h)) * g.ny * g.h;
+    if (periodic(b, 2)) p.z -= floorf(p.z / (g.nz * g.h)) * g.nz * g.h;
+    const int x = max(0, min(g.nx - 1, static_cast<int>(floorf(p.x / g.h))));
+    const int y = max(0, min(g.ny - 1, static_cast<int>(floorf(p.y / g.h))));
+    const int z = max(0, min(g.nz - 1, static_cast<int>(floorf(p.z / g.h))));
+    return __ldg(mask + idx3(x, y, z, g.nx, g.ny)) != 0u;
+}
+
+// operators.cu:256-276: RK2 midpoint backtrace.  Non-periodic axes clamp to
+// the domain and zero that axis' derivative; a trace ending in a solid cell
+// is bisected 8 times along the segment from the start.
+__device__ __forceinline__ Trace trace_rk2(const Vec3& s, const float* __restrict__ ux, const float* __restrict__ uy,
+                                           const float* __restrict__ uz, const uint32_t* mask, const Grid& g,
+                                           const XsVelocityBoundary& b) {
+    const Vec3 v0 = sample_velocity(ux, uy, uz, s, g, b);
+    const Vec3 mid{s.x - 0.5f * g.dt * v0.x, s.y - 0.5f * g.dt * v0.y, s.z - 0.5f * g.dt * v0.z};
+    const Vec3 v1 = sample_velocity(ux, uy, uz, mid, g, b);
+    Vec3 raw{s.x - g.dt * v1.x, s.y - g.dt * v1.y, s.z - g.dt * v1.z};
+    Vec3 der{1.0f, 1.0f, 1.0f};
+    const Vec3 mx{g.nx * g.h, g.ny * g.h, g.nz * g.h};
+    if (!periodic(b, 0) && (raw.x < 0.0f || raw.x > mx.x)) { raw.x = fminf(fmaxf(raw.x, 0.0f), mx.x); der.x = 0.0f; }
+    if (!periodic(b, 1) && (raw.y < 0.0f || raw.y > mx.y)) { raw.y = fminf(fmaxf(raw.y, 0.0f), mx.y); der.y = 0.0f; }
+    if (!periodic(b, 2) && (raw.z < 0.0f || raw.z > mx.z)) { raw.z = fminf(fmaxf(raw.z, 0.0f), mx.z); der.z = 0.0f; }
+    if (!solid_at(raw, mask, g, b)) return Trace{raw, der};
+    float lo = 0.0f, hi = 1.0f;
+    for (int it = 0; it < 8; ++it) {
+        const float f = 0.5f * (lo + hi);
+        const Vec3 t{s.x + f * (raw.x - s.x), s.y + f * (raw.y - s.y), s.z + f * (raw.z - s.z)};
+        if (solid_at(t, mask, g, b)) hi = f; else lo = f;
+    }
+    return Trace{Vec3{s.x + lo * (raw.x - s.x), s.y + lo * (raw.y - s.y), s.z + lo * (raw.z - s.z)},
+                 Vec3{lo * der.x, lo * der.y, lo * der.z}};
+}
+
+// operators.cu:278-284
+__device__ __forceinline__ Vec3 face_position(int axis, int x, int y, int z, const Grid& g) {
+    return Vec3{(x + (axis == 0 ? 0.0f : 0.5f)) * g.h, (y + (axis == 1 ? 0.0f : 0.5f)) * g.h, (z + (axis == 2 ? 0.0f : 0.5f)) * g.h};
+}
+__device__ __forceinline__ Vec3 cell_position(int x, int y, int z, const Grid& g) {
+    return Vec3{(x + 0.5f) * g.h, (y + 0.5f) * g.h, (z + 0.5f) * g.h};
+}
+
+// Inflow spheres travel as a kernel parameter.
+struct InflowSet {
+    uint32_t count;
+    XsInflow items[XS_MAX_INFLOWS];
+};
+
+// Index of the last inflow containing cell (x,y,z), or -1.
+__device__ __forceinline__ int inflow_hit(const InflowSet& f, int x, int y, int z, const Grid& g) {
+    if (f.count == 0) return -1;
+    const Vec3 p = cell_position(x, y, z, g);
+    int hit = -1;
+    for (uint32_t k = 0; k < f.count; ++k) {
+        const float dx = p.x - f.items[k].center[0], dy = p.y - f.items[k].center[1], dz = p.z - f.items[k].center[2];
+        const float r = f.items[k].radius;
+        if (dx * dx + dy * dy + dz * dz <= r * r) hit = static_cast<int>(k);
+    }
+    return hit;
+}
+
+// Zeroed copies of boundary values, for tangents (operators.cu:396-397, 516-519).
+__device__ __forceinline__ XsVelocityBoundary zero_values(XsVelocityBoundary b) {
+#pragma unroll
+    for (int i = 0; i < 18; ++i) b.values[i] = 0.0f;
+    return b;
+}
+__device__ __forceinline__ XsScalarBoundary zero_values(XsScalarBoundary b) {
+#pragma unroll
+    for (int i = 0; i < 6; ++i) b.values[i] = 0.0f;
+    return b;
+}
+
+// ---------------------------------------------------------------- reductions
+__device__ __forceinline__ double warp_sum(double v) {
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
+
+// Block-wide sum of K (<= 4) doubles; the result is valid in every thread.
+template <int K>
+__device__ __forceinline__ void block_sum(double* v, double* smem /* [4][32] */) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = (blockDim.x + 31) >> 5;
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] = warp_sum(v[k]);
+    __syncthreads();
+    if (lane == 0) {
+#pragma unroll
+        for (int k = 0; k < K; ++k) smem[k * 32 + warp] = v[k];
+    }
+    __syncthreads();
+#pragma unroll
+    for (int k = 0; k < K; ++k) {
+        const double t = lane < nw ? smem[k * 32 + lane] : 0.0;
+        v[k] = warp_sum(t);
+    }
+    __syncthreads();
+}
+
+inline unsigned blocks_for(uint64_t n, int block = kBlock) {
+    return static_cast<unsigned>((n + block - 1) / block);
+}
+
+}  // namespace xs

@@ -1,0 +1,451 @@
+// Forward smoke operators on sm_100a: sources and inflow, buoyancy, force
+// integration, MAC advection with boundary constraints, scalar advection,
+// divergence and projection.  Operator-level C ABI (operators.h:40-72).
+#include <atomic>
+
+#include "common.cuh"
+#include "launch.cuh"
+#include "ops.cuh"
+
+namespace xs {
+
+// ------------------------------------------------------------ sources
+// operators.cu:286-290, plus inflow spheres that set the value.
+__global__ void source_forward_kernel(Grid g, const uint32_t* __restrict__ mask, const float* __restrict__ state,
+                                      const float* __restrict__ source, InflowSet inflows, uint32_t which, float* __restrict__ out) {
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= cell_count(g)) return;
+    if (is_solid(mask, i)) { out[i] = 0.0f; return; }
+    if (inflows.count) {
+        int x, y, z;
+        decode(i, g.nx, g.ny, x, y, z);
+        const int k = inflow_hit(inflows, x, y, z, g);
+        if (k >= 0) { out[i] = which == 0 ? inflows.items[k].density : inflows.items[k].temperature; return; }
+    }
+    out[i] = state[i] + g.dt * source[i];
+}
+
+// Sources of density and temperature and the buoyancy force in one pass
+// (operators.cu:286-290 twice, then :304-313 on the sourced fields, as
+// model.cpp:342-344 composes them).
+__global__ void source_buoyancy_kernel(Grid g, const uint32_t* __restrict__ mask, const float* __restrict__ rho,
+                                       const float* __restrict__ temp, const float* __restrict__ rho_src,
+                                       const float* __restrict__ temp_src, const float* __restrict__ ax,
+                                       const float* __restrict__ ay, const float* __restrict__ az,
+                                       const float* __restrict__ ambient, const float* __restrict__ beta_rho,
+                                       const float* __restrict__ beta_temp, InflowSet inflows, float* __restrict__ rho_out,
+                                       float* __restrict__ temp_out, float* __restrict__ fx, float* __restrict__ fy,
+                                       float* __restrict__ fz) {
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= cell_count(g)) return;
+    if (is_solid(mask, i)) {
+        rho_out[i] = 0.0f; temp_out[i] = 0.0f; fx[i] = 0.0f; fy[i] = 0.0f; fz[i] = 0.0f;
+        return;
+    }
+    float r, t;
+    int k = -1;
+    if (inflows.count) {
+        int x, y, z;
+        decode(i, g.nx, g.ny, x, y, z);
+        k = inflow_hit(inflows, x, y, z, g);
+    }
+    if (k >= 0) {
+        r = inflows.items[k].density;
+        t = inflows.items[k].temperature;
+    } else {
+        r = rho[i] + g.dt * rho_src[i];
+        t = temp[i] + g.dt * temp_src[i];
+    }
+    rho_out[i] = r;
+    temp_out[i] = t;
+    fx[i] = ax[i];
+    fy[i] = ay[i] + __ldg(beta_rho) * r + __ldg(beta_temp) * (t - __ldg(ambient));
+    fz[i] = az[i];
+}
+
+// ------------------------------------------------------------ buoyancy
+// operators.cu:304-313
+__global__ void buoyancy_forward_kernel(Grid g, const uint32_t* __restrict__ mask, const float* __restrict__ rho,
+                                        const float* __restrict__ temp, const float* __restrict__ ax, const float* __restrict__ ay,
+                                        const float* __restrict__ az, const float* __restrict__ ambient,
+                                        const float* __restrict__ beta_rho, const float* __restrict__ beta_temp,
+                                        float* __restrict__ fx, float* __restrict__ fy, float* __restrict__ fz) {
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= cell_count(g)) return;
+    if (is_solid(mask, i)) { fx[i] = 0.0f; fy[i] = 0.0f; fz[i] = 0.0f; return; }
+    fx[i] = ax[i];
+    fy[i] = ay[i] + __ldg(beta_rho) * rho[i] + __ldg(beta_temp) * (temp[i] - __ldg(ambient));
+    fz[i] = az[i];
+}
+
+// ------------------------------------------------------------ integrate
+// Face index space of all three components, concatenated.
+struct FaceSpace {
+    uint64_t f0, f1, f2;
+    __host__ __device__ uint64_t total() const { return f0 + f1 + f2; }
+    __device__ __forceinline__ int locate(uint64_t i, uint64_t& local) const {
+        if (i < f0) { local = i; return 0; }
+        if (i < f0 + f1) { local = i - f0; return 1; }
+        local = i - f0 - f1;
+        return 2;
+    }
+};
+
+inline FaceSpace face_space(const Grid& g) { return FaceSpace{face_count(g, 0), face_count(g, 1), face_count(g, 2)}; }
+
+// operators.cu:339-356: mean force of the fluid cells either side of a face.
+__device__ __forceinline__ float averaged_center_force(const float* __restrict__ f, int axis, int x, int y, int z, const Grid& g,
+                                                       const uint32_t* __restrict__ mask) {
+    const int fx = x - (axis == 0), fy = y - (axis == 1), fz = z - (axis == 2);
+    float sum = 0.0f, count = 0.0f;
+    if (in_grid(g, fx, fy, fz)) {
+        const uint64_t c = idx3(fx, fy, fz, g.nx, g.ny);
+        if (!is_solid(mask, c)) { sum += __ldg(f + c); count += 1.0f; }
+    }
+    if (in_grid(g, x, y, z)) {
+        const uint64_t c = idx3(x, y, z, g.nx, g.ny);
+        if (!is_solid(mask, c)) { sum += __ldg(f + c); count += 1.0f; }
+    }
+    return count == 0.0f ? 0.0f : sum / count;
+}
+
+// operators.cu:358-364 for all three components in one launch.
+__global__ void integrate_kernel(Grid g, FaceSpace fs, const uint32_t* __restrict__ mask, XsVector u, XsVector f, XsVector out) {
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= fs.total()) return;
+    uint64_t local;
+    const int a = fs.locate(i, local);
+    int x, y, z;
+    decode(local, extent(g, a, 0), extent(g, a, 1), x, y, z);
+    const float* ua = component(u.x, u.y, u.z, a);
+    const float* fa = component(f.x, f.y, f.z, a);
+    float* oa = component(out.x, out.y, out.z, a);
+    oa[local] = ua[local] + g.dt * averaged_center_force(fa, a, x, y, z, g, mask);
+}
+
+// ------------------------------------------------------------ advection
+// operators.cu:441-449
+__device__ __forceinline__ bool adjacent_solid(int a, int x, int y, int z, const Grid& g, const uint32_t* __restrict__ mask) {
+    if (mask == nullptr) return false;
+    const int fx = x - (a == 0), fy = y - (a == 1), fz = z - (a == 2);
+    if (in_grid(g, fx, fy, fz) && __ldg(mask + idx3(fx, fy, fz, g.nx, g.ny)) != 0u) return true;
+    if (in_grid(g, x, y, z) && __ldg(mask + idx3(x, y, z, g.nx, g.ny)) != 0u) return true;
+    return false;
+}
+
+// operators.cu:451-464
+__device__ __forceinline__ bool constrained_boundary(int a, int x, int y, int z, const Grid& g, const XsVelocityBoundary& b,
+                                                     float& value) {
+    const int coord = a == 0 ? x : (a == 1 ? y : z);
+    const int mx = a == 0 ? g.nx : (a == 1 ? g.ny : g.nz);
+    if (coord != 0 && coord != mx) return false;
+    const int face = a * 2 + (coord == mx);
+    const uint32_t mode = b.modes[face];
+    if (mode != 0u && mode != 2u) return false;
+    value = b.values[face * 3 + a];
+    return true;
+}
+
+// operators.cu:381-388: one face, RK2 trace through u, sample own component.
+__device__ __forceinline__ float advect_face(int a, int x, int y, int z, const Grid& g, const uint32_t* __restrict__ mask,
+                                             const XsVector& u, const XsVelocityBoundary& b) {
+    const Trace t = trace_rk2(face_position(a, x, y, z, g), u.x, u.y, u.z, mask, g, b);
+    return sample_face<false>(component<const float>(u.x, u.y, u.z, a), a, t.position, g, b).value;
+}
+
+__global__ void advect_velocity_kernel(Grid g, FaceSpace fs, const uint32_t* __restrict__ mask, XsVector u, XsVelocityBoundary b,
+                                       XsVector out) {
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= fs.total()) return;
+    uint64_t local;
+    const int a = fs.locate(i, local);
+    int x, y, z;
+    decode(local, extent(g, a, 0), extent(g, a, 1), x, y, z);
+    component(out.x, out.y, out.z, a)[local] = advect_face(a, x, y, z, g, mask, u, b);
+}
+
+// operators.cu:466-481 (collider components may be null: zero).
+__global__ void constrain_kernel(Grid g, FaceSpace fs, const uint32_t* __restrict__ mask, XsVector col, XsVector u,
+                                 XsVelocityBoundary b, XsVector out) {
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= fs.total()) return;
+    uint64_t local;
+    const int a = fs.locate(i, local);
+    int x, y, z;
+    decode(local, extent(g, a, 0), extent(g, a, 1), x, y, z);
+    float* oa = component(out.x, out.y, out.z, a);
+    float v;
+    if (constrained_boundary(a, x, y, z, g, b, v)) { oa[local] = v; return; }
+    if (adjacent_solid(a, x, y, z, g, mask)) {
+        const float* ca = component(col.x, col.y, col.z, a);
+        oa[local] = ca == nullptr ? 0.0f : ca[local];
+        return;
+    }
+    const float* ua = component(u.x, u.y, u.z, a);
+    if (periodic(b, a) && (a == 0 ? x == g.nx : (a == 1 ? y == g.ny : z == g.nz))) {
+        if (a == 0) x = 0;
+        if (a == 1) y = 0;
+        if (a == 2) z = 0;
+        oa[local] = ua[idx3(x, y, z, extent(g, a, 0), extent(g, a, 1))];
+        return;
+    }
+    oa[local] = ua[local];
+}
+
+// Advection and constraint fused (operators.cu:381-388 then :466-481): the
+// constrained output is written directly; a periodic face at the upper end
+// takes the advected value of its wrapped partner at coordinate 0.
+__global__ void advect_constrain_kernel(Grid g, FaceSpace fs, const uint32_t* __restrict__ mask, XsVector col, XsVector u,
+                                        XsVelocityBoundary b, XsVector out) {
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= fs.total()) return;
+    uint64_t local;
+    const int a = fs.locate(i, local);
+    int x, y, z;
+    decode(local, extent(g, a, 0), extent(g, a, 1), x, y, z);
+    float* oa = component(out.x, out.y, out.z, a);
+    float v;
+    if (constrained_boundary(a, x, y, z, g, b, v)) { oa[local] = v; return; }
+    if (adjacent_solid(a, x, y, z, g, mask)) {
+        const float* ca = component(col.x, col.y, col.z, a);
+        oa[local] = ca == nullptr ? 0.0f : ca[local];
+        return;
+    }
+    if (periodic(b, a) && (a == 0 ? x == g.nx : (a == 1 ? y == g.ny : z == g.nz))) {
+        if (a == 0) x = 0;
+        if (a == 1) y = 0;
+        if (a == 2) z = 0;
+    }
+    oa[local] = advect_face(a, x, y, z, g, mask, u, b);
+}
+
+// operators.cu:499-507
+__global__ void advect_scalar_kernel(Grid g, const uint32_t* __restrict__ mask, const float* __restrict__ collider,
+                                     const float* __restrict__ src, XsVector u, XsScalarBoundary sb, XsVelocityBoundary vb,
+                                     float* __restrict__ out) {
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= cell_count(g)) return;
+    if (is_solid(mask, i)) { out[i] = collider == nullptr ? 0.0f : collider[i]; return; }
+    int x, y, z;
+    decode(i, g.nx, g.ny, x, y, z);
+    const Trace t = trace_rk2(cell_position(x, y, z, g), u.x, u.y, u.z, mask, g, vb);
+    out[i] = sample_scalar<false>(src, t.position, g, sb).value;
+}
+
+// Density and temperature advected along one shared trace (the reference
+// traces twice, model.cpp:347-348).
+__global__ void advect_scalar_pair_kernel(Grid g, const uint32_t* __restrict__ mask, const float* __restrict__ col_rho,
+                                          const float* __restrict__ col_temp, const float* __restrict__ src_rho,
+                                          const float* __restrict__ src_temp, XsVector u, XsScalarBoundary rb,
+                                          XsScalarBoundary tb, XsVelocityBoundary vb, float* __restrict__ out_rho,
+                                          float* __restrict__ out_temp) {
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= cell_count(g)) return;
+    if (is_solid(mask, i)) {
+        out_rho[i] = col_rho == nullptr ? 0.0f : col_rho[i];
+        out_temp[i] = col_temp == nullptr ? 0.0f : col_temp[i];
+        return;
+    }
+    int x, y, z;
+    decode(i, g.nx, g.ny, x, y, z);
+    const Trace t = trace_rk2(cell_position(x, y, z, g), u.x, u.y, u.z, mask, g, vb);
+    out_rho[i] = sample_scalar<false>(src_rho, t.position, g, rb).value;
+    out_temp[i] = sample_scalar<false>(src_temp, t.position, g, tb).value;
+}
+
+// ------------------------------------------------------------ projection
+// operators.cu:904-910
+__device__ __forceinline__ bool projectable_face(const Grid& g, int a, int x, int y, int z, const uint32_t* __restrict__ mask,
+                                                 uint64_t& first, uint64_t& second) {
+    const int fx = x - (a == 0), fy = y - (a == 1), fz = z - (a == 2);
+    if (!in_grid(g, fx, fy, fz) || !in_grid(g, x, y, z)) return false;
+    first = idx3(fx, fy, fz, g.nx, g.ny);
+    second = idx3(x, y, z, g.nx, g.ny);
+    return !is_solid(mask, first) && !is_solid(mask, second);
+}
+
+// operators.cu:912-920 with an FP32 pressure.
+__global__ void project_kernel(Grid g, FaceSpace fs, const uint32_t* __restrict__ mask, XsVector u, const float* __restrict__ p,
+                               XsVector out) {
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= fs.total()) return;
+    uint64_t local;
+    const int a = fs.locate(i, local);
+    int x, y, z;
+    decode(local, extent(g, a, 0), extent(g, a, 1), x, y, z);
+    const float* ua = component(u.x, u.y, u.z, a);
+    float* oa = component(out.x, out.y, out.z, a);
+    uint64_t f, s;
+    if (!projectable_face(g, a, x, y, z, mask, f, s)) { oa[local] = ua[local]; return; }
+    oa[local] = ua[local] - g.dt * (__ldg(p + s) - __ldg(p + f)) / g.h;
+}
+
+// The same with the FP64 pressure iterate of the PCG solve: the pressure
+// difference is taken in FP64 and the velocity rounded once.
+__global__ void project64_kernel(Grid g, FaceSpace fs, const uint32_t* __restrict__ mask, XsVector u, const double* __restrict__ p,
+                                 XsVector out) {
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= fs.total()) return;
+    uint64_t local;
+    const int a = fs.locate(i, local);
+    int x, y, z;
+    decode(local, extent(g, a, 0), extent(g, a, 1), x, y, z);
+    const float* ua = component(u.x, u.y, u.z, a);
+    float* oa = component(out.x, out.y, out.z, a);
+    uint64_t f, s;
+    if (!projectable_face(g, a, x, y, z, mask, f, s)) { oa[local] = ua[local]; return; }
+    const double dp = __ldg(p + s) - __ldg(p + f);
+    oa[local] = static_cast<float>(static_cast<double>(ua[local]) - static_cast<double>(g.dt) * dp / static_cast<double>(g.h));
+}
+
+// operators.cu:875-883
+__global__ void pressure_rhs_kernel(Grid g, uint32_t anchor, const uint32_t* __restrict__ mask, XsVector u, float* __restrict__ rhs) {
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= cell_count(g)) return;
+    if (is_solid(mask, i) || i == anchor) { rhs[i] = 0.0f; return; }
+    int x, y, z;
+    decode(i, g.nx, g.ny, x, y, z);
+    const float div = (__ldg(u.x + idx3(x + 1, y, z, g.nx + 1, g.ny)) - __ldg(u.x + idx3(x, y, z, g.nx + 1, g.ny)) +
+                       __ldg(u.y + idx3(x, y + 1, z, g.nx, g.ny + 1)) - __ldg(u.y + idx3(x, y, z, g.nx, g.ny + 1)) +
+                       __ldg(u.z + idx3(x, y, z + 1, g.nx, g.ny)) - __ldg(u.z + idx3(x, y, z, g.nx, g.ny))) / g.h;
+    rhs[i] = -g.h * g.h * div / g.dt;
+}
+
+__global__ void accumulate_kernel(const double* __restrict__ src, double* __restrict__ dst, uint64_t n) {
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i < n) dst[i] += src[i];
+}
+
+// ------------------------------------------------------------ launchers
+InflowSet make_inflows(const XsInflow* inflows, uint32_t count) {
+    InflowSet s{};
+    s.count = inflows == nullptr ? 0u : count;
+    for (uint32_t k = 0; k < s.count; ++k) s.items[k] = inflows[k];
+    return s;
+}
+
+XsStatus launch_source_buoyancy(cudaStream_t st, const Grid& g, const uint32_t* mask, const float* rho, const float* temp,
+                                const float* rho_src, const float* temp_src, const XsVector& acc, const float* ambient,
+                                const float* beta_rho, const float* beta_temp, const InflowSet& inflows, float* rho_out,
+                                float* temp_out, const XsVector& force) {
+    source_buoyancy_kernel<<<blocks_for(cell_count(g)), kBlock, 0, st>>>(g, mask, rho, temp, rho_src, temp_src, acc.x, acc.y, acc.z,
+                                                                          ambient, beta_rho, beta_temp, inflows, rho_out, temp_out,
+                                                                          force.x, force.y, force.z);
+    return check_launch();
+}
+
+XsStatus launch_integrate(cudaStream_t st, const Grid& g, const uint32_t* mask, const XsVector& u, const XsVector& f, const XsVector& out) {
+    const FaceSpace fs = face_space(g);
+    integrate_kernel<<<blocks_for(fs.total()), kBlock, 0, st>>>(g, fs, mask, u, f, out);
+    return check_launch();
+}
+
+XsStatus launch_advect_constrain(cudaStream_t st, const Grid& g, const uint32_t* mask, const XsVector& col, const XsVector& u,
+                                 const XsVelocityBoundary& b, const XsVector& out) {
+    const FaceSpace fs = face_space(g);
+    advect_constrain_kernel<<<blocks_for(fs.total()), kBlock, 0, st>>>(g, fs, mask, col, u, b, out);
+    return check_launch();
+}
+
+XsStatus launch_constrain(cudaStream_t st, const Grid& g, const uint32_t* mask, const XsVector& col, const XsVector& u,
+                          const XsVelocityBoundary& b, const XsVector& out) {
+    const FaceSpace fs = face_space(g);
+    constrain_kernel<<<blocks_for(fs.total()), kBlock, 0, st>>>(g, fs, mask, col, u, b, out);
+    return check_launch();
+}
+
+XsStatus launch_advect_scalar_pair(cudaStream_t st, const Grid& g, const uint32_t* mask, const float* col_rho, const float* col_temp,
+                                   const float* src_rho, const float* src_temp, const XsVector& u, const XsScalarBoundary& rb,
+                                   const XsScalarBoundary& tb, const XsVelocityBoundary& vb, float* out_rho, float* out_temp) {
+    advect_scalar_pair_kernel<<<blocks_for(cell_count(g)), kBlock, 0, st>>>(g, mask, col_rho, col_temp, src_rho, src_temp, u, rb, tb,
+                                                                             vb, out_rho, out_temp);
+    return check_launch();
+}
+
+XsStatus launch_pressure_rhs(cudaStream_t st, const Grid& g, uint32_t anchor, const uint32_t* mask, const XsVector& u, float* rhs) {
+    pressure_rhs_kernel<<<blocks_for(cell_count(g)), kBlock, 0, st>>>(g, anchor, mask, u, rhs);
+    return check_launch();
+}
+
+XsStatus launch_project(cudaStream_t st, const Grid& g, const uint32_t* mask, const XsVector& u, const float* p, const XsVector& out) {
+    const FaceSpace fs = face_space(g);
+    project_kernel<<<blocks_for(fs.total()), kBlock, 0, st>>>(g, fs, mask, u, p, out);
+    return check_launch();
+}
+
+XsStatus launch_project64(cudaStream_t st, const Grid& g, const uint32_t* mask, const XsVector& u, const double* p, const XsVector& out) {
+    const FaceSpace fs = face_space(g);
+    project64_kernel<<<blocks_for(fs.total()), kBlock, 0, st>>>(g, fs, mask, u, p, out);
+    return check_launch();
+}
+
+}  // namespace xs
+
+using namespace xs;
+
+extern "C" {
+
+XsStatus xs_accumulate(cudaStream_t stream, const double* source, double* destination, uint64_t count) {
+    if (count == 0) return XS_OK;
+    if (!source || !destination) return XS_INVALID_ARGUMENT;
+    accumulate_kernel<<<blocks_for(count), kBlock, 0, stream>>>(source, destination, count);
+    return check_launch();
+}
+
+XsStatus xs_source_forward(cudaStream_t stream, XsGrid grid, const uint32_t* cell_mask, const float* state, const float* source,
+                           const XsInflow* inflows, uint32_t inflow_count, uint32_t which, float* output) {
+    if (!valid_grid(grid) || !state || !source || !output || inflow_count > XS_MAX_INFLOWS) return XS_INVALID_ARGUMENT;
+    const Grid g = make_grid(grid);
+    source_forward_kernel<<<blocks_for(cell_count(g)), kBlock, 0, stream>>>(g, cell_mask, state, source, make_inflows(inflows, inflow_count),
+                                                                             which, output);
+    return check_launch();
+}
+
+XsStatus xs_buoyancy_forward(cudaStream_t stream, XsGrid grid, const uint32_t* cell_mask, const float* density, const float* temperature,
+                             XsVector external_acceleration, const float* ambient_temperature, const float* density_buoyancy,
+                             const float* temperature_buoyancy, XsVector force) {
+    if (!valid_grid(grid) || !density || !temperature || !ambient_temperature || !density_buoyancy || !temperature_buoyancy ||
+        !valid(external_acceleration) || !valid(force))
+        return XS_INVALID_ARGUMENT;
+    const Grid g = make_grid(grid);
+    buoyancy_forward_kernel<<<blocks_for(cell_count(g)), kBlock, 0, stream>>>(
+        g, cell_mask, density, temperature, external_acceleration.x, external_acceleration.y, external_acceleration.z, ambient_temperature,
+        density_buoyancy, temperature_buoyancy, force.x, force.y, force.z);
+    return check_launch();
+}
+
+XsStatus xs_integrate_velocity_forward(cudaStream_t stream, XsGrid grid, const uint32_t* cell_mask, XsVector velocity, XsVector force,
+                                       XsVector output) {
+    if (!valid_grid(grid) || !valid(velocity) || !valid(force) || !valid(output)) return XS_INVALID_ARGUMENT;
+    return launch_integrate(stream, make_grid(grid), cell_mask, velocity, force, output);
+}
+
+XsStatus xs_advect_velocity_forward(cudaStream_t stream, XsGrid grid, const uint32_t* cell_mask, XsVector velocity,
+                                    XsVelocityBoundary boundary, XsVector output) {
+    if (!valid_grid(grid) || !valid(velocity) || !valid(output)) return XS_INVALID_ARGUMENT;
+    const Grid g = make_grid(grid);
+    const FaceSpace fs = face_space(g);
+    advect_velocity_kernel<<<blocks_for(fs.total()), kBlock, 0, stream>>>(g, fs, cell_mask, velocity, boundary, output);
+    return check_launch();
+}
+
+XsStatus xs_constrain_velocity_forward(cudaStream_t stream, XsGrid grid, const uint32_t* cell_mask, XsVector collider_velocity,
+                                       XsVector velocity, XsVelocityBoundary boundary, XsVector output) {
+    if (!valid_grid(grid) || !valid(velocity) || !valid(output)) return XS_INVALID_ARGUMENT;
+    const Grid g = make_grid(grid);
+    const FaceSpace fs = face_space(g);
+    constrain_kernel<<<blocks_for(fs.total()), kBlock, 0, stream>>>(g, fs, cell_mask, collider_velocity, velocity, boundary, output);
+    return check_launch();
+}
+
+XsStatus xs_advect_scalar_forward(cudaStream_t stream, XsGrid grid, const uint32_t* cell_mask, const float* collider_value,
+                                  const float* source, XsVector velocity, XsScalarBoundary scalar_boundary,
+                                  XsVelocityBoundary velocity_boundary, float* output) {
+    if (!valid_grid(grid) || !source || !valid(velocity) || !output) return XS_INVALID_ARGUMENT;
+    const Grid g = make_grid(grid);
+    advect_scalar_kernel<<<blocks_for(cell_count(g)), kBlock, 0, stream>>>(g, cell_mask, collider_value, source, velocity, scalar_boundary,
+                                                                            velocity_boundary, output);
+    return check_launch();
+}
+
+}  // extern "C"

@@ -1,0 +1,704 @@
+// Pressure Poisson solve on sm_100a.
+//
+// The system is the one the reference's red-black Gauss-Seidel iteration
+// converges to (solvers/smoke/operators.cu:852-902): for every fluid cell i
+// that is not the pressure anchor and has a non-zero diagonal,
+//
+//     diag_i p_i - sum_{connected j} p_j = rhs_i + sum_{fixed faces} value
+//
+// where diag_i counts connected fluid neighbours plus fixed-value boundary
+// faces, Neumann faces drop out and periodic faces wrap.  Every other cell
+// holds p = 0.  The matrix is symmetric positive definite on the active
+// cells whenever every fluid region touches a fixed face or the anchor.
+//
+// Solvers (one cooperative persistent launch each, bounded grid barriers):
+//   * Jacobi-PCG.  CG vectors are FP32 (z = r/diag, p ping-pong, q, e), all
+//     reductions are FP64 and deterministic (block partials summed in fixed
+//     order by the last block to arrive).  The solution is accumulated in an
+//     FP64 iterate x64: each CG pass solves for an FP32 correction e, which
+//     is folded into x64, after which the true residual b - A x64 is
+//     recomputed in FP64 and, if still above tolerance, a further pass runs
+//     on it.  FP32 storage of the pressure alone cannot reach a 1e-6
+//     relative residual on large grids; this refinement can.
+//   * Red-black Gauss-Seidel with a fixed sweep count, the reference's own
+//     method (operators.cu:1004-1013), in FP32, for drop-in behaviour.
+//   * The reverse of those sweeps (operators.cu:935-955, 1025-1028) in
+//     gather form, for the reference-compatible VJP.
+#include <cmath>
+#include <cstring>
+#include <mutex>
+
+#include "common.cuh"
+#include "launch.cuh"
+#include "pressure.cuh"
+
+namespace xs {
+
+// ------------------------------------------------------------------ layout
+size_t align_up(size_t v, size_t a) { return (v + a - 1) / a * a; }
+
+PressureWorkspace carve_pressure_workspace(void* base, const Grid& g) {
+    const size_t n = cell_count(g);
+    PressureWorkspace w{};
+    char* p = static_cast<char*>(base);
+    size_t off = 0;
+    auto take = [&](size_t bytes) {
+        void* r = p ? p + off : nullptr;
+        off = align_up(off + bytes, 256);
+        return r;
+    };
+    w.state = static_cast<SolverState*>(take(sizeof(SolverState)));
+    w.partials = static_cast<double*>(take(sizeof(double) * kPartialSlots * kMaxPersistentBlocks));
+    w.x64 = static_cast<double*>(take(sizeof(double) * n));
+    w.z = static_cast<float*>(take(sizeof(float) * n));
+    w.p0 = static_cast<float*>(take(sizeof(float) * n));
+    w.p1 = static_cast<float*>(take(sizeof(float) * n));
+    w.q = static_cast<float*>(take(sizeof(float) * n));
+    w.e = static_cast<float*>(take(sizeof(float) * n));
+    w.bytes = off;
+    return w;
+}
+
+size_t pressure_workspace_bytes(const Grid& g) { return carve_pressure_workspace(nullptr, g).bytes; }
+
+// ------------------------------------------------------------ the operator
+struct Operator {
+    Grid g;
+    const uint32_t* mask;
+    uint32_t anchor;
+    XsScalarBoundary pb;
+    bool use_fixed_values;
+};
+
+// Neighbour structure of cell (x,y,z) (operators.cu:852-873).  Returns
+// whether the cell is an unknown of the system; nb[] holds the six
+// neighbour indices (valid where bit d of conn is set).
+struct CellStencil {
+    uint64_t nb[6];
+    unsigned conn;
+    float diag;
+    float fixed_sum;
+};
+
+__device__ __forceinline__ bool stencil(const Operator& op, int x, int y, int z, uint64_t i, CellStencil& s) {
+    const Grid& g = op.g;
+    s.conn = 0u;
+    s.diag = 0.0f;
+    s.fixed_sum = 0.0f;
+    if (is_solid(op.mask, i)) return false;
+    const uint64_t sx = 1, sy = static_cast<uint64_t>(g.nx), sz = static_cast<uint64_t>(g.nx) * g.ny;
+    const int coord[3] = {x, y, z};
+    const int size[3] = {g.nx, g.ny, g.nz};
+    const uint64_t stride[3] = {sx, sy, sz};
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+#pragma unroll
+        for (int side = 0; side < 2; ++side) {
+            const int dir = side ? 1 : -1;
+            const int c = coord[d] + dir;
+            const int face = 2 * d + side;
+            uint64_t j;
+            if (c < 0 || c >= size[d]) {
+                if (periodic(op.pb, d)) {
+                    j = side ? i - stride[d] * (size[d] - 1) : i + stride[d] * (size[d] - 1);
+                } else {
+                    if (op.pb.modes[face] == 0u) {
+                        s.diag += 1.0f;
+                        if (op.use_fixed_values) s.fixed_sum += op.pb.values[face];
+                    }
+                    continue;
+                }
+            } else {
+                j = side ? i + stride[d] : i - stride[d];
+            }
+            if (!is_solid(op.mask, j)) {
+                s.nb[face] = j;
+                s.conn |= 1u << face;
+                s.diag += 1.0f;
+            }
+        }
+    }
+    return i != op.anchor && s.diag > 0.0f;
+}
+
+// ------------------------------------------------------------- grid sync
+// Arrive at the grid barrier with K block-summed values; the last block to
+// arrive sums every block's partials in block order (deterministic), stores
+// the totals and releases the others.  Waits are bounded: a wait that runs
+// past kBarrierTimeoutCycles marks state->error and returns.  Returns false
+// if any block has flagged an error.
+constexpr long long kBarrierTimeoutCycles = 8000000000ll;  // ~4 s at 2 GHz
+
+template <int K>
+__device__ bool grid_reduce(SolverState* st, double* partials, double* v, double* red) {
+    __shared__ unsigned s_last, s_gen;
+    if (K > 0) {
+        block_sum<K>(v, red);
+        if (threadIdx.x == 0) {
+#pragma unroll
+            for (int k = 0; k < K; ++k) partials[static_cast<size_t>(blockIdx.x) * kPartialSlots + k] = v[k];
+        }
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        const unsigned gen = *reinterpret_cast<volatile unsigned*>(&st->gen);
+        __threadfence();
+        const unsigned prev = atomicAdd(&st->count, 1u);
+        s_last = prev == gridDim.x - 1 ? 1u : 0u;
+        s_gen = gen;
+    }
+    __syncthreads();
+    if (s_last) {
+        __threadfence();
+        if (K > 0) {
+            double acc[K > 0 ? K : 1];
+#pragma unroll
+            for (int k = 0; k < K; ++k) acc[k] = 0.0;
+            for (unsigned b = threadIdx.x; b < gridDim.x; b += blockDim.x) {
+#pragma unroll
+                for (int k = 0; k < K; ++k) acc[k] += __ldcg(partials + static_cast<size_t>(b) * kPartialSlots + k);
+            }
+            block_sum<K>(acc, red);
+            if (threadIdx.x == 0) {
+#pragma unroll
+                for (int k = 0; k < K; ++k) st->sum[k] = acc[k];
+            }
+        }
+        __syncthreads();
+        if (threadIdx.x == 0) {
+            st->count = 0u;
+            __threadfence();
+            atomicExch(&st->gen, s_gen + 1u);
+        }
+    } else if (threadIdx.x == 0) {
+        const long long t0 = clock64();
+        while (*reinterpret_cast<volatile unsigned*>(&st->gen) == s_gen) {
+            __nanosleep(64);
+            if (clock64() - t0 > kBarrierTimeoutCycles) {
+                atomicExch(&st->error, 1u);
+                break;
+            }
+        }
+        __threadfence();
+    }
+    __syncthreads();
+    __threadfence();
+#pragma unroll
+    for (int k = 0; k < K; ++k) v[k] = __ldcg(&st->sum[k]);
+    return __ldcg(&st->error) == 0u;
+}
+
+__device__ __forceinline__ bool grid_barrier(SolverState* st, double* partials, double* red) {
+    return grid_reduce<0>(st, partials, nullptr, red);
+}
+
+// --------------------------------------------------------------- PCG phases
+struct PcgArgs {
+    Operator op;
+    const float* rhs_f;   // forward right-hand side (FP32), or
+    const double* rhs_d;  // adjoint right-hand side (FP64)
+    const float* guess;   // warm start or null
+    double* x64;
+    float* z;
+    float* p[2];
+    float* q;
+    float* e;
+    float* pressure_out;  // FP32 copy of the solution (null: none)
+    double* solution_out; // FP64 copy of the solution (null: none)
+    double* partials;
+    SolverState* st;
+    double tol;
+    uint32_t max_iterations;
+};
+
+enum ResidualMode { kFromZero = 0, kFromGuess = 1, kFromX64 = 2 };
+
+__device__ __forceinline__ double rhs_at(const PcgArgs& a, uint64_t i) {
+    return a.rhs_d ? a.rhs_d[i] : static_cast<double>(a.rhs_f[i]);
+}
+
+// r = b - A x in FP64; z = r/diag, p0 = z, e = 0; partial sums
+// v = {||b||^2, ||r||^2, r.z}.
+__device__ void residual_phase(const PcgArgs& a, int mode, double (&v)[3]) {
+    const Grid& g = a.op.g;
+    const uint64_t n = cell_count(g);
+    v[0] = v[1] = v[2] = 0.0;
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        int x, y, z;
+        decode(i, g.nx, g.ny, x, y, z);
+        CellStencil s;
+        const bool act = stencil(a.op, x, y, z, i, s);
+        if (!act) {
+            a.z[i] = 0.0f; a.p[0][i] = 0.0f; a.e[i] = 0.0f;
+            if (mode != kFromX64) a.x64[i] = 0.0;
+            if (a.pressure_out) a.pressure_out[i] = 0.0f;
+            if (a.solution_out) a.solution_out[i] = 0.0;
+            continue;
+        }
+        const double b = rhs_at(a, i) + static_cast<double>(s.fixed_sum);
+        double xi = 0.0, ax = 0.0;
+        if (mode == kFromGuess) {
+            xi = a.guess[i];
+            ax = s.diag * xi;
+#pragma unroll
+            for (int f = 0; f < 6; ++f)
+                if ((s.conn >> f) & 1u) { const uint64_t j = s.nb[f]; if (j != a.op.anchor) ax -= static_cast<double>(a.guess[j]); }
+            a.x64[i] = xi;
+        } else if (mode == kFromX64) {
+            xi = a.x64[i];
+            ax = s.diag * xi;
+#pragma unroll
+            for (int f = 0; f < 6; ++f)
+                if ((s.conn >> f) & 1u) ax -= a.x64[s.nb[f]];
+        } else {
+            a.x64[i] = 0.0;
+        }
+        const double r = b - ax;
+        const float zf = static_cast<float>(r / s.diag);
+        a.z[i] = zf;
+        a.p[0][i] = zf;
+        a.e[i] = 0.0f;
+        if (a.pressure_out) a.pressure_out[i] = static_cast<float>(xi);
+        if (a.solution_out) a.solution_out[i] = xi;
+        v[0] += b * b;
+        v[1] += r * r;
+        v[2] += r * static_cast<double>(zf);
+    }
+}
+
+// Iteration k: p_k = z + beta p_{k-1} (k > 0), q = A p_k, e += alpha_{k-1} p_{k-1};
+// partial p_k.q.
+__device__ void spmv_phase(const PcgArgs& a, int k, float beta, float alpha_prev, double& pq) {
+    const Grid& g = a.op.g;
+    const uint64_t n = cell_count(g);
+    const float* pold = a.p[(k + 1) & 1];
+    float* pnew = a.p[k & 1];
+    pq = 0.0;
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        int x, y, z;
+        decode(i, g.nx, g.ny, x, y, z);
+        CellStencil s;
+        const bool act = stencil(a.op, x, y, z, i, s);
+        if (!act) {
+            if (k > 0) pnew[i] = 0.0f;
+            a.q[i] = 0.0f;
+            continue;
+        }
+        float pc, acc;
+        if (k == 0) {
+            pc = pnew[i];
+            acc = 0.0f;
+#pragma unroll
+            for (int f = 0; f < 6; ++f)
+                if ((s.conn >> f) & 1u) acc += pnew[s.nb[f]];
+        } else {
+            const float po = pold[i];
+            pc = a.z[i] + beta * po;
+            acc = 0.0f;
+#pragma unroll
+            for (int f = 0; f < 6; ++f)
+                if ((s.conn >> f) & 1u) { const uint64_t j = s.nb[f]; acc += a.z[j] + beta * pold[j]; }
+            pnew[i] = pc;
+            a.e[i] += alpha_prev * po;
+        }
+        const float qv = s.diag * pc - acc;
+        a.q[i] = qv;
+        pq += static_cast<double>(pc) * static_cast<double>(qv);
+    }
+}
+
+// z -= alpha q / diag; partial {r.z, r.r} with r = z diag.
+__device__ void update_phase(const PcgArgs& a, float alpha, double (&v)[2]) {
+    const Grid& g = a.op.g;
+    const uint64_t n = cell_count(g);
+    v[0] = v[1] = 0.0;
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        int x, y, z;
+        decode(i, g.nx, g.ny, x, y, z);
+        CellStencil s;
+        if (!stencil(a.op, x, y, z, i, s)) continue;
+        const float zn = a.z[i] - alpha * a.q[i] / s.diag;
+        a.z[i] = zn;
+        const double r = static_cast<double>(zn) * s.diag;
+        v[0] += r * static_cast<double>(zn);
+        v[1] += r * r;
+    }
+}
+
+// x64 += e + alpha p_k
+__device__ void fold_phase(const PcgArgs& a, int k, float alpha) {
+    const Grid& g = a.op.g;
+    const uint64_t n = cell_count(g);
+    const float* pk = a.p[k & 1];
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        a.x64[i] += static_cast<double>(a.e[i]) + static_cast<double>(alpha) * static_cast<double>(pk[i]);
+    }
+}
+
+constexpr uint32_t kMaxRefinements = 4;
+
+__global__ void __launch_bounds__(kBlock) pcg_kernel(PcgArgs a) {
+    __shared__ double red[4 * 32];
+    SolverState* st = a.st;
+    double v3[3];
+    residual_phase(a, a.guess ? kFromGuess : kFromZero, v3);
+    if (!grid_reduce<3>(st, a.partials, v3, red)) return;
+    const double bb = v3[0];
+    double rr = v3[1], rz = v3[2];
+    uint32_t warm = a.guess ? 1u : 0u;
+    if (a.guess && rr > bb) {  // the guess is worse than zero: fall back
+        warm = 0u;
+        residual_phase(a, kFromZero, v3);
+        if (!grid_reduce<3>(st, a.partials, v3, red)) return;
+        rr = v3[1];
+        rz = v3[2];
+    }
+    const double initial = bb > 0.0 ? sqrt(rr / bb) : 0.0;
+    const double target2 = a.tol * a.tol * bb;
+    uint32_t iterations = 0, refinements = 0;
+    uint32_t status = XS_OK;
+    while (true) {
+        if (!(rr <= target2)) {
+            if (!isfinite(rr)) { status = XS_NUMERICAL_ERROR; break; }
+            if (iterations >= a.max_iterations || refinements > kMaxRefinements) { status = XS_NOT_CONVERGED; break; }
+        } else {
+            status = XS_OK;
+            break;
+        }
+        // one CG pass on the current residual (z, p0 set, e = 0)
+        int k = 0;
+        float beta = 0.0f, alpha = 0.0f;
+        bool broke = false;
+        while (true) {
+            double pq[1];
+            spmv_phase(a, k, beta, alpha, pq[0]);
+            if (!grid_reduce<1>(st, a.partials, pq, red)) return;
+            if (!(pq[0] > 0.0) || !isfinite(pq[0])) { broke = true; break; }
+            alpha = static_cast<float>(rz / pq[0]);
+            double v2[2];
+            update_phase(a, alpha, v2);
+            if (!grid_reduce<2>(st, a.partials, v2, red)) return;
+            ++iterations;
+            beta = static_cast<float>(v2[0] / rz);
+            rz = v2[0];
+            if (!isfinite(v2[1])) { broke = true; break; }
+            if (v2[1] <= target2 || iterations >= a.max_iterations) break;
+            ++k;
+        }
+        if (broke) {
+            status = XS_NUMERICAL_ERROR;
+            break;
+        }
+        fold_phase(a, k, alpha);
+        if (!grid_barrier(st, a.partials, red)) return;
+        residual_phase(a, kFromX64, v3);
+        if (!grid_reduce<3>(st, a.partials, v3, red)) return;
+        rr = v3[1];
+        rz = v3[2];
+        ++refinements;
+    }
+    if (status != XS_OK && rr <= target2) status = XS_OK;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        st->stats.iterations = iterations;
+        st->stats.status = status;
+        st->stats.refinements = refinements;
+        st->stats.warm_start_used = warm;
+        st->stats.rhs_norm = sqrt(bb);
+        st->stats.initial_residual = initial;
+        st->stats.final_residual = bb > 0.0 ? sqrt(rr / bb) : 0.0;
+    }
+}
+
+// -------------------------------------------------- red-black Gauss-Seidel
+// operators.cu:885-902 applied to the cells of one parity.
+__device__ void rbgs_phase(const Operator& op, int parity, const float* rhs, float* p) {
+    const Grid& g = op.g;
+    const uint64_t n = cell_count(g);
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        int x, y, z;
+        decode(i, g.nx, g.ny, x, y, z);
+        if (((x + y + z) & 1) != parity || is_solid(op.mask, i) || i == op.anchor) continue;
+        // neighbour order of the reference: -x, +x, -y, +y, -z, +z
+        float sum = rhs[i], diag = 0.0f;
+        CellStencil s;
+        stencil(op, x, y, z, i, s);
+        const int coord[3] = {x, y, z};
+        const int size[3] = {g.nx, g.ny, g.nz};
+#pragma unroll
+        for (int f = 0; f < 6; ++f) {
+            if ((s.conn >> f) & 1u) {
+                sum += p[s.nb[f]];
+                diag += 1.0f;
+            } else {
+                const int d = f >> 1, dir = (f & 1) ? 1 : -1;
+                const int c = coord[d] + dir;
+                if ((c < 0 || c >= size[d]) && !periodic(op.pb, d) && op.pb.modes[f] == 0u) {
+                    sum += op.pb.values[f];
+                    diag += 1.0f;
+                }
+            }
+        }
+        p[i] = diag == 0.0f ? 0.0f : sum / diag;
+    }
+}
+
+struct RbgsArgs {
+    Operator op;
+    const float* rhs;
+    float* p;
+    uint32_t sweeps;
+    double* partials;
+    SolverState* st;
+};
+
+__global__ void __launch_bounds__(kBlock) rbgs_kernel(RbgsArgs a) {
+    __shared__ double red[4 * 32];
+    for (uint32_t it = 0; it < a.sweeps; ++it) {
+        rbgs_phase(a.op, 0, a.rhs, a.p);
+        if (!grid_barrier(a.st, a.partials, red)) return;
+        rbgs_phase(a.op, 1, a.rhs, a.p);
+        if (!grid_barrier(a.st, a.partials, red)) return;
+    }
+    // report the relative residual reached, in FP64
+    const Grid& g = a.op.g;
+    const uint64_t n = cell_count(g);
+    double v[2] = {0.0, 0.0};
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        int x, y, z;
+        decode(i, g.nx, g.ny, x, y, z);
+        CellStencil s;
+        Operator op = a.op;
+        op.use_fixed_values = true;
+        if (!stencil(op, x, y, z, i, s)) continue;
+        const double b = static_cast<double>(a.rhs[i]) + s.fixed_sum;
+        double ax = s.diag * static_cast<double>(a.p[i]);
+#pragma unroll
+        for (int f = 0; f < 6; ++f)
+            if ((s.conn >> f) & 1u) { const uint64_t j = s.nb[f]; if (j != a.op.anchor) ax -= a.p[j]; }
+        v[0] += b * b;
+        v[1] += (b - ax) * (b - ax);
+    }
+    if (!grid_reduce<2>(a.st, a.partials, v, red)) return;
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.st->stats.iterations = a.sweeps;
+        a.st->stats.status = XS_OK;
+        a.st->stats.refinements = 0;
+        a.st->stats.warm_start_used = 0;
+        a.st->stats.rhs_norm = sqrt(v[0]);
+        a.st->stats.initial_residual = 1.0;
+        a.st->stats.final_residual = v[0] > 0.0 ? sqrt(v[1] / v[0]) : 0.0;
+    }
+}
+
+// Reverse sweeps (operators.cu:935-955) in gather form: the cells of one
+// parity hand lambda_p / diag to the right-hand-side adjoint and to their
+// connected neighbours; a second phase gathers those contributions.
+struct RbgsReverseArgs {
+    Operator op;
+    double* pressure_adjoint;
+    double* rhs_adjoint;
+    double* handoff;
+    uint32_t sweeps;
+    double* partials;
+    SolverState* st;
+};
+
+__device__ void reverse_emit_phase(const RbgsReverseArgs& a, int parity) {
+    const Grid& g = a.op.g;
+    const uint64_t n = cell_count(g);
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        int x, y, z;
+        decode(i, g.nx, g.ny, x, y, z);
+        double out = 0.0;
+        if (((x + y + z) & 1) == parity && !is_solid(a.op.mask, i) && i != a.op.anchor) {
+            CellStencil s;
+            stencil(a.op, x, y, z, i, s);
+            const double adj = s.diag == 0.0f ? 0.0 : a.pressure_adjoint[i] / static_cast<double>(s.diag);
+            a.pressure_adjoint[i] = 0.0;
+            a.rhs_adjoint[i] += adj;
+            out = adj;
+        }
+        a.handoff[i] = out;
+    }
+}
+
+__device__ void reverse_gather_phase(const RbgsReverseArgs& a, int parity) {
+    const Grid& g = a.op.g;
+    const uint64_t n = cell_count(g);
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        int x, y, z;
+        decode(i, g.nx, g.ny, x, y, z);
+        if (is_solid(a.op.mask, i)) continue;
+        CellStencil s;
+        stencil(a.op, x, y, z, i, s);
+        double acc = 0.0;
+#pragma unroll
+        for (int f = 0; f < 6; ++f)
+            if ((s.conn >> f) & 1u) {
+                const uint64_t j = s.nb[f];
+                int jx, jy, jz;
+                decode(j, g.nx, g.ny, jx, jy, jz);
+                if (((jx + jy + jz) & 1) == parity) acc += a.handoff[j];
+            }
+        if (acc != 0.0) a.pressure_adjoint[i] += acc;
+    }
+}
+
+__global__ void __launch_bounds__(kBlock) rbgs_reverse_kernel(RbgsReverseArgs a) {
+    __shared__ double red[4 * 32];
+    for (uint32_t it = 0; it < a.sweeps; ++it) {
+        for (int parity = 1; parity >= 0; --parity) {
+            reverse_emit_phase(a, parity);
+            if (!grid_barrier(a.st, a.partials, red)) return;
+            reverse_gather_phase(a, parity);
+            if (!grid_barrier(a.st, a.partials, red)) return;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        a.st->stats.iterations = a.sweeps;
+        a.st->stats.status = XS_OK;
+    }
+}
+
+// ------------------------------------------------------------ launching
+namespace {
+
+struct DeviceLimits {
+    int sms = 0;
+    int pcg_blocks_per_sm = 0;
+    int rbgs_blocks_per_sm = 0;
+    int rev_blocks_per_sm = 0;
+};
+
+XsStatus device_limits(DeviceLimits& out) {
+    static std::mutex mu;
+    static int cached_device = -1;
+    static DeviceLimits cached;
+    int dev;
+    if (cudaGetDevice(&dev) != cudaSuccess) return XS_CUDA_ERROR;
+    std::lock_guard<std::mutex> lock(mu);
+    if (dev != cached_device) {
+        DeviceLimits l;
+        if (cudaDeviceGetAttribute(&l.sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return XS_CUDA_ERROR;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&l.pcg_blocks_per_sm, pcg_kernel, kBlock, 0) != cudaSuccess) return XS_CUDA_ERROR;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&l.rbgs_blocks_per_sm, rbgs_kernel, kBlock, 0) != cudaSuccess) return XS_CUDA_ERROR;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&l.rev_blocks_per_sm, rbgs_reverse_kernel, kBlock, 0) != cudaSuccess)
+            return XS_CUDA_ERROR;
+        cached = l;
+        cached_device = dev;
+    }
+    out = cached;
+    return XS_OK;
+}
+
+unsigned persistent_blocks(int per_sm, int sms, uint64_t n) {
+    uint64_t want = (n + kBlock - 1) / kBlock;
+    uint64_t cap = static_cast<uint64_t>(per_sm) * sms;
+    if (cap > kMaxPersistentBlocks) cap = kMaxPersistentBlocks;
+    if (want > cap) want = cap;
+    if (want < 1) want = 1;
+    return static_cast<unsigned>(want);
+}
+
+template <class Args>
+XsStatus launch_cooperative(void (*kernel)(Args), unsigned blocks, Args& args, cudaStream_t stream) {
+    void* params[] = {&args};
+    const cudaError_t e = cudaLaunchCooperativeKernel(reinterpret_cast<void*>(kernel), dim3(blocks), dim3(kBlock), params, 0, stream);
+    if (e != cudaSuccess) return check_cuda(e);
+    return check_launch();
+}
+
+}  // namespace
+
+XsStatus solve_pressure(cudaStream_t stream, const Grid& g, const XsPressureSolve& solve, uint32_t anchor, const uint32_t* mask,
+                        const XsScalarBoundary& pb, const float* rhs_f, const double* rhs_d, float* pressure_out,
+                        double* solution_out, void* workspace, PressureWorkspace* carved) {
+    if (!workspace) return XS_INVALID_ARGUMENT;
+    const PressureWorkspace w = carve_pressure_workspace(workspace, g);
+    if (carved) *carved = w;
+    DeviceLimits lim;
+    XsStatus s = device_limits(lim);
+    if (s != XS_OK) return s;
+    if (cudaMemsetAsync(w.state, 0, sizeof(SolverState), stream) != cudaSuccess) return XS_CUDA_ERROR;
+    Operator op{g, mask, anchor, pb, rhs_d == nullptr};
+    if (solve.kind == XS_SOLVER_RED_BLACK_GAUSS_SEIDEL) {
+        if (!rhs_f || !pressure_out) return XS_INVALID_ARGUMENT;
+        if (cudaMemsetAsync(pressure_out, 0, sizeof(float) * cell_count(g), stream) != cudaSuccess) return XS_CUDA_ERROR;
+        RbgsArgs a{op, rhs_f, pressure_out, solve.max_iterations, w.partials, w.state};
+        return launch_cooperative(rbgs_kernel, persistent_blocks(lim.rbgs_blocks_per_sm, lim.sms, cell_count(g)), a, stream);
+    }
+    if (solve.kind != XS_SOLVER_JACOBI_PCG || !(solve.tolerance >= 0.0)) return XS_INVALID_ARGUMENT;
+    PcgArgs a{};
+    a.op = op;
+    a.rhs_f = rhs_f;
+    a.rhs_d = rhs_d;
+    a.guess = solve.initial_guess;
+    a.x64 = w.x64;
+    a.z = w.z;
+    a.p[0] = w.p0;
+    a.p[1] = w.p1;
+    a.q = w.q;
+    a.e = w.e;
+    a.pressure_out = pressure_out;
+    a.solution_out = solution_out;
+    a.partials = w.partials;
+    a.st = w.state;
+    a.tol = solve.tolerance;
+    a.max_iterations = solve.max_iterations;
+    return launch_cooperative(pcg_kernel, persistent_blocks(lim.pcg_blocks_per_sm, lim.sms, cell_count(g)), a, stream);
+}
+
+XsStatus reverse_rbgs(cudaStream_t stream, const Grid& g, uint32_t sweeps, uint32_t anchor, const uint32_t* mask,
+                      const XsScalarBoundary& pb, double* pressure_adjoint, double* rhs_adjoint, void* workspace) {
+    const PressureWorkspace w = carve_pressure_workspace(workspace, g);
+    DeviceLimits lim;
+    XsStatus s = device_limits(lim);
+    if (s != XS_OK) return s;
+    if (cudaMemsetAsync(w.state, 0, sizeof(SolverState), stream) != cudaSuccess) return XS_CUDA_ERROR;
+    RbgsReverseArgs a{Operator{g, mask, anchor, pb, false}, pressure_adjoint, rhs_adjoint, w.x64, sweeps, w.partials, w.state};
+    return launch_cooperative(rbgs_reverse_kernel, persistent_blocks(lim.rev_blocks_per_sm, lim.sms, cell_count(g)), a, stream);
+}
+
+XsStatus read_solve_stats(cudaStream_t stream, const void* workspace, const Grid& g, XsSolveStats* out) {
+    const PressureWorkspace w = carve_pressure_workspace(const_cast<void*>(workspace), g);
+    SolverState host;
+    if (cudaMemcpyAsync(&host, w.state, sizeof(SolverState), cudaMemcpyDeviceToHost, stream) != cudaSuccess) return XS_CUDA_ERROR;
+    if (cudaStreamSynchronize(stream) != cudaSuccess) return XS_CUDA_ERROR;
+    *out = host.stats;
+    if (host.error) out->status = XS_TIMEOUT;
+    return XS_OK;
+}
+
+}  // namespace xs
+
+using namespace xs;
+
+extern "C" {
+
+size_t xs_projection_workspace_bytes(XsGrid grid) {
+    if (!valid_grid(grid)) return 0;
+    return pressure_workspace_bytes(make_grid(grid));
+}
+
+XsStatus xs_pressure_solve(cudaStream_t stream, XsGrid grid, const XsPressureSolve* solve, uint32_t pressure_anchor,
+                           const uint32_t* cell_mask, XsScalarBoundary pressure_boundary, const float* rhs, float* pressure,
+                           void* workspace) {
+    if (!valid_grid(grid) || !solve || !rhs || !pressure || !workspace) return XS_INVALID_ARGUMENT;
+    return solve_pressure(stream, make_grid(grid), *solve, pressure_anchor, cell_mask, pressure_boundary, rhs, nullptr, pressure,
+                          nullptr, workspace, nullptr);
+}
+
+size_t xs_solve_stats_offset(void) { return offsetof(SolverState, stats); }
+
+XsStatus xs_read_solve_stats(cudaStream_t stream, const void* workspace, XsSolveStats* host_stats) {
+    if (!workspace || !host_stats) return XS_INVALID_ARGUMENT;
+    const SolverState* st = static_cast<const SolverState*>(workspace);
+    SolverState host;
+    if (cudaMemcpyAsync(&host, st, sizeof(SolverState), cudaMemcpyDeviceToHost, stream) != cudaSuccess) return XS_CUDA_ERROR;
+    if (cudaStreamSynchronize(stream) != cudaSuccess) return XS_CUDA_ERROR;
+    *host_stats = host.stats;
+    if (host.error) host_stats->status = XS_TIMEOUT;
+    return XS_OK;
+}
+
+}  // extern "C"

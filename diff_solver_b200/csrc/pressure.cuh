@@ -1,0 +1,50 @@
+// Pressure solver interface shared between translation units.
+#pragma once
+
+#include "common.cuh"
+
+namespace xs {
+
+constexpr int kPartialSlots = 4;
+constexpr int kMaxPersistentBlocks = 4096;
+
+// Device-side solver control block (first bytes of a pressure workspace).
+struct SolverState {
+    unsigned int count;   // grid-barrier arrivals
+    unsigned int gen;     // grid-barrier generation
+    unsigned int error;   // set when a bounded wait gave up
+    unsigned int pad;
+    double sum[kPartialSlots];  // totals of the last grid reduction
+    XsSolveStats stats;
+};
+
+struct PressureWorkspace {
+    SolverState* state;
+    double* partials;
+    double* x64;  // FP64 solution iterate (also the reverse-sweep hand-off)
+    float* z;     // preconditioned residual r / diag
+    float* p0;
+    float* p1;
+    float* q;
+    float* e;     // FP32 correction of the current CG pass
+    size_t bytes;
+};
+
+PressureWorkspace carve_pressure_workspace(void* base, const Grid& g);
+size_t pressure_workspace_bytes(const Grid& g);
+
+// Solves the pressure system for rhs_f (forward, FP32, fixed boundary values
+// enter b) or rhs_d (adjoint, FP64, no fixed values).  pressure_out receives
+// an FP32 copy, solution_out an FP64 copy (either may be null); the FP64
+// iterate stays in the workspace (carved->x64).
+XsStatus solve_pressure(cudaStream_t stream, const Grid& g, const XsPressureSolve& solve, uint32_t anchor, const uint32_t* mask,
+                        const XsScalarBoundary& pb, const float* rhs_f, const double* rhs_d, float* pressure_out,
+                        double* solution_out, void* workspace, PressureWorkspace* carved);
+
+// The reference's reversed red-black sweeps (operators.cu:1025-1028).
+XsStatus reverse_rbgs(cudaStream_t stream, const Grid& g, uint32_t sweeps, uint32_t anchor, const uint32_t* mask,
+                      const XsScalarBoundary& pb, double* pressure_adjoint, double* rhs_adjoint, void* workspace);
+
+XsStatus read_solve_stats(cudaStream_t stream, const void* workspace, const Grid& g, XsSolveStats* out);
+
+}  // namespace xs

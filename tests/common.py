@@ -1,0 +1,154 @@
+"""Shared helpers of the test suite: scenario configurations, seeded inputs,
+conversions between product tensors and oracle arrays, error metrics."""
+from __future__ import annotations
+
+import copy
+import os
+import sys
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+from diff_solver_b200.data import (Box, Collider, Configuration, Ellipsoid, Inflow, PressureSolver, ScalarBoundaryMode,  # noqa: E402
+                                   Vector3, VelocityBoundaryMode, plume_configuration)
+
+PARAMS = dict(ambient_temperature=0.0, density_buoyancy=-0.1, temperature_buoyancy=0.5, vorticity_confinement=2.0)
+
+
+def scenario(name: str, res=(16, 14, 12)) -> Configuration:
+    """Small test problems covering every boundary mode the reference has."""
+    nx, ny, nz = res
+    h = 1.0 / nx
+    if name == "plume":
+        cfg = plume_configuration(res, cell_size=h, inflow_center=(0.5, 0.15, 0.4), inflow_radius=0.2)
+    elif name == "vorticity":
+        cfg = plume_configuration(res, cell_size=h, inflow_center=(0.5, 0.15, 0.4), inflow_radius=0.2, vorticity=True)
+    elif name == "colliders":
+        cfg = plume_configuration(res, cell_size=h, vorticity=True, inflow_center=(0.3, 0.15, 0.3), inflow_radius=0.15)
+        cfg.colliders = [
+            Collider(Box(Vector3(0.55, 0.45, 0.4), Vector3(0.12, 0.08, 0.1)), Vector3(0.3, -0.2, 0.1), 0.5, 0.25),
+            Collider(Ellipsoid(Vector3(0.3, 0.7, 0.35), Vector3(0.15, 0.1, 0.12)), Vector3(-0.1, 0.0, 0.4), 0.2, 0.7),
+        ]
+    elif name == "periodic":
+        cfg = Configuration(resolution=[nx, ny, nz], cell_size=h, time_step=0.5 * h, vorticity_confinement_enabled=True)
+        vb = cfg.velocity_boundary
+        for f in (vb.x_min, vb.x_max, vb.z_min, vb.z_max):
+            f.mode = VelocityBoundaryMode.periodic
+        vb.y_min.mode = VelocityBoundaryMode.normal_fixed_tangent_zero_gradient
+        vb.y_max.mode = VelocityBoundaryMode.zero_gradient
+        for sb in (cfg.pressure_boundary, cfg.density_boundary, cfg.temperature_boundary):
+            for f in (sb.x_min, sb.x_max, sb.z_min, sb.z_max):
+                f.mode = ScalarBoundaryMode.periodic
+        cfg.inflows = [Inflow(Vector3(0.5, 0.2, 0.5), 0.2, 1.0, 1.0)]
+    elif name == "fixed_values":
+        cfg = Configuration(resolution=[nx, ny, nz], cell_size=h, time_step=0.5 * h, vorticity_confinement_enabled=False)
+        vb = cfg.velocity_boundary
+        vb.x_min.mode = VelocityBoundaryMode.fixed_value
+        vb.x_min.value = Vector3(0.2, 0.05, -0.1)
+        vb.x_max.mode = VelocityBoundaryMode.normal_fixed_tangent_zero_gradient
+        vb.x_max.value = Vector3(0.1, 0.0, 0.0)
+        vb.y_min.mode = VelocityBoundaryMode.normal_fixed_tangent_zero_gradient
+        vb.y_max.mode = VelocityBoundaryMode.zero_gradient
+        vb.z_min.mode = VelocityBoundaryMode.fixed_value
+        vb.z_max.mode = VelocityBoundaryMode.zero_gradient
+        cfg.pressure_boundary.y_max.mode = ScalarBoundaryMode.fixed_value
+        cfg.pressure_boundary.y_max.value = 0.05
+        cfg.pressure_boundary.x_max.mode = ScalarBoundaryMode.fixed_value
+        cfg.pressure_boundary.x_max.value = -0.02
+        cfg.density_boundary.x_min.mode = ScalarBoundaryMode.fixed_value
+        cfg.density_boundary.x_min.value = 0.3
+        cfg.temperature_boundary.y_min.mode = ScalarBoundaryMode.fixed_value
+        cfg.temperature_boundary.y_min.value = 0.6
+    else:
+        raise KeyError(name)
+    return cfg
+
+
+SCENARIOS = ("plume", "vorticity", "colliders", "periodic", "fixed_values")
+
+
+def with_solver(cfg: Configuration, kind: str, iterations=None, tolerance=None) -> Configuration:
+    cfg = copy.deepcopy(cfg)
+    if kind == "rbgs":
+        cfg.pressure_solver = PressureSolver.red_black_gauss_seidel
+        if iterations is not None:
+            cfg.pressure_iterations = iterations
+    else:
+        cfg.pressure_solver = PressureSolver.jacobi_pcg
+        if iterations is not None:
+            cfg.pressure_max_iterations = iterations
+        if tolerance is not None:
+            cfg.pressure_tolerance = tolerance
+    return cfg
+
+
+def sizes(res):
+    nx, ny, nz = res
+    n = nx * ny * nz
+    return n, ((nx + 1) * ny * nz, nx * (ny + 1) * nz, nx * ny * (nz + 1))
+
+
+def seeded_state(res, seed=0, amp=0.3, scalars=True):
+    rng = np.random.default_rng(seed)
+    n, f = sizes(res)
+    return {"density": rng.uniform(0, 1, n) if scalars else np.zeros(n),
+            "temperature": rng.uniform(0, 1, n) if scalars else np.zeros(n),
+            "velocity": [rng.uniform(-amp, amp, f[a]) for a in range(3)]}
+
+
+def seeded_control(res, seed=1, amp=0.5):
+    rng = np.random.default_rng(seed)
+    n, _ = sizes(res)
+    return {"density_source": rng.uniform(0, amp, n), "temperature_source": rng.uniform(0, amp, n),
+            "acceleration": [rng.uniform(-amp, amp, n) for _ in range(3)]}
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, np.float64).ravel()
+    b = np.asarray(b, np.float64).ravel()
+    d = np.linalg.norm(a - b)
+    s = max(np.linalg.norm(b), 1e-300)
+    return float(d / s)
+
+
+def state_arrays(s):
+    return [s["density"], s["temperature"], *s["velocity"]]
+
+
+# ---------------------------------------------------------------- torch side
+def to_model_state(model, ctx, arrays, dtype=None):
+    import torch
+    s = model.allocate_state(ctx) if dtype is None else model.allocate_state_adjoint(ctx)
+    for t, a in zip(model._state_tensors(s), state_arrays(arrays)):
+        t.copy_(torch.as_tensor(np.asarray(a), dtype=t.dtype))
+    return s
+
+
+def to_model_control(model, ctx, arrays, adjoint=False):
+    import torch
+    c = model.allocate_control_adjoint(ctx) if adjoint else model.allocate_control(ctx)
+    ts = [c.density_source.values, c.temperature_source.values, c.external_acceleration.x.values, c.external_acceleration.y.values,
+          c.external_acceleration.z.values]
+    arrs = [arrays["density_source"], arrays["temperature_source"], *arrays["acceleration"]]
+    for t, a in zip(ts, arrs):
+        t.copy_(torch.as_tensor(np.asarray(a), dtype=t.dtype))
+    return c
+
+
+def from_model_state(model, s):
+    ts = [t.detach().cpu().numpy() for t in model._state_tensors(s)]
+    return {"density": ts[0], "temperature": ts[1], "velocity": ts[2:5]}
+
+
+def cache_arrays(k):
+    """Model StepCache -> oracle cache dict."""
+    v = k.vorticity.detach().cpu().numpy()
+    return {"sourced_density": k.sourced_density.values.cpu().numpy(), "sourced_temperature": k.sourced_temperature.values.cpu().numpy(),
+            "force": [k.force.x.values.cpu().numpy(), k.force.y.values.cpu().numpy(), k.force.z.values.cpu().numpy()],
+            "centered_velocity": [v[0], v[1], v[2]], "vorticity": [v[3], v[4], v[5]], "magnitude": v[6],
+            "normal": [v[7], v[8], v[9]], "normalizer": v[10],
+            "forced_velocity": [t.cpu().numpy() for t in k.forced_velocity.components()],
+            "advected_velocity": [t.cpu().numpy() for t in k.advected_velocity.components()]}

@@ -1,0 +1,74 @@
+"""The C ABI library loads and exports every function include/*.h declares
+(no compute: runs without a GPU)."""
+import ctypes
+import glob
+import os
+import re
+
+from common import ROOT
+
+from diff_solver_b200 import _native
+
+
+def declared_functions():
+    names = set()
+    for h in glob.glob(os.path.join(ROOT, "include", "*.h")):
+        text = open(h).read()
+        text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+        for m in re.finditer(r"^\s*(?:XsStatus|size_t|uint64_t|int|const char\*|void)\s+(xs_[a-z0-9_]+)\s*\(", text, flags=re.M):
+            names.add(m.group(1))
+    return names
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _native.lib()
+    names = declared_functions()
+    assert len(names) > 30
+    missing = [n for n in sorted(names) if not hasattr(lib, n)]
+    assert not missing, f"declared in include/*.h but not exported: {missing}"
+
+
+def test_python_signatures_cover_the_header():
+    assert declared_functions() <= set(_native.SIGNATURES), set(declared_functions()) - set(_native.SIGNATURES)
+
+
+def test_struct_layouts_match_header():
+    # sizes on x86-64: pointers 8 bytes, doubles 8-aligned
+    assert ctypes.sizeof(_native.XsGrid) == 20
+    assert ctypes.sizeof(_native.XsScalarBoundary) == 48
+    assert ctypes.sizeof(_native.XsVelocityBoundary) == 96
+    assert ctypes.sizeof(_native.XsPressureSolve) == 24
+    assert ctypes.sizeof(_native.XsSolveStats) == 40
+    assert ctypes.sizeof(_native.XsInflow) == 24
+
+
+def test_status_strings_and_launch_counter_without_gpu():
+    lib = _native.lib()
+    assert lib.xs_status_string(_native.XS_NOT_CONVERGED).decode().startswith("pressure")
+    assert isinstance(lib.xs_launch_count(), int)
+
+
+def test_workspace_queries_without_gpu():
+    lib = _native.lib()
+    g = _native.XsGrid(16, 14, 12, 1 / 16, 1 / 32)
+    n = 16 * 14 * 12
+    ws = lib.xs_projection_workspace_bytes(g)
+    assert ws >= n * (8 + 4 * 5)
+    bad = _native.XsGrid(0, 14, 12, 1 / 16, 1 / 32)
+    assert lib.xs_projection_workspace_bytes(bad) == 0
+    m = _native.XsSmokeModel()
+    m.grid = g
+    fwd = lib.xs_smoke_workspace_bytes(ctypes.byref(m), 0)
+    diff = lib.xs_smoke_workspace_bytes(ctypes.byref(m), 1)
+    assert diff > fwd > ws
+
+
+def test_invalid_arguments_are_rejected_before_any_launch():
+    lib = _native.lib()
+    g = _native.XsGrid(0, 4, 4, 0.25, 0.1)
+    st = lib.xs_source_forward(None, g, None, None, None, None, 0, 0, None)
+    assert st == _native.XS_INVALID_ARGUMENT
+    solve = _native.XsPressureSolve(0, 10, 1e-6, None)
+    g2 = _native.XsGrid(4, 4, 4, 0.25, 0.1)
+    assert lib.xs_pressure_solve(None, g2, ctypes.byref(solve), 0, None, _native.XsScalarBoundary(), None, None, None) == \
+        _native.XS_INVALID_ARGUMENT

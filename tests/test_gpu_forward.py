@@ -1,0 +1,161 @@
+"""GPU parity of the forward step: CUDA product vs the CPU oracle and vs the
+reference's own kernels (oracle/_ref), through the C ABI."""
+import numpy as np
+import pytest
+
+from common import (PARAMS, SCENARIOS, cache_arrays, from_model_state, rel_l2, scenario, seeded_control, seeded_state, state_arrays,
+                    to_model_control, to_model_state, with_solver)
+
+from oracle import binding as ob
+
+pytestmark = pytest.mark.gpu
+
+STATE_FIELDS = ("density", "temperature", "u", "v", "w")
+
+
+def run_product(cfg, st_arr, ctl_arr, mode=0):
+    import torch
+    from diff_solver_b200.model import ExecutionMode, Model, fill_parameters
+    model = Model(cfg)
+    ctx = model.allocate_context(ExecutionMode(mode))
+    st = to_model_state(model, ctx, st_arr)
+    ctl = to_model_control(model, ctx, ctl_arr)
+    par = fill_parameters(model.allocate_parameters(ctx), **PARAMS)
+    nxt = model.allocate_state(ctx)
+    k = model.allocate_step_cache(ctx)
+    model.forward_step(st, ctl, par, nxt, k, ctx)
+    torch.cuda.synchronize()
+    return model, ctx, from_model_state(model, nxt), cache_arrays(k), ctx.read_solve_stats()
+
+
+def domain_of(ctx):
+    d = ctx.domain
+    return {"mask": d.cell_mask, "cv": list(d.collider_velocity.components()), "cd": d.collider_density.values,
+            "ct": d.collider_temperature.values, "anchor": d.pressure_anchor}
+
+
+@pytest.mark.parametrize("name", SCENARIOS)
+def test_forward_step_matches_fp64_oracle(cuda, name):
+    cfg = with_solver(scenario(name), "pcg", iterations=20000, tolerance=1e-10)
+    st, ctl = seeded_state(tuple(cfg.resolution), seed=21), seeded_control(tuple(cfg.resolution), seed=22)
+    _, _, nxt, k, stats = run_product(cfg, st, ctl)
+    assert stats["status"] == 0 and stats["final_residual"] <= 1e-10
+    P = ob.Problem(cfg, "f64", solver="pcg", iterations=20000, tolerance=1e-13)
+    onxt, ok, ost, _ = P.forward_step(st, ctl, PARAMS)
+    for f, a, b in zip(STATE_FIELDS, state_arrays(nxt), state_arrays(onxt)):
+        assert rel_l2(a, b) < 1e-5, (name, f, rel_l2(a, b))
+    for key in ("sourced_density", "sourced_temperature"):
+        assert rel_l2(k[key], ok[key]) < 1e-6
+    for a in range(3):
+        assert rel_l2(k["force"][a], ok["force"][a]) < 1e-5
+        assert rel_l2(k["forced_velocity"][a], ok["forced_velocity"][a]) < 1e-6
+        assert rel_l2(k["advected_velocity"][a], ok["advected_velocity"][a]) < 1e-5
+
+
+@pytest.mark.parametrize("name", SCENARIOS)
+def test_fixed_sweeps_match_the_reference_kernels(cuda, name):
+    """RBGS kind, same sweep count: the product against the reference's own
+    operators.cu on identical seeded inputs (1e-5 relative L2 per field)."""
+    import torch
+    from oracle import ref_binding as rb
+    if not rb.available():
+        pytest.skip("reference harness not built")
+    cfg = with_solver(scenario(name), "rbgs", iterations=40)
+    res = tuple(cfg.resolution)
+    st, ctl = seeded_state(res, seed=23), seeded_control(res, seed=24)
+    model, ctx, nxt, k, _ = run_product(cfg, st, ctl)
+    ref = rb.Reference(cfg, domain_of(ctx))
+    dev = torch.device("cuda")
+    t = lambda a: torch.as_tensor(np.asarray(a), dtype=torch.float32, device=dev).contiguous()
+    s_in = [t(a) for a in state_arrays(st)]
+    c_in = [t(ctl["density_source"]), t(ctl["temperature_source"])] + [t(a) for a in ctl["acceleration"]]
+    p_in = [torch.tensor([PARAMS[k_]], dtype=torch.float32, device=dev) for k_ in
+            ("ambient_temperature", "density_buoyancy", "temperature_buoyancy", "vorticity_confinement")]
+    out = [torch.zeros_like(x) for x in s_in]
+    n = s_in[0].numel()
+    cache = [torch.zeros(n, device=dev) for _ in range(5)] + [torch.zeros((11, n), device=dev)] + \
+            [torch.zeros_like(x) for x in s_in[2:]] * 2
+    cache = cache[:6] + [torch.zeros_like(x) for x in s_in[2:]] + [torch.zeros_like(x) for x in s_in[2:]]
+    ref.forward_step(s_in, c_in, p_in, out, cache)
+    torch.cuda.synchronize()
+    for f, a, b in zip(STATE_FIELDS, state_arrays(nxt), [o.cpu().numpy() for o in out]):
+        assert rel_l2(a, b) < 1e-5, (name, f, rel_l2(a, b))
+    # and the CPU oracle (FP32 build) is pinned by the same kernels
+    P = ob.Problem(cfg, "f32", solver="rbgs", iterations=40)
+    onxt, _, _, _ = P.forward_step(st, ctl, PARAMS)
+    for f, a, b in zip(STATE_FIELDS, state_arrays(onxt), [o.cpu().numpy() for o in out]):
+        assert rel_l2(a, b) < 1e-5, ("oracle", name, f, rel_l2(a, b))
+
+
+def test_pcg_step_matches_reference_rbgs_run_to_the_same_residual(cuda):
+    """The plain method against the reference kernels with their red-black
+    sweeps iterated until the same 1e-6 relative residual."""
+    import torch
+    from oracle import ref_binding as rb
+    if not rb.available():
+        pytest.skip("reference harness not built")
+    cfg = with_solver(scenario("plume", res=(24, 24, 24)), "pcg", iterations=20000, tolerance=1e-6)
+    res = tuple(cfg.resolution)
+    st, ctl = seeded_state(res, seed=25, amp=0.2), seeded_control(res, seed=26)
+    model, ctx, nxt, k, stats = run_product(cfg, st, ctl)
+    assert stats["final_residual"] <= 1e-6
+    ref = rb.Reference(cfg, domain_of(ctx))
+    dev = torch.device("cuda")
+    t = lambda a: torch.as_tensor(np.asarray(a), dtype=torch.float32, device=dev).contiguous()
+    s_in = [t(a) for a in state_arrays(st)]
+    c_in = [t(ctl["density_source"]), t(ctl["temperature_source"])] + [t(a) for a in ctl["acceleration"]]
+    p_in = [torch.tensor([PARAMS[k_]], dtype=torch.float32, device=dev) for k_ in
+            ("ambient_temperature", "density_buoyancy", "temperature_buoyancy", "vorticity_confinement")]
+    out = [torch.zeros_like(x) for x in s_in]
+    n = s_in[0].numel()
+    cache = [torch.zeros(n, device=dev) for _ in range(5)] + [torch.zeros((11, n), device=dev)] + \
+            [torch.zeros_like(x) for x in s_in[2:]] + [torch.zeros_like(x) for x in s_in[2:]]
+    sweeps, residual = ref.forward_step(s_in, c_in, p_in, out, cache, tolerance=1e-6)
+    torch.cuda.synchronize()
+    assert residual <= 1e-6 and sweeps > 0
+    for f, a, b in zip(STATE_FIELDS, state_arrays(nxt), [o.cpu().numpy() for o in out]):
+        assert rel_l2(a, b) < 1e-5, (f, rel_l2(a, b), sweeps)
+
+
+def test_pressure_solve_reports_convergence_and_respects_the_cap(cuda):
+    cfg = with_solver(scenario("plume", res=(20, 20, 20)), "pcg", iterations=20000, tolerance=1e-6)
+    st, ctl = seeded_state(tuple(cfg.resolution), seed=27), seeded_control(tuple(cfg.resolution), seed=28)
+    _, _, _, _, stats = run_product(cfg, st, ctl)
+    assert stats["status"] == 0 and 0 < stats["final_residual"] <= 1e-6 and stats["iterations"] > 10
+    capped = with_solver(cfg, "pcg", iterations=5, tolerance=1e-6)
+    _, _, _, _, s2 = run_product(capped, st, ctl)
+    assert s2["status"] == 2 and s2["iterations"] <= 5 and s2["final_residual"] > 1e-6
+
+
+def test_warm_start_exact_guess_and_fallback(cuda):
+    import torch
+    from diff_solver_b200 import _native as N
+    cfg = scenario("colliders", res=(20, 18, 16))
+    model_cfg = with_solver(cfg, "pcg", iterations=20000, tolerance=1e-8)
+    st = seeded_state(tuple(cfg.resolution), seed=29)
+    P = ob.Problem(model_cfg, "f64")
+    rhs = P.pressure_rhs(st["velocity"])
+    p, _ = P.pcg(rhs, 20000, 1e-13)
+    from diff_solver_b200.model import ExecutionMode, Model
+    model = Model(model_cfg)
+    ctx = model.allocate_context(ExecutionMode.forward)
+    L = N.lib()
+    g = ctx.native.grid
+    ws = torch.zeros(L.xs_projection_workspace_bytes(g), dtype=torch.uint8, device="cuda")
+    rhs_t = torch.as_tensor(rhs, dtype=torch.float32, device="cuda")
+    out = torch.zeros_like(rhs_t)
+    mask = ctx.native.cell_mask
+
+    def solve(guess):
+        s = N.XsPressureSolve(0, 20000, 1e-8, None if guess is None else guess.data_ptr())
+        N.check("solve", L.xs_pressure_solve(None, g, s, ctx.native.pressure_anchor, mask, ctx.native.pressure_boundary,
+                                             rhs_t.data_ptr(), out.data_ptr(), ws.data_ptr()))
+        st_ = N.XsSolveStats()
+        N.check("stats", L.xs_read_solve_stats(None, ws.data_ptr(), st_))
+        return st_
+    cold = solve(None)
+    exact = solve(torch.as_tensor(p, dtype=torch.float32, device="cuda"))
+    assert exact.warm_start_used == 1 and exact.iterations < cold.iterations // 4
+    garbage = solve(torch.full_like(rhs_t, 1e3))
+    assert garbage.warm_start_used == 0 and garbage.status == 0 and garbage.iterations == cold.iterations
+    assert rel_l2(out.cpu().numpy(), p) < 1e-5
