@@ -109,8 +109,8 @@ __device__ __forceinline__ void scatter_scalar(double* v, const Vec3& p, double 
 #pragma unroll
             for (int dx = 0; dx < 2; ++dx) {
                 const int x = x0 + dx, y = y0 + dy, z = z0 + dz;
-                if ((x < 0 && b.modes[0] == 0u) || (x >= g.nx && b.modes[1] == 0u) || (y < 0 && b.modes[2] == 0u) ||
-                    (y >= g.ny && b.modes[3] == 0u) || (z < 0 && b.modes[4] == 0u) || (z >= g.nz && b.modes[5] == 0u))
+                if ((x < 0 && b.modes[0] == 0u) || (beyond(x, g.nx) && b.modes[1] == 0u) || (y < 0 && b.modes[2] == 0u) ||
+                    (beyond(y, g.ny) && b.modes[3] == 0u) || (z < 0 && b.modes[4] == 0u) || (beyond(z, g.nz) && b.modes[5] == 0u))
                     continue;
                 atomicAdd(v + mapped_cell(x, y, z, g, periodic(b, 0), periodic(b, 1), periodic(b, 2)), adj * wx[dx] * wy[dy] * wz[dz]);
             }

@@ -113,14 +113,21 @@ __device__ __forceinline__ uint64_t mapped_face(int x, int y, int z, const Grid&
                 map_coordinate(z, ez, periodic(b, 2), g.nz), ex, ey);
 }
 
+// The reference compares int coordinates with the grid's uint32_t extents
+// (cuda_types.h:13-19): `x >= grid.nx` is then also true for x < 0, and
+// `max(0, min(grid.nx - 1, x))` clamps as unsigned, sending x = -1 to nx - 1.
+// Both behaviours are part of its results and are kept here.
+__device__ __forceinline__ bool beyond(int c, int n) { return static_cast<unsigned>(c) >= static_cast<unsigned>(n); }
+__device__ __forceinline__ int uclamp(int c, int n) { return static_cast<int>(umin(static_cast<unsigned>(c), static_cast<unsigned>(n - 1))); }
+
 // operators.cu:115-123: value of a cell-centred field, boundary aware.
 __device__ __forceinline__ float load_scalar(const float* __restrict__ v, int x, int y, int z, const Grid& g, const XsScalarBoundary& b) {
     if (x < 0 && b.modes[0] == 0u) return b.values[0];
-    if (x >= g.nx && b.modes[1] == 0u) return b.values[1];
+    if (beyond(x, g.nx) && b.modes[1] == 0u) return b.values[1];
     if (y < 0 && b.modes[2] == 0u) return b.values[2];
-    if (y >= g.ny && b.modes[3] == 0u) return b.values[3];
+    if (beyond(y, g.ny) && b.modes[3] == 0u) return b.values[3];
     if (z < 0 && b.modes[4] == 0u) return b.values[4];
-    if (z >= g.nz && b.modes[5] == 0u) return b.values[5];
+    if (beyond(z, g.nz) && b.modes[5] == 0u) return b.values[5];
     return __ldg(v + mapped_cell(x, y, z, g, periodic(b, 0), periodic(b, 1), periodic(b, 2)));
 }
 
@@ -237,9 +244,9 @@ __device__ __forceinline__ bool solid_at(Vec3 p, const uint32_t* mask, const Gri
     if (periodic(b, 0)) p.x -= floorf(p.x / (g.nx * g.h)) * g.nx * g.h;
     if (periodic(b, 1)) p.y -= floorf(p.y / (g.ny * g.h)) * g.ny * g.h;
     if (periodic(b, 2)) p.z -= floorf(p.z / (g.nz * g.h)) * g.nz * g.h;
-    const int x = max(0, min(g.nx - 1, static_cast<int>(floorf(p.x / g.h))));
-    const int y = max(0, min(g.ny - 1, static_cast<int>(floorf(p.y / g.h))));
-    const int z = max(0, min(g.nz - 1, static_cast<int>(floorf(p.z / g.h))));
+    const int x = uclamp(static_cast<int>(floorf(p.x / g.h)), g.nx);
+    const int y = uclamp(static_cast<int>(floorf(p.y / g.h)), g.ny);
+    const int z = uclamp(static_cast<int>(floorf(p.z / g.h)), g.nz);
     return __ldg(mask + idx3(x, y, z, g.nx, g.ny)) != 0u;
 }
 

@@ -209,6 +209,8 @@ struct PcgArgs {
     SolverState* st;
     double tol;
     uint32_t max_iterations;
+    FastGeom fast;
+    uint32_t use_fast;
 };
 
 enum ResidualMode { kFromZero = 0, kFromGuess = 1, kFromX64 = 2 };
@@ -335,9 +337,155 @@ __device__ void fold_phase(const PcgArgs& a, int k, float alpha) {
     }
 }
 
+// ------------------------------------------------------------ fast path
+// Grids without colliders whose x extent is a multiple of 4: each thread
+// owns 4 consecutive cells of a row (float4 loads and stores), indices are
+// 32-bit, and the operator's diagonal and neighbour offsets follow from the
+// row's boundary flags instead of a per-cell stencil.
+
+inline FastDiv make_fastdiv(uint32_t d) {
+    uint32_t l = 0;
+    while ((1ull << l) < d) ++l;
+    const uint32_t shift = 31 + l;
+    return FastDiv{((1ull << shift) / d) + 1, shift};
+}
+
+__device__ __forceinline__ uint32_t fastdiv(uint32_t n, const FastDiv& f) {
+    return static_cast<uint32_t>((static_cast<uint64_t>(n) * f.m) >> f.shift);
+}
+
+struct RowGeom {
+    int32_t off[4];  // -y, +y, -z, +z neighbour offsets; 0 = no neighbour
+    float dyz;       // diagonal share of the y and z directions
+};
+
+__device__ __forceinline__ RowGeom row_geom(const FastGeom& f, uint32_t y, uint32_t z) {
+    RowGeom r;
+    r.dyz = 0.0f;
+    const int32_t sy = static_cast<int32_t>(f.nx), sz = static_cast<int32_t>(f.nx * f.ny);
+    const uint32_t c[2] = {y, z};
+    const uint32_t size[2] = {f.ny, f.nz};
+    const int32_t stride[2] = {sy, sz};
+#pragma unroll
+    for (int d = 0; d < 2; ++d) {
+        // lower side
+        if (c[d] > 0) { r.off[2 * d] = -stride[d]; r.dyz += 1.0f; }
+        else if (f.kind[2 + 2 * d] == 2u) { r.off[2 * d] = stride[d] * static_cast<int32_t>(size[d] - 1); r.dyz += 1.0f; }
+        else { r.off[2 * d] = 0; if (f.kind[2 + 2 * d] == 1u) r.dyz += 1.0f; }
+        // upper side
+        if (c[d] + 1 < size[d]) { r.off[2 * d + 1] = stride[d]; r.dyz += 1.0f; }
+        else if (f.kind[3 + 2 * d] == 2u) { r.off[2 * d + 1] = -stride[d] * static_cast<int32_t>(size[d] - 1); r.dyz += 1.0f; }
+        else { r.off[2 * d + 1] = 0; if (f.kind[3 + 2 * d] == 1u) r.dyz += 1.0f; }
+    }
+    return r;
+}
+
+// Offsets of the x neighbours of the group's first and last cell (0: none)
+// and the diagonals of the four cells.
+__device__ __forceinline__ void x_geom(const FastGeom& f, uint32_t x0, float dyz, int32_t& left, int32_t& right, float4& d) {
+    d = make_float4(dyz + 2.0f, dyz + 2.0f, dyz + 2.0f, dyz + 2.0f);
+    if (x0 > 0) left = -1;
+    else if (f.kind[0] == 2u) left = static_cast<int32_t>(f.nx) - 1;
+    else { left = 0; d.x -= f.kind[0] == 1u ? 0.0f : 1.0f; }
+    if (x0 + 4 < f.nx) right = 4;
+    else if (f.kind[1] == 2u) right = 4 - static_cast<int32_t>(f.nx);
+    else { right = 0; d.w -= f.kind[1] == 1u ? 0.0f : 1.0f; }
+}
+
+__device__ __forceinline__ float4 ld4(const float* p) { return *reinterpret_cast<const float4*>(p); }
+__device__ __forceinline__ void st4(float* p, const float4& v) { *reinterpret_cast<float4*>(p) = v; }
+__device__ __forceinline__ float4 axpy4(const float4& a, float b, const float4& x) {
+    return make_float4(fmaf(b, x.x, a.x), fmaf(b, x.y, a.y), fmaf(b, x.z, a.z), fmaf(b, x.w, a.w));
+}
+
+// spmv_phase for the fast path.
+template <bool kFirst>
+__device__ void spmv_fast(const PcgArgs& a, const FastGeom& f, int k, float beta, float alpha_prev, double& pq) {
+    const float* zv = a.z;
+    const float* pold = a.p[(k + 1) & 1];
+    float* pnew = a.p[k & 1];
+    pq = 0.0;
+    auto value4 = [&](uint32_t j) -> float4 { return kFirst ? ld4(pnew + j) : axpy4(ld4(zv + j), beta, ld4(pold + j)); };
+    auto value1 = [&](uint32_t j) -> float { return kFirst ? pnew[j] : fmaf(beta, pold[j], zv[j]); };
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < f.groups; t += gridDim.x * blockDim.x) {
+        const uint32_t i = 4u * t;
+        const uint32_t row = fastdiv(i, f.dnx);
+        const uint32_t x0 = i - row * f.nx;
+        const uint32_t z = fastdiv(row, f.dny);
+        const uint32_t y = row - z * f.ny;
+        const RowGeom rg = row_geom(f, y, z);
+        int32_t left, right;
+        float4 d;
+        x_geom(f, x0, rg.dyz, left, right, d);
+        float4 po;
+        float4 c;
+        if (kFirst) {
+            c = ld4(pnew + i);
+        } else {
+            po = ld4(pold + i);
+            c = axpy4(ld4(zv + i), beta, po);
+        }
+        float4 s = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            if (rg.off[q] != 0) {
+                const float4 v = value4(static_cast<uint32_t>(static_cast<int32_t>(i) + rg.off[q]));
+                s.x += v.x; s.y += v.y; s.z += v.z; s.w += v.w;
+            }
+        }
+        const float l = left != 0 ? value1(static_cast<uint32_t>(static_cast<int32_t>(i) + left)) : 0.0f;
+        const float r = right != 0 ? value1(static_cast<uint32_t>(static_cast<int32_t>(i) + right)) : 0.0f;
+        float4 qv;
+        qv.x = d.x * c.x - (s.x + l + c.y);
+        qv.y = d.y * c.y - (s.y + c.x + c.z);
+        qv.z = d.z * c.z - (s.z + c.y + c.w);
+        qv.w = d.w * c.w - (s.w + c.z + r);
+        if (f.anchor - i < 4u) {  // the anchor cell is not an unknown
+            const uint32_t lane = f.anchor - i;
+            if (lane == 0) qv.x = 0.0f; else if (lane == 1) qv.y = 0.0f; else if (lane == 2) qv.z = 0.0f; else qv.w = 0.0f;
+        }
+        if (!kFirst) {
+            st4(pnew + i, c);
+            const float4 e = ld4(a.e + i);
+            st4(a.e + i, axpy4(e, alpha_prev, po));
+        }
+        st4(a.q + i, qv);
+        pq += static_cast<double>(c.x) * qv.x + static_cast<double>(c.y) * qv.y + static_cast<double>(c.z) * qv.z +
+              static_cast<double>(c.w) * qv.w;
+    }
+}
+
+// update_phase for the fast path.
+__device__ void update_fast(const PcgArgs& a, const FastGeom& f, float alpha, double (&v)[2]) {
+    v[0] = v[1] = 0.0;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < f.groups; t += gridDim.x * blockDim.x) {
+        const uint32_t i = 4u * t;
+        const uint32_t row = fastdiv(i, f.dnx);
+        const uint32_t x0 = i - row * f.nx;
+        const uint32_t z = fastdiv(row, f.dny);
+        const uint32_t y = row - z * f.ny;
+        const RowGeom rg = row_geom(f, y, z);
+        int32_t left, right;
+        float4 d;
+        x_geom(f, x0, rg.dyz, left, right, d);
+        float4 zz = ld4(a.z + i);
+        const float4 q = ld4(a.q + i);
+        zz.x -= alpha * q.x / d.x;
+        zz.y -= alpha * q.y / d.y;
+        zz.z -= alpha * q.z / d.z;
+        zz.w -= alpha * q.w / d.w;
+        st4(a.z + i, zz);
+        const double r0 = static_cast<double>(zz.x) * d.x, r1 = static_cast<double>(zz.y) * d.y, r2 = static_cast<double>(zz.z) * d.z,
+                     r3 = static_cast<double>(zz.w) * d.w;
+        v[0] += r0 * zz.x + r1 * zz.y + r2 * zz.z + r3 * zz.w;
+        v[1] += r0 * r0 + r1 * r1 + r2 * r2 + r3 * r3;
+    }
+}
+
 constexpr uint32_t kMaxRefinements = 4;
 
-__global__ void __launch_bounds__(kBlock) pcg_kernel(PcgArgs a) {
+template <bool kFast>
+__global__ void __launch_bounds__(kBlock, 4) pcg_kernel(PcgArgs a) {
     __shared__ double red[4 * 32];
     SolverState* st = a.st;
     double v3[3];
@@ -371,12 +519,18 @@ __global__ void __launch_bounds__(kBlock) pcg_kernel(PcgArgs a) {
         bool broke = false;
         while (true) {
             double pq[1];
-            spmv_phase(a, k, beta, alpha, pq[0]);
+            if (kFast) {
+                if (k == 0) spmv_fast<true>(a, a.fast, k, beta, alpha, pq[0]);
+                else spmv_fast<false>(a, a.fast, k, beta, alpha, pq[0]);
+            } else {
+                spmv_phase(a, k, beta, alpha, pq[0]);
+            }
             if (!grid_reduce<1>(st, a.partials, pq, red)) return;
             if (!(pq[0] > 0.0) || !isfinite(pq[0])) { broke = true; break; }
             alpha = static_cast<float>(rz / pq[0]);
             double v2[2];
-            update_phase(a, alpha, v2);
+            if (kFast) update_fast(a, a.fast, alpha, v2);
+            else update_phase(a, alpha, v2);
             if (!grid_reduce<2>(st, a.partials, v2, red)) return;
             ++iterations;
             beta = static_cast<float>(v2[0] / rz);
@@ -566,6 +720,7 @@ namespace {
 struct DeviceLimits {
     int sms = 0;
     int pcg_blocks_per_sm = 0;
+    int pcg_fast_blocks_per_sm = 0;
     int rbgs_blocks_per_sm = 0;
     int rev_blocks_per_sm = 0;
 };
@@ -580,7 +735,10 @@ XsStatus device_limits(DeviceLimits& out) {
     if (dev != cached_device) {
         DeviceLimits l;
         if (cudaDeviceGetAttribute(&l.sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return XS_CUDA_ERROR;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&l.pcg_blocks_per_sm, pcg_kernel, kBlock, 0) != cudaSuccess) return XS_CUDA_ERROR;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&l.pcg_blocks_per_sm, pcg_kernel<false>, kBlock, 0) != cudaSuccess)
+            return XS_CUDA_ERROR;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&l.pcg_fast_blocks_per_sm, pcg_kernel<true>, kBlock, 0) != cudaSuccess)
+            return XS_CUDA_ERROR;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&l.rbgs_blocks_per_sm, rbgs_kernel, kBlock, 0) != cudaSuccess) return XS_CUDA_ERROR;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&l.rev_blocks_per_sm, rbgs_reverse_kernel, kBlock, 0) != cudaSuccess)
             return XS_CUDA_ERROR;
@@ -645,7 +803,26 @@ XsStatus solve_pressure(cudaStream_t stream, const Grid& g, const XsPressureSolv
     a.st = w.state;
     a.tol = solve.tolerance;
     a.max_iterations = solve.max_iterations;
-    return launch_cooperative(pcg_kernel, persistent_blocks(lim.pcg_blocks_per_sm, lim.sms, cell_count(g)), a, stream);
+    const uint64_t n = cell_count(g);
+    a.use_fast = (mask == nullptr && g.nx % 4 == 0 && n < (1ull << 31)) ? 1u : 0u;
+    if (a.use_fast) {
+        FastGeom& f = a.fast;
+        f.nx = static_cast<uint32_t>(g.nx);
+        f.ny = static_cast<uint32_t>(g.ny);
+        f.nz = static_cast<uint32_t>(g.nz);
+        f.n = static_cast<uint32_t>(n);
+        f.groups = static_cast<uint32_t>(n / 4);
+        f.dnx = make_fastdiv(f.nx);
+        f.dny = make_fastdiv(f.ny);
+        f.anchor = anchor < n ? anchor : static_cast<uint32_t>(n);
+        for (int face = 0; face < 6; ++face) {
+            const int d = face / 2;
+            const bool per = pb.modes[2 * d] == 2u && pb.modes[2 * d + 1] == 2u;
+            f.kind[face] = per ? 2u : (pb.modes[face] == 0u ? 1u : 0u);
+        }
+    }
+    if (a.use_fast) return launch_cooperative(pcg_kernel<true>, persistent_blocks(lim.pcg_fast_blocks_per_sm, lim.sms, n / 4), a, stream);
+    return launch_cooperative(pcg_kernel<false>, persistent_blocks(lim.pcg_blocks_per_sm, lim.sms, n), a, stream);
 }
 
 XsStatus reverse_rbgs(cudaStream_t stream, const Grid& g, uint32_t sweeps, uint32_t anchor, const uint32_t* mask,

@@ -30,6 +30,23 @@ struct PressureWorkspace {
     size_t bytes;
 };
 
+// Division by a runtime constant for numerators below 2^31:
+// q = (n * m) >> shift with m = floor(2^shift / d) + 1, shift = 31 + ceil(log2 d).
+struct FastDiv {
+    uint64_t m;
+    uint32_t shift;
+};
+
+// Geometry of the collider-free fast path of the pressure operator.  Face
+// kinds: 0 Neumann (dropped), 1 fixed value (counts in the diagonal),
+// 2 periodic (wraps).
+struct FastGeom {
+    uint32_t nx, ny, nz, n, groups;
+    FastDiv dnx, dny;
+    uint32_t anchor;  // n when there is none
+    uint32_t kind[6];
+};
+
 PressureWorkspace carve_pressure_workspace(void* base, const Grid& g);
 size_t pressure_workspace_bytes(const Grid& g);
 

@@ -25,8 +25,28 @@ __host__ __device__ inline VortCache vort_cache(float* base, uint64_t n) {
                      base + 7 * n, base + 8 * n, base + 9 * n, base + 10 * n};
 }
 
+// operators.cu:662-667: the reference's clamp mixes uint32_t and int, so a
+// coordinate of -1 reads the far side (n - 1); see uclamp.
 __device__ __forceinline__ uint64_t clamped(int x, int y, int z, const Grid& g) {
-    return idx3(max(0, min(g.nx - 1, x)), max(0, min(g.ny - 1, y)), max(0, min(g.nz - 1, z)), g.nx, g.ny);
+    return idx3(uclamp(x, g.nx), uclamp(y, g.ny), uclamp(z, g.nz), g.nx, g.ny);
+}
+
+// Sources of the transposed clamped central difference along axis d for
+// cell m at coordinate c (extent n): a cell j reads uclamp(c_j + 1) with
+// weight +1 and uclamp(c_j - 1) with weight -1.  Fills up to 4 (j, w).
+__device__ __forceinline__ int difference_sources(int x, int y, int z, int d, const Grid& g, uint64_t (&j)[4], double (&w)[4]) {
+    const int c = d == 0 ? x : (d == 1 ? y : z);
+    const int n = d == 0 ? g.nx : (d == 1 ? g.ny : g.nz);
+    const int64_t stride = d == 0 ? 1 : (d == 1 ? static_cast<int64_t>(g.nx) : static_cast<int64_t>(g.nx) * g.ny);
+    const int64_t m = static_cast<int64_t>(idx3(x, y, z, g.nx, g.ny));
+    int k = 0;
+    if (c >= 1) { j[k] = static_cast<uint64_t>(m - stride); w[k++] = 1.0; }
+    if (c + 1 < n) { j[k] = static_cast<uint64_t>(m + stride); w[k++] = -1.0; }
+    if (c == n - 1) {
+        j[k] = static_cast<uint64_t>(m); w[k++] = 1.0;                    // c_j + 1 = n clamps back to n - 1
+        j[k] = static_cast<uint64_t>(m - stride * c); w[k++] = -1.0;    // c_j - 1 = -1 lands on n - 1
+    }
+    return k;
 }
 
 // operators.cu:676-685
@@ -188,40 +208,16 @@ __global__ void magnitude_gather_kernel(Grid g, const uint32_t* __restrict__ mas
     decode(m, g.nx, g.ny, x, y, z);
     const double s = 0.5 / g.h;
     double acc = 0.0;
-    // A cell j at offset (dx,dy,dz) = +-1 along one axis reads m through
-    // clamped(j + e) / clamped(j - e).  Enumerate candidate j: the cells at
-    // m -+ e, and m itself when m sits on a boundary (clamping maps j +- e
-    // back onto j).
-    const int coord[3] = {x, y, z};
-    const int size[3] = {g.nx, g.ny, g.nz};
 #pragma unroll
     for (int d = 0; d < 3; ++d) {
-        // j = m - e reads m as its "+" neighbour (weight +s) when j exists.
-        // j = m + e reads m as its "-" neighbour (weight -s) when j exists.
-        // j = m reads itself as "+" neighbour if m is at the upper edge and as
-        // "-" neighbour if m is at the lower edge.
-        for (int side = 0; side < 3; ++side) {
-            int jx = x, jy = y, jz = z;
-            double w;
-            if (side == 0) {
-                if (coord[d] - 1 < 0) continue;
-                if (d == 0) jx -= 1; else if (d == 1) jy -= 1; else jz -= 1;
-                w = s;
-            } else if (side == 1) {
-                if (coord[d] + 1 >= size[d]) continue;
-                if (d == 0) jx += 1; else if (d == 1) jy += 1; else jz += 1;
-                w = -s;
-            } else {
-                w = 0.0;
-                if (coord[d] == size[d] - 1) w += s;
-                if (coord[d] == 0) w -= s;
-                if (w == 0.0) continue;
-            }
-            const uint64_t j = idx3(jx, jy, jz, g.nx, g.ny);
-            if (is_solid(mask, j)) continue;
+        uint64_t j[4];
+        double w[4];
+        const int k = difference_sources(x, y, z, d, g, j, w);
+        for (int q = 0; q < k; ++q) {
+            if (is_solid(mask, j[q])) continue;
             double gx, gy, gz;
-            normal_gradient_adjoint(c, a, j, gx, gy, gz);
-            acc += w * (d == 0 ? gx : (d == 1 ? gy : gz));
+            normal_gradient_adjoint(c, a, j[q], gx, gy, gz);
+            acc += s * w[q] * (d == 0 ? gx : (d == 1 ? gy : gz));
         }
     }
     a.mag[m] = acc;
@@ -242,30 +238,12 @@ __global__ void magnitude_apply_kernel(Grid g, const uint32_t* __restrict__ mask
 // Sum over fluid cells j of coefficient * wa(j) where j's clamped stencil
 // along axis d reads m: weight +1 for "plus" reads, -1 for "minus" reads.
 __device__ __forceinline__ double gather_axis(const Grid& g, const uint32_t* mask, int x, int y, int z, int d, const double* wa) {
-    const int coord[3] = {x, y, z};
-    const int size[3] = {g.nx, g.ny, g.nz};
+    uint64_t j[4];
+    double w[4];
+    const int k = difference_sources(x, y, z, d, g, j, w);
     double acc = 0.0;
-    for (int side = 0; side < 3; ++side) {
-        int jx = x, jy = y, jz = z;
-        double w;
-        if (side == 0) {
-            if (coord[d] - 1 < 0) continue;
-            if (d == 0) jx -= 1; else if (d == 1) jy -= 1; else jz -= 1;
-            w = 1.0;
-        } else if (side == 1) {
-            if (coord[d] + 1 >= size[d]) continue;
-            if (d == 0) jx += 1; else if (d == 1) jy += 1; else jz += 1;
-            w = -1.0;
-        } else {
-            w = 0.0;
-            if (coord[d] == size[d] - 1) w += 1.0;
-            if (coord[d] == 0) w -= 1.0;
-            if (w == 0.0) continue;
-        }
-        const uint64_t j = idx3(jx, jy, jz, g.nx, g.ny);
-        if (is_solid(mask, j)) continue;
-        acc += w * wa[j];
-    }
+    for (int q = 0; q < k; ++q)
+        if (!is_solid(mask, j[q])) acc += w[q] * wa[j[q]];
     return acc;
 }
 

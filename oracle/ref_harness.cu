@@ -347,4 +347,20 @@ int ref_rbgs(cudaStream_t stream, const RefModel* m, const float* rhs, float* pr
     return cudaStreamSynchronize(stream) == cudaSuccess ? 0 : 2;
 }
 
+// The reference's vorticity_forward (operators.cu:973-979) alone.
+int ref_vorticity_forward(cudaStream_t stream, const RefModel* m, float* const u[3], const float* confinement, float* cache, float* force[3]) {
+    try {
+        vorticity_forward(stream, m->grid, m->cell_mask, {u[0], u[1], u[2]}, confinement, vort_view(cache, cells(m->grid)),
+                          {force[0], force[1], force[2]});
+    } catch (const std::exception&) { return 1; }
+    return cudaStreamSynchronize(stream) == cudaSuccess ? 0 : 2;
+}
+
+// Layout check: the harness' view of the model block as 32-bit words.
+size_t ref_model_words(const RefModel* m, uint32_t* out, size_t capacity) {
+    const size_t words = sizeof(RefModel) / 4;
+    std::memcpy(out, m, 4 * (words < capacity ? words : capacity));
+    return sizeof(RefModel);
+}
+
 }  // extern "C"

@@ -173,13 +173,21 @@ static size_t mapped_face(int x, int y, int z, G g, int axis, const VB* b) {
     return idx3(x, y, z, ex, ey);
 }
 /* operators.cu:115-123 */
+/* The reference compares the int coordinate with the grid's uint32_t
+ * extent (cuda_types.h:13-19), so `x >= grid.nx` is also true for x < 0:
+ * below the grid, an upper face with a fixed value is hit too (after the
+ * lower face's own test).  Restated with unsigned comparisons. */
+static int beyond(int c, int n) { return (unsigned)c >= (unsigned)n; }
+/* max(0, min(n - 1, c)) with one uint32_t operand: an unsigned clamp, so
+ * c = -1 maps to n - 1 (used by solid_at and the vorticity stencils). */
+static int uclamp(int c, int n) { unsigned u = (unsigned)c, m = (unsigned)(n - 1); return (int)(u < m ? u : m); }
 static real load_scalar(const real* v, int x, int y, int z, G g, const SB* b) {
     if (x < 0 && b->modes[0] == 0u) return b->values[0];
-    if (x >= g.nx && b->modes[1] == 0u) return b->values[1];
+    if (beyond(x, g.nx) && b->modes[1] == 0u) return b->values[1];
     if (y < 0 && b->modes[2] == 0u) return b->values[2];
-    if (y >= g.ny && b->modes[3] == 0u) return b->values[3];
+    if (beyond(y, g.ny) && b->modes[3] == 0u) return b->values[3];
     if (z < 0 && b->modes[4] == 0u) return b->values[4];
-    if (z >= g.nz && b->modes[5] == 0u) return b->values[5];
+    if (beyond(z, g.nz) && b->modes[5] == 0u) return b->values[5];
     return v[mapped_cell(x, y, z, g, speriodic(b, 0), speriodic(b, 1), speriodic(b, 2))];
 }
 /* operators.cu:125-134 */
@@ -237,8 +245,8 @@ static void scatter_scalar(adj* v, V3 p, adj a, G g, const SB* b) {
     adj wz[2] = {1.0 - (adj)(gz - (real)z0), (adj)(gz - (real)z0)};
     for (int dz = 0; dz < 2; ++dz) for (int dy = 0; dy < 2; ++dy) for (int dx = 0; dx < 2; ++dx) {
         int x = x0 + dx, y = y0 + dy, z = z0 + dz;
-        if ((x < 0 && b->modes[0] == 0u) || (x >= g.nx && b->modes[1] == 0u) || (y < 0 && b->modes[2] == 0u) ||
-            (y >= g.ny && b->modes[3] == 0u) || (z < 0 && b->modes[4] == 0u) || (z >= g.nz && b->modes[5] == 0u)) continue;
+        if ((x < 0 && b->modes[0] == 0u) || (beyond(x, g.nx) && b->modes[1] == 0u) || (y < 0 && b->modes[2] == 0u) ||
+            (beyond(y, g.ny) && b->modes[3] == 0u) || (z < 0 && b->modes[4] == 0u) || (beyond(z, g.nz) && b->modes[5] == 0u)) continue;
         v[mapped_cell(x, y, z, g, speriodic(b, 0), speriodic(b, 1), speriodic(b, 2))] += a * wx[dx] * wy[dy] * wz[dz];
     }
 }
@@ -274,9 +282,9 @@ static int solid_at(V3 p, const uint32_t* mask, G g, const VB* b) {
     if (vperiodic(b, 0)) p.x -= rfloor(p.x / ((real)g.nx * g.h)) * (real)g.nx * g.h;
     if (vperiodic(b, 1)) p.y -= rfloor(p.y / ((real)g.ny * g.h)) * (real)g.ny * g.h;
     if (vperiodic(b, 2)) p.z -= rfloor(p.z / ((real)g.nz * g.h)) * (real)g.nz * g.h;
-    int x = clampi((int)rfloor(p.x / g.h), 0, g.nx - 1);
-    int y = clampi((int)rfloor(p.y / g.h), 0, g.ny - 1);
-    int z = clampi((int)rfloor(p.z / g.h), 0, g.nz - 1);
+    int x = uclamp((int)rfloor(p.x / g.h), g.nx);
+    int y = uclamp((int)rfloor(p.y / g.h), g.ny);
+    int z = uclamp((int)rfloor(p.z / g.h), g.nz);
     return mask[idx3(x, y, z, g.nx, g.ny)] != 0u;
 }
 /* operators.cu:256-276 */
@@ -614,11 +622,14 @@ static void advect_scalar_vjp(const og_config* c, G g, const SB* sb, const VB* v
 static const real smooth_eps = (real)1.0e-6;
 
 /* operators.cu:662-674 */
+/* `max(0, min(grid.nx - 1, x))` in the reference mixes uint32_t and int;
+ * CUDA's mixed min/max compare as unsigned, so x = -1 lands on nx - 1
+ * (the far side) and x >= nx on nx - 1. */
 static real cload(const real* v, int x, int y, int z, G g) {
-    return v[idx3(clampi(x, 0, g.nx - 1), clampi(y, 0, g.ny - 1), clampi(z, 0, g.nz - 1), g.nx, g.ny)];
+    return v[idx3(uclamp(x, g.nx), uclamp(y, g.ny), uclamp(z, g.nz), g.nx, g.ny)];
 }
 static void cscatter(adj* v, int x, int y, int z, G g, adj a) {
-    v[idx3(clampi(x, 0, g.nx - 1), clampi(y, 0, g.ny - 1), clampi(z, 0, g.nz - 1), g.nx, g.ny)] += a;
+    v[idx3(uclamp(x, g.nx), uclamp(y, g.ny), uclamp(z, g.nz), g.nx, g.ny)] += a;
 }
 /* operators.cu:676-685 */
 static void centered_velocity(const og_config* c, G g, real* const u[3], real* cv[3]) {

@@ -106,6 +106,40 @@ def seeded_control(res, seed=1, amp=0.5):
             "acceleration": [rng.uniform(-amp, amp, n) for _ in range(3)]}
 
 
+def inflow_mask(cfg):
+    """Cells whose centre lies in an inflow sphere (FP32, as the kernels test it)."""
+    nx, ny, nz = (int(v) for v in cfg.resolution)
+    h = np.float32(cfg.cell_size)
+    z, y, x = np.meshgrid(np.arange(nz, dtype=np.float32), np.arange(ny, dtype=np.float32), np.arange(nx, dtype=np.float32), indexing="ij")
+    px, py, pz = (x + np.float32(0.5)) * h, (y + np.float32(0.5)) * h, (z + np.float32(0.5)) * h
+    hit = np.zeros((nz, ny, nx), bool)
+    dens = np.zeros((nz, ny, nx), np.float32)
+    temp = np.zeros((nz, ny, nx), np.float32)
+    for f in cfg.inflows:
+        dx, dy, dz = px - np.float32(f.center.x), py - np.float32(f.center.y), pz - np.float32(f.center.z)
+        inside = dx * dx + dy * dy + dz * dz <= np.float32(f.radius) * np.float32(f.radius)
+        hit |= inside
+        dens[inside] = f.density
+        temp[inside] = f.temperature
+    return hit.ravel(), dens.ravel(), temp.ravel()
+
+
+def reference_control(cfg, state, control):
+    """Control arrays that make the reference's additive sources
+    (operators.cu:286-290) reproduce the inflow spheres: inside a sphere the
+    source is (value - state) / dt."""
+    hit, dens, temp = inflow_mask(cfg)
+    dt = np.float32(cfg.time_step)
+    out = {"density_source": np.array(control["density_source"], np.float32),
+           "temperature_source": np.array(control["temperature_source"], np.float32),
+           "acceleration": [np.array(a, np.float32) for a in control["acceleration"]]}
+    rho = np.asarray(state["density"], np.float32)
+    tem = np.asarray(state["temperature"], np.float32)
+    out["density_source"][hit] = (dens[hit] - rho[hit]) / dt
+    out["temperature_source"][hit] = (temp[hit] - tem[hit]) / dt
+    return out
+
+
 def rel_l2(a, b):
     a = np.asarray(a, np.float64).ravel()
     b = np.asarray(b, np.float64).ravel()

@@ -3,8 +3,8 @@ reference's own kernels (oracle/_ref), through the C ABI."""
 import numpy as np
 import pytest
 
-from common import (PARAMS, SCENARIOS, cache_arrays, from_model_state, rel_l2, scenario, seeded_control, seeded_state, state_arrays,
-                    to_model_control, to_model_state, with_solver)
+from common import (PARAMS, SCENARIOS, cache_arrays, from_model_state, reference_control, rel_l2, scenario, seeded_control,
+                    seeded_state, state_arrays, to_model_control, to_model_state, with_solver)
 
 from oracle import binding as ob
 
@@ -68,7 +68,8 @@ def test_fixed_sweeps_match_the_reference_kernels(cuda, name):
     dev = torch.device("cuda")
     t = lambda a: torch.as_tensor(np.asarray(a), dtype=torch.float32, device=dev).contiguous()
     s_in = [t(a) for a in state_arrays(st)]
-    c_in = [t(ctl["density_source"]), t(ctl["temperature_source"])] + [t(a) for a in ctl["acceleration"]]
+    rctl = reference_control(cfg, st, ctl)  # the reference has no inflow primitive: emulate it with sources
+    c_in = [t(rctl["density_source"]), t(rctl["temperature_source"])] + [t(a) for a in rctl["acceleration"]]
     p_in = [torch.tensor([PARAMS[k_]], dtype=torch.float32, device=dev) for k_ in
             ("ambient_temperature", "density_buoyancy", "temperature_buoyancy", "vorticity_confinement")]
     out = [torch.zeros_like(x) for x in s_in]
@@ -103,7 +104,8 @@ def test_pcg_step_matches_reference_rbgs_run_to_the_same_residual(cuda):
     dev = torch.device("cuda")
     t = lambda a: torch.as_tensor(np.asarray(a), dtype=torch.float32, device=dev).contiguous()
     s_in = [t(a) for a in state_arrays(st)]
-    c_in = [t(ctl["density_source"]), t(ctl["temperature_source"])] + [t(a) for a in ctl["acceleration"]]
+    rctl = reference_control(cfg, st, ctl)  # the reference has no inflow primitive: emulate it with sources
+    c_in = [t(rctl["density_source"]), t(rctl["temperature_source"])] + [t(a) for a in rctl["acceleration"]]
     p_in = [torch.tensor([PARAMS[k_]], dtype=torch.float32, device=dev) for k_ in
             ("ambient_temperature", "density_buoyancy", "temperature_buoyancy", "vorticity_confinement")]
     out = [torch.zeros_like(x) for x in s_in]
