@@ -11,7 +11,8 @@ import os
 _HERE = os.path.dirname(os.path.abspath(__file__))
 LIBRARY_PATH = os.path.join(_HERE, "libdiffsmoke.so")
 
-XS_OK, XS_CUDA_ERROR, XS_NOT_CONVERGED, XS_NUMERICAL_ERROR, XS_INVALID_ARGUMENT, XS_TIMEOUT = range(6)
+XS_OK, XS_CUDA_ERROR, XS_NOT_CONVERGED, XS_NUMERICAL_ERROR, XS_INVALID_ARGUMENT, XS_TIMEOUT, XS_CAPACITY_EXCEEDED = range(7)
+XS_STATIC_SOLVE_MAX_CELLS = 64 * 64 * 64
 XS_SOLVER_JACOBI_PCG, XS_SOLVER_RED_BLACK_GAUSS_SEIDEL = 0, 1
 XS_MODE_FORWARD, XS_MODE_DIFFERENTIABLE = 0, 1
 XS_MAX_INFLOWS = 8
@@ -126,6 +127,8 @@ SIGNATURES = {
     "xs_pressure_solve": (_S, [_V, _G, C.POINTER(XsPressureSolve), C.c_uint32, _V, XsScalarBoundary, _V, _V, _V]),
     "xs_read_solve_stats": (_S, [_V, _V, C.POINTER(XsSolveStats)]),
     "xs_solve_stats_offset": (C.c_size_t, []),
+    "xs_pressure_solve_static": (_S, [_V, _G, C.POINTER(XsPressureSolve), C.c_uint32, _V, XsScalarBoundary, _V, _V,
+                                      C.POINTER(XsSolveStats)]),
     "xs_smoke_build_domain": (_S, [_V, _G, XsScalarBoundary, _V, C.c_uint32, _V, XsVector, _V, _V, C.POINTER(C.c_uint32)]),
     "xs_smoke_workspace_bytes": (C.c_size_t, [C.POINTER(XsSmokeModel), C.c_uint32]),
     "xs_smoke_forward_step": (_S, [_V, C.POINTER(XsSmokeModel), XsState, XsControl, XsParameters, XsState, XsStepCache, _V]),

@@ -36,6 +36,7 @@ const char* xs_status_string(int status) {
         case XS_NUMERICAL_ERROR: return "numerical error (NaN/Inf or breakdown)";
         case XS_INVALID_ARGUMENT: return "invalid argument";
         case XS_TIMEOUT: return "device-side wait timed out";
+        case XS_CAPACITY_EXCEEDED: return "grid larger than the entry point's fixed capacity";
         default: return "unknown status";
     }
 }

@@ -42,7 +42,8 @@ typedef enum XsStatus {
     XS_NOT_CONVERGED = 2,       /* a pressure solve hit its iteration cap */
     XS_NUMERICAL_ERROR = 3,     /* NaN/Inf or breakdown inside a solve */
     XS_INVALID_ARGUMENT = 4,    /* sizes, pointers or modes rejected before launch */
-    XS_TIMEOUT = 5              /* a bounded device-side wait gave up */
+    XS_TIMEOUT = 5,             /* a bounded device-side wait gave up */
+    XS_CAPACITY_EXCEEDED = 6    /* the grid is larger than a fixed-size entry point admits */
 } XsStatus;
 
 /* cuda_types.h:13-19 */
@@ -215,6 +216,23 @@ XsStatus xs_projection_vjp(cudaStream_t stream, XsGrid grid, const XsPressureSol
 XsStatus xs_pressure_solve(cudaStream_t stream, XsGrid grid, const XsPressureSolve* solve, uint32_t pressure_anchor,
                            const uint32_t* cell_mask, XsScalarBoundary pressure_boundary, const float* rhs, float* pressure,
                            void* workspace);
+
+/* No counterpart in the reference.  The same pressure solve as
+ * xs_pressure_solve for callers that cannot allocate device memory (hosts
+ * that only hand over their input and output buffers, or that forbid
+ * allocations outside their own pool): it takes no workspace and calls no
+ * allocator; its scratch is one library-owned device array sized for at
+ * most XS_STATIC_SOLVE_MAX_CELLS cells (about 7.5 MB, held by each GPU the
+ * entry point runs on until the process exits).  Larger grids return
+ * XS_CAPACITY_EXCEEDED without launching.  All calls share that array:
+ * calls that overlap on the GPU race, so order them on one stream.  The
+ * first call on a device resolves the array's address (make it before any
+ * stream capture).  host_stats may be NULL; when given, the call
+ * synchronises the stream and copies the solve statistics into it. */
+#define XS_STATIC_SOLVE_MAX_CELLS (64u * 64u * 64u)
+XsStatus xs_pressure_solve_static(cudaStream_t stream, XsGrid grid, const XsPressureSolve* solve, uint32_t pressure_anchor,
+                                  const uint32_t* cell_mask, XsScalarBoundary pressure_boundary, const float* rhs, float* pressure,
+                                  XsSolveStats* host_stats);
 
 /* Byte offset of the XsSolveStats record inside a projection or step
  * workspace (device memory), for asynchronous copies that do not
