@@ -139,6 +139,8 @@ SIGNATURES = {
     "xs_smoke_reduce_metrics": (_S, [_V, C.POINTER(XsSmokeModel), _V, _V, XsVector, XsVector, _V]),
     "xs_smoke_read_solve_stats": (_S, [_V, C.POINTER(XsSmokeModel), _V, C.c_uint32, C.POINTER(XsSolveStats),
                                        C.POINTER(XsSolveStats)]),
+    "xs_conv3d_bf16": (_S, [_V, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, _V, _V, _V, _V, C.c_uint32,
+                            _V]),
     "xs_launch_count": (C.c_uint64, []),
     "xs_last_cuda_error": (C.c_int, []),
     "xs_status_string": (C.c_char_p, [C.c_int]),

@@ -339,6 +339,20 @@ XsStatus xs_smoke_reduce_metrics(cudaStream_t stream, const XsSmokeModel* model,
 XsStatus xs_smoke_read_solve_stats(cudaStream_t stream, const XsSmokeModel* model, const void* workspace, uint32_t mode,
                                    XsSolveStats* forward_stats, XsSolveStats* adjoint_stats);
 
+/* ------------------------------------------------------------------------ */
+/* learned pressure warm start (no reference counterpart)                    */
+/* ------------------------------------------------------------------------ */
+
+/* 3x3x3 convolution with zero padding on tcgen05 tensor cores: out = relu?(
+ * conv(input, weights) + bias).  input [batch][nz][ny][nx][in_channels] and
+ * output [..][out_channels] BF16 (NDHWC); weights [27][out][in] BF16 with tap
+ * = (dz * 3 + dy) * 3 + dx; bias FP32 or NULL.  Channels 16, 32 or 64;
+ * nx * ny >= 128 with min(nx, 128) dividing 128, nx and 128 / that dividing ny.
+ * error_flag (device int, may be NULL) is set if a bounded wait expired. */
+XsStatus xs_conv3d_bf16(cudaStream_t stream, uint32_t batch, uint32_t nx, uint32_t ny, uint32_t nz, uint32_t in_channels,
+                        uint32_t out_channels, const void* input, const void* weights, const float* bias, void* output, uint32_t relu,
+                        int* error_flag);
+
 /* Number of kernel launches the library has issued since load (for launch
  * accounting). */
 uint64_t xs_launch_count(void);
