@@ -141,6 +141,9 @@ SIGNATURES = {
                                        C.POINTER(XsSolveStats)]),
     "xs_conv3d_bf16": (_S, [_V, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, _V, _V, _V, _V, C.c_uint32,
                             _V]),
+    "xs_conv3d_weight_grad_bf16": (_S, [_V, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, _V, _V, _V, _V,
+                                        C.c_uint32, _V]),
+    "xs_conv3d_weight_grad_scratch_floats": (C.c_size_t, [C.c_uint32] * 6),
     "xs_launch_count": (C.c_uint64, []),
     "xs_last_cuda_error": (C.c_int, []),
     "xs_status_string": (C.c_char_p, [C.c_int]),

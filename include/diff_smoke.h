@@ -353,6 +353,18 @@ XsStatus xs_conv3d_bf16(cudaStream_t stream, uint32_t batch, uint32_t nx, uint32
                         uint32_t out_channels, const void* input, const void* weights, const float* bias, void* output, uint32_t relu,
                         int* error_flag);
 
+/* Weight gradient of xs_conv3d_bf16 on tcgen05: weight_grad[27][out][in]
+ * (FP32) = (accumulate ? weight_grad : 0) + sum over voxels of
+ * input[v + tap][in] * output_grad[v][out] (output_grad is the gradient of
+ * the pre-activation, BF16 NDHWC).  partial is FP32 scratch of
+ * xs_conv3d_weight_grad_scratch_floats() elements; the per-CTA partial sums
+ * are added in a fixed order, so the result is deterministic. */
+XsStatus xs_conv3d_weight_grad_bf16(cudaStream_t stream, uint32_t batch, uint32_t nx, uint32_t ny, uint32_t nz, uint32_t in_channels,
+                                    uint32_t out_channels, const void* input, const void* output_grad, float* partial, float* weight_grad,
+                                    uint32_t accumulate, int* error_flag);
+size_t xs_conv3d_weight_grad_scratch_floats(uint32_t batch, uint32_t nx, uint32_t ny, uint32_t nz, uint32_t in_channels,
+                                            uint32_t out_channels);
+
 /* Number of kernel launches the library has issued since load (for launch
  * accounting). */
 uint64_t xs_launch_count(void);
