@@ -42,12 +42,14 @@ class XsInflow(C.Structure):
 
 
 class XsPressureSolve(C.Structure):
-    _fields_ = [("kind", C.c_uint32), ("max_iterations", C.c_uint32), ("tolerance", C.c_double), ("initial_guess", C.c_void_p)]
+    _fields_ = [("kind", C.c_uint32), ("max_iterations", C.c_uint32), ("tolerance", C.c_double), ("initial_guess", C.c_void_p),
+                ("scale_guess", C.c_uint32)]
 
 
 class XsSolveStats(C.Structure):
     _fields_ = [("iterations", C.c_uint32), ("status", C.c_uint32), ("refinements", C.c_uint32), ("warm_start_used", C.c_uint32),
-                ("rhs_norm", C.c_double), ("initial_residual", C.c_double), ("final_residual", C.c_double)]
+                ("rhs_norm", C.c_double), ("initial_residual", C.c_double), ("final_residual", C.c_double),
+                ("guess_scale", C.c_double)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -64,7 +66,7 @@ class XsSmokeModel(C.Structure):
                 ("vorticity_confinement_enabled", C.c_uint32), ("pressure_anchor", C.c_uint32), ("pressure", XsPressureSolve),
                 ("inflows", C.c_void_p), ("inflow_count", C.c_uint32), ("cell_mask", C.c_void_p), ("collider_velocity", XsVector),
                 ("collider_density", C.c_void_p), ("collider_temperature", C.c_void_p), ("solve_begin", C.c_void_p),
-                ("solve_end", C.c_void_p)]
+                ("solve_end", C.c_void_p), ("warm_start", C.c_void_p)]
 
 
 class XsState(C.Structure):
@@ -139,11 +141,24 @@ SIGNATURES = {
     "xs_smoke_reduce_metrics": (_S, [_V, C.POINTER(XsSmokeModel), _V, _V, XsVector, XsVector, _V]),
     "xs_smoke_read_solve_stats": (_S, [_V, C.POINTER(XsSmokeModel), _V, C.c_uint32, C.POINTER(XsSolveStats),
                                        C.POINTER(XsSolveStats)]),
+    "xs_smoke_pressure_fields": (_S, [C.POINTER(XsSmokeModel), _V, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
     "xs_conv3d_bf16": (_S, [_V, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, _V, _V, _V, _V, C.c_uint32,
                             _V]),
     "xs_conv3d_weight_grad_bf16": (_S, [_V, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, _V, _V, _V, _V,
                                         C.c_uint32, _V]),
     "xs_conv3d_weight_grad_scratch_floats": (C.c_size_t, [C.c_uint32] * 6),
+    "xs_warm_start_create": (_S, [C.POINTER(C.c_void_p), C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32]),
+    "xs_warm_start_destroy": (_S, [_V]),
+    "xs_warm_start_parameter_count": (C.c_size_t, []),
+    "xs_warm_start_initialize": (_S, [_V, _V, C.c_uint64]),
+    "xs_warm_start_set_parameters": (_S, [_V, _V, _V]),
+    "xs_warm_start_get_parameters": (_S, [_V, _V, _V]),
+    "xs_warm_start_predict": (_S, [_V, _V, C.c_uint32, _V, _V]),
+    "xs_warm_start_gradient": (_S, [_V, _V, C.c_uint32, _V, _V, _V, _V]),
+    "xs_warm_start_adam_step": (_S, [_V, _V, C.c_float, C.c_float, C.c_float, C.c_float]),
+    "xs_warm_start_train_step": (_S, [_V, _V, C.c_uint32, _V, _V, C.c_float, _V]),
+    "xs_warm_start_guess": (_S, [_V, _V, _G, _V, _V]),
+    "xs_warm_start_status": (_S, [_V, _V]),
     "xs_launch_count": (C.c_uint64, []),
     "xs_last_cuda_error": (C.c_int, []),
     "xs_status_string": (C.c_char_p, [C.c_int]),

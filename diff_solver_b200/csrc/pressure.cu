@@ -198,6 +198,7 @@ struct PcgArgs {
     const float* rhs_f;   // forward right-hand side (FP32), or
     const double* rhs_d;  // adjoint right-hand side (FP64)
     const float* guess;   // warm start or null
+    uint32_t scale_guess; // start from alpha * guess, alpha = (g.b) / (g.A g)
     double* x64;
     float* z;
     float* p[2];
@@ -219,9 +220,31 @@ __device__ __forceinline__ double rhs_at(const PcgArgs& a, uint64_t i) {
     return a.rhs_d ? a.rhs_d[i] : static_cast<double>(a.rhs_f[i]);
 }
 
+// Partial sums v = {g.b, g.A g} of the guess g over the active cells, for the
+// energy-optimal scale alpha = (g.b) / (g.A g) that minimises the A-norm of
+// the error of alpha g.
+__device__ void guess_energy_phase(const PcgArgs& a, double (&v)[2]) {
+    const Grid& g = a.op.g;
+    const uint64_t n = cell_count(g);
+    v[0] = v[1] = 0.0;
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        int x, y, z;
+        decode(i, g.nx, g.ny, x, y, z);
+        CellStencil s;
+        if (!stencil(a.op, x, y, z, i, s)) continue;
+        const double gi = a.guess[i];
+        double ag = s.diag * gi;
+#pragma unroll
+        for (int f = 0; f < 6; ++f)
+            if ((s.conn >> f) & 1u) { const uint64_t j = s.nb[f]; if (j != a.op.anchor) ag -= static_cast<double>(a.guess[j]); }
+        v[0] += gi * (rhs_at(a, i) + static_cast<double>(s.fixed_sum));
+        v[1] += gi * ag;
+    }
+}
+
 // r = b - A x in FP64; z = r/diag, p0 = z, e = 0; partial sums
-// v = {||b||^2, ||r||^2, r.z}.
-__device__ void residual_phase(const PcgArgs& a, int mode, double (&v)[3]) {
+// v = {||b||^2, ||r||^2, r.z}.  kFromGuess starts from scale * guess.
+__device__ void residual_phase(const PcgArgs& a, int mode, double (&v)[3], double scale = 1.0) {
     const Grid& g = a.op.g;
     const uint64_t n = cell_count(g);
     v[0] = v[1] = v[2] = 0.0;
@@ -245,6 +268,8 @@ __device__ void residual_phase(const PcgArgs& a, int mode, double (&v)[3]) {
 #pragma unroll
             for (int f = 0; f < 6; ++f)
                 if ((s.conn >> f) & 1u) { const uint64_t j = s.nb[f]; if (j != a.op.anchor) ax -= static_cast<double>(a.guess[j]); }
+            xi *= scale;
+            ax *= scale;
             a.x64[i] = xi;
         } else if (mode == kFromX64) {
             xi = a.x64[i];
@@ -489,13 +514,21 @@ __global__ void __launch_bounds__(kBlock, 4) pcg_kernel(PcgArgs a) {
     __shared__ double red[4 * 32];
     SolverState* st = a.st;
     double v3[3];
-    residual_phase(a, a.guess ? kFromGuess : kFromZero, v3);
+    double scale = a.guess ? 1.0 : 0.0;
+    if (a.guess && a.scale_guess) {
+        double e2[2];
+        guess_energy_phase(a, e2);
+        if (!grid_reduce<2>(st, a.partials, e2, red)) return;
+        scale = (e2[1] > 0.0 && isfinite(e2[0] / e2[1])) ? e2[0] / e2[1] : 0.0;
+    }
+    residual_phase(a, a.guess ? kFromGuess : kFromZero, v3, scale);
     if (!grid_reduce<3>(st, a.partials, v3, red)) return;
     const double bb = v3[0];
     double rr = v3[1], rz = v3[2];
     uint32_t warm = a.guess ? 1u : 0u;
-    if (a.guess && rr > bb) {  // the guess is worse than zero: fall back
+    if (a.guess && !(rr <= bb)) {  // the guess is worse than zero: fall back
         warm = 0u;
+        scale = 0.0;
         residual_phase(a, kFromZero, v3);
         if (!grid_reduce<3>(st, a.partials, v3, red)) return;
         rr = v3[1];
@@ -560,6 +593,7 @@ __global__ void __launch_bounds__(kBlock, 4) pcg_kernel(PcgArgs a) {
         st->stats.rhs_norm = sqrt(bb);
         st->stats.initial_residual = initial;
         st->stats.final_residual = bb > 0.0 ? sqrt(rr / bb) : 0.0;
+        st->stats.guess_scale = scale;
     }
 }
 
@@ -791,6 +825,7 @@ XsStatus solve_pressure(cudaStream_t stream, const Grid& g, const XsPressureSolv
     a.rhs_f = rhs_f;
     a.rhs_d = rhs_d;
     a.guess = solve.initial_guess;
+    a.scale_guess = solve.scale_guess;
     a.x64 = w.x64;
     a.z = w.z;
     a.p[0] = w.p0;

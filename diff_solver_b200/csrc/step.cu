@@ -7,6 +7,7 @@
 #include "common.cuh"
 #include "launch.cuh"
 #include "ops.cuh"
+#include "unet.cuh"
 
 namespace xs {
 
@@ -15,12 +16,20 @@ namespace xs {
 // the PCG kind the velocity is corrected from the FP64 iterate.
 XsStatus projection_forward(cudaStream_t st, const Grid& g, const XsPressureSolve& solve, uint32_t anchor, const uint32_t* mask,
                             const XsVector& u, const XsScalarBoundary& pb, float* pressure, float* rhs, const XsVector& out,
-                            void* workspace, cudaEvent_t begin, cudaEvent_t end) {
+                            void* workspace, cudaEvent_t begin, cudaEvent_t end, WarmStartNet* warm_start) {
     XsStatus s = launch_pressure_rhs(st, g, anchor, mask, u, rhs);
     if (s != XS_OK) return s;
     PressureWorkspace w{};
     if (begin && cudaEventRecord(begin, st) != cudaSuccess) return XS_CUDA_ERROR;
-    s = solve_pressure(st, g, solve, anchor, mask, pb, rhs, nullptr, pressure, nullptr, workspace, &w);
+    XsPressureSolve used = solve;
+    if (warm_start && solve.kind == XS_SOLVER_JACOBI_PCG) {
+        // learned guess (inside the timed solve): energy-scaled, with fallback to zero
+        float* guess = nullptr;
+        if ((s = warm_start_guess(warm_start, st, g, rhs, &guess)) != XS_OK) return s;
+        used.initial_guess = guess;
+        used.scale_guess = 1u;
+    }
+    s = solve_pressure(st, g, used, anchor, mask, pb, rhs, nullptr, pressure, nullptr, workspace, &w);
     if (s != XS_OK) return s;
     if (end && cudaEventRecord(end, st) != cudaSuccess) return XS_CUDA_ERROR;
     if (solve.kind == XS_SOLVER_RED_BLACK_GAUSS_SEIDEL) return launch_project(st, g, mask, u, pressure, out);
@@ -238,7 +247,8 @@ XsStatus xs_smoke_forward_step(cudaStream_t stream, const XsSmokeModel* m, XsSta
     if (s != XS_OK) return s;
     // projection
     s = projection_forward(stream, g, m->pressure, m->pressure_anchor, m->cell_mask, cache.advected_velocity, m->pressure_boundary,
-                           w.pressure, w.rhs, next_state.velocity, w.solver, m->solve_begin, m->solve_end);
+                           w.pressure, w.rhs, next_state.velocity, w.solver, m->solve_begin, m->solve_end,
+                           reinterpret_cast<WarmStartNet*>(m->warm_start));
     if (s != XS_OK) return s;
     // scalar advection of the sourced fields through the projected velocity
     return launch_advect_scalar_pair(stream, g, m->cell_mask, m->collider_density, m->collider_temperature, cache.sourced_density,
@@ -378,6 +388,14 @@ XsStatus xs_smoke_read_solve_stats(cudaStream_t stream, const XsSmokeModel* mode
     if (forward_stats) *forward_stats = st;
     if (adjoint_stats) *adjoint_stats = st;
     return s;
+}
+
+XsStatus xs_smoke_pressure_fields(const XsSmokeModel* model, void* workspace, float** pressure, float** rhs) {
+    if (!valid_model(model) || !workspace) return XS_INVALID_ARGUMENT;
+    const StepWorkspace w = carve_step(workspace, make_grid(model->grid), XS_MODE_FORWARD);
+    if (pressure) *pressure = w.pressure;
+    if (rhs) *rhs = w.rhs;
+    return XS_OK;
 }
 
 }  // extern "C"

@@ -23,4 +23,17 @@ bool make_weight_map(CUtensorMap* map, const void* base, uint32_t rows, uint32_t
 XsStatus conv3_forward(cudaStream_t st, const VolumeShape& s, int cin, int cout, const __nv_bfloat16* in, const __nv_bfloat16* w,
                        const float* bias, __nv_bfloat16* out, bool relu, int* error);
 
+// dw[27][cout][cin] (+)= sum_v x[v + tap][cin] * dy[v][cout]; partial is
+// scratch of wgrad_partial_floats(s, cin, cout) floats.
+XsStatus conv3_wgrad(cudaStream_t st, const VolumeShape& s, int cin, int cout, const __nv_bfloat16* x, const __nv_bfloat16* dy, float* partial,
+                     float* dw, bool accumulate, int* error);
+size_t wgrad_partial_floats(const VolumeShape& s, int cin, int cout);
+
+struct Grid;
+struct WarmStartNet;
+// Restricts a fine-grid right-hand side to the network grid, runs the
+// network and prolongs its output to the fine grid; *guess points into the
+// network's own storage.
+XsStatus warm_start_guess(WarmStartNet* net, cudaStream_t st, const Grid& g, const float* rhs, float** guess);
+
 }  // namespace xs

@@ -145,6 +145,41 @@ class ExecutionContext:
         self._warm_start = guess
         self.native.pressure.initial_guess = None if guess is None else guess.data_ptr()
 
+    def set_inflow(self, index: int, center=None, radius=None) -> None:
+        """Moves or resizes inflow ``index`` for the following steps (the
+        inflow table travels to the device with every launch)."""
+        if not 0 <= index < int(self.native.inflow_count):
+            raise IndexError(index)
+        f = self._inflows[index]
+        if center is not None:
+            f.center[:] = [float(v) for v in center]
+        if radius is not None:
+            f.radius = float(radius)
+
+    def set_learned_warm_start(self, network) -> None:
+        """Warm-start the forward pressure solves with a
+        :class:`~diff_solver_b200.warm_start.WarmStartNetwork` whose grid times
+        its factor equals this model's grid (None: zero guess).  The guess is
+        energy-scaled and PCG falls back to zero whenever it does not help."""
+        self._learned = network
+        self.native.warm_start = None if network is None else network.handle.value
+
+    def pressure_fields(self):
+        """(pressure, rhs) of the last forward pressure solve, as device tensors
+        viewing the workspace: the pairs the warm-start network trains on."""
+        p, b = C.c_void_p(), C.c_void_p()
+        N.check("xs_smoke_pressure_fields", N.lib().xs_smoke_pressure_fields(C.byref(self.native), C.c_void_p(self.workspace.data_ptr()),
+                                                                               C.byref(p), C.byref(b)))
+        n = int(self.native.grid.nx) * int(self.native.grid.ny) * int(self.native.grid.nz)
+        base = self.workspace.data_ptr()
+        flat = self.workspace.view(torch.uint8)
+
+        def view(ptr):
+            off = ptr.value - base
+            return flat[off:off + 4 * n].view(torch.float32)
+
+        return view(p), view(b)
+
 
 def _grid(cfg: Configuration) -> N.XsGrid:
     nx, ny, nz = (int(v) for v in cfg.resolution)

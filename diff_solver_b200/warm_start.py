@@ -1,0 +1,278 @@
+"""Learned pressure warm start (no reference counterpart).
+
+:class:`WarmStartNetwork` holds the native U-Net (``xs_warm_start_*`` in
+``include/diff_smoke.h``: tcgen05 convolutions, hand-written backward pass and
+Adam, all on the GPU).  :func:`train_on_plumes` trains it on (right-hand side,
+pressure) pairs that the plain PCG solver produces while it runs plume
+simulations with seeded random inflow centre, radius and buoyancy.
+
+A model uses a trained network through
+``ExecutionContext.set_learned_warm_start``: every forward pressure solve
+then restricts its right-hand side to the network grid, runs the network,
+prolongs the output, scales it by the energy-optimal factor and starts PCG
+from it, falling back to a zero guess whenever that is not better.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import math
+import time
+from dataclasses import dataclass
+from typing import Callable, List, Optional, Sequence
+
+import numpy as np
+import torch
+
+from . import _native as N
+
+
+class WarmStartNetwork:
+    """Handle of the native warm-start network on the grid ``shape`` (nx, ny,
+    nz, each a multiple of 8 with at least 128 cells per x-y plane at 1/8 of
+    the resolution).  ``factor`` is the ratio of a fluid grid to this grid
+    when the network serves a model."""
+
+    def __init__(self, shape: Sequence[int], max_batch: int = 1, factor: int = 1, seed: int = 0, stream: Optional[torch.cuda.Stream] = None):
+        self.shape = tuple(int(v) for v in shape)
+        self.max_batch = int(max_batch)
+        self.factor = int(factor)
+        self._stream = stream
+        self.handle = C.c_void_p()
+        N.check("xs_warm_start_create", N.lib().xs_warm_start_create(C.byref(self.handle), self.max_batch, *self.shape, self.factor))
+        N.check("xs_warm_start_initialize", N.lib().xs_warm_start_initialize(self.handle, self.stream_handle, int(seed)))
+
+    # ------------------------------------------------------------ plumbing
+    @property
+    def stream(self) -> torch.cuda.Stream:
+        return self._stream if self._stream is not None else torch.cuda.current_stream()
+
+    @property
+    def stream_handle(self):
+        return C.c_void_p(self.stream.cuda_stream)
+
+    @property
+    def cells(self) -> int:
+        return self.shape[0] * self.shape[1] * self.shape[2]
+
+    @staticmethod
+    def parameter_count() -> int:
+        return int(N.lib().xs_warm_start_parameter_count())
+
+    def close(self) -> None:
+        if self.handle and self.handle.value:
+            N.lib().xs_warm_start_destroy(self.handle)
+            self.handle = C.c_void_p()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ------------------------------------------------------------ parameters
+    def parameters(self) -> np.ndarray:
+        out = np.empty(self.parameter_count(), dtype=np.float32)
+        N.check("xs_warm_start_get_parameters", N.lib().xs_warm_start_get_parameters(self.handle, self.stream_handle, out.ctypes.data))
+        return out
+
+    def set_parameters(self, values: np.ndarray) -> None:
+        values = np.ascontiguousarray(values, dtype=np.float32)
+        if values.size != self.parameter_count():
+            raise ValueError(f"expected {self.parameter_count()} parameters, got {values.size}")
+        N.check("xs_warm_start_set_parameters", N.lib().xs_warm_start_set_parameters(self.handle, self.stream_handle, values.ctypes.data))
+
+    def save(self, path: str, **metadata) -> None:
+        np.savez(path, parameters=self.parameters(), grid=np.array(self.shape), **{k: np.asarray(v) for k, v in metadata.items()})
+
+    def load(self, path: str) -> dict:
+        with np.load(path) as f:
+            self.set_parameters(f["parameters"])
+            return {k: f[k] for k in f.files if k != "parameters"}
+
+    # ------------------------------------------------------------ compute
+    def _check_batch(self, t: torch.Tensor) -> int:
+        if t.dtype != torch.float32 or not t.is_cuda or not t.is_contiguous():
+            raise ValueError("expected a contiguous CUDA float32 tensor")
+        if t.numel() % self.cells:
+            raise ValueError(f"size {t.numel()} is not a whole number of {self.cells}-cell samples")
+        b = t.numel() // self.cells
+        if not 1 <= b <= self.max_batch:
+            raise ValueError(f"batch {b} outside 1..{self.max_batch}")
+        return b
+
+    def predict(self, rhs: torch.Tensor) -> torch.Tensor:
+        """Network output (channel 0) for a batch of right-hand sides on the
+        network grid, in units of the predicted pressure's RMS."""
+        b = self._check_batch(rhs)
+        out = torch.empty_like(rhs)
+        N.check("xs_warm_start_predict", N.lib().xs_warm_start_predict(self.handle, self.stream_handle, b, rhs.data_ptr(), out.data_ptr()))
+        return out
+
+    def gradient(self, rhs: torch.Tensor, pressure: torch.Tensor):
+        """(loss, gradient) of mean (out - p / rms(p))^2 (device tensors)."""
+        b = self._check_batch(rhs)
+        if pressure.shape != rhs.shape:
+            raise ValueError("rhs and pressure differ in shape")
+        grad = torch.empty(self.parameter_count(), dtype=torch.float32, device=rhs.device)
+        loss = torch.empty(1, dtype=torch.float64, device=rhs.device)
+        N.check("xs_warm_start_gradient", N.lib().xs_warm_start_gradient(self.handle, self.stream_handle, b, rhs.data_ptr(),
+                                                                         pressure.contiguous().data_ptr(), grad.data_ptr(), loss.data_ptr()))
+        return loss, grad
+
+    def adam_step(self, learning_rate: float, beta1: float = 0.9, beta2: float = 0.999, epsilon: float = 1e-8) -> None:
+        N.check("xs_warm_start_adam_step", N.lib().xs_warm_start_adam_step(self.handle, self.stream_handle, learning_rate, beta1, beta2,
+                                                                           epsilon))
+
+    def train_step(self, rhs: torch.Tensor, pressure: torch.Tensor, learning_rate: float, loss: Optional[torch.Tensor] = None):
+        b = self._check_batch(rhs)
+        if loss is None:
+            loss = torch.empty(1, dtype=torch.float64, device=rhs.device)
+        N.check("xs_warm_start_train_step", N.lib().xs_warm_start_train_step(self.handle, self.stream_handle, b, rhs.data_ptr(),
+                                                                             pressure.data_ptr(), learning_rate, loss.data_ptr()))
+        return loss
+
+    def guess(self, grid: N.XsGrid, rhs: torch.Tensor) -> torch.Tensor:
+        """Prolonged network guess for a right-hand side on a fluid grid of
+        ``factor`` x the network grid (before the solver's energy scaling)."""
+        out = torch.empty_like(rhs)
+        N.check("xs_warm_start_guess", N.lib().xs_warm_start_guess(self.handle, self.stream_handle, grid, rhs.data_ptr(), out.data_ptr()))
+        return out
+
+    def check(self) -> None:
+        """Synchronises and raises if a bounded wait inside a network kernel expired."""
+        N.check("xs_warm_start_status", N.lib().xs_warm_start_status(self.handle, self.stream_handle))
+
+
+# ---------------------------------------------------------------- training
+@dataclass
+class PlumeSampler:
+    """Seeded uniform ranges of the training plumes: inflow centre, radius and
+    temperature buoyancy (density buoyancy stays -0.1)."""
+    centre_low: tuple = (0.3, 0.06, 0.3)
+    centre_high: tuple = (0.7, 0.2, 0.7)
+    radius: tuple = (0.05, 0.12)
+    buoyancy: tuple = (0.2, 1.0)
+
+    def draw(self, rng: np.random.Generator):
+        c = tuple(float(rng.uniform(lo, hi)) for lo, hi in zip(self.centre_low, self.centre_high))
+        return c, float(rng.uniform(*self.radius)), float(rng.uniform(*self.buoyancy))
+
+
+class _Plume:
+    """One running plume simulation that yields a (rhs, pressure) pair per step."""
+
+    def __init__(self, resolution, rng: np.random.Generator, sampler: PlumeSampler, stream):
+        from .data import plume_configuration
+        from .model import ExecutionMode, Model, fill_parameters
+        self.rng = rng
+        self.sampler = sampler
+        centre, radius, buoyancy = sampler.draw(rng)
+        cfg = plume_configuration(tuple(resolution), inflow_center=centre, inflow_radius=radius)
+        self.model = Model(cfg)
+        self.ctx = self.model.allocate_context(ExecutionMode.forward, stream=stream)
+        self.state = self.model.allocate_state(self.ctx)
+        self.next = self.model.allocate_state(self.ctx)
+        self.control = self.model.allocate_control(self.ctx)
+        self.params = self.model.allocate_parameters(self.ctx)
+        self.cache = self.model.allocate_step_cache(self.ctx)
+        fill_parameters(self.params, ambient_temperature=0.0, density_buoyancy=-0.1, temperature_buoyancy=buoyancy)
+        self.steps = 0
+        self._reset_state()
+
+    def _reset_state(self):
+        seed = int(self.rng.integers(1 << 31))
+        g = torch.Generator(device="cpu").manual_seed(seed)
+        with torch.cuda.stream(self.ctx.stream):
+            for t in (self.state.density.values, self.state.temperature.values):
+                t.zero_()
+            for t in self.state.velocity.components():
+                t.copy_((torch.rand(t.shape, generator=g) * 0.02 - 0.01).to(t.device))
+        self.steps = 0
+
+    def restart(self):
+        from .model import fill_parameters
+        centre, radius, buoyancy = self.sampler.draw(self.rng)
+        self.ctx.set_inflow(0, center=centre, radius=radius)
+        fill_parameters(self.params, ambient_temperature=0.0, density_buoyancy=-0.1, temperature_buoyancy=buoyancy)
+        self._reset_state()
+
+    def step(self):
+        self.model.forward_step(self.state, self.control, self.params, self.next, self.cache, self.ctx)
+        self.state, self.next = self.next, self.state
+        self.steps += 1
+        return self.ctx.pressure_fields()
+
+
+def train_on_plumes(network: WarmStartNetwork, pairs: int = 20000, batch: int = 8, learning_rate: float = 1e-3,
+                    buffer_size: int = 256, episode_steps: int = 200, warmup_pairs: int = 64, seed: int = 0,
+                    log: Optional[Callable[[dict], None]] = None, log_every: int = 50) -> List[dict]:
+    """Trains ``network`` on ``pairs`` (rhs, pressure) pairs generated by the
+    plain PCG solver on its own grid: ``batch`` plumes run side by side, each
+    step adds their pairs to a replay buffer of ``buffer_size`` pairs in device
+    memory, and one Adam step runs on ``batch`` pairs drawn from the buffer.
+    A plume restarts with new random parameters after ``episode_steps``
+    steps.  Returns the logged records."""
+    if network.max_batch < batch:
+        raise ValueError(f"the network was created for batches of at most {network.max_batch}")
+    rng = np.random.default_rng(seed)
+    sampler = PlumeSampler()
+    stream = network.stream
+    n = network.cells
+    dev = torch.device("cuda")
+    plumes = [_Plume(network.shape, rng, sampler, stream) for _ in range(batch)]
+    # stagger the episodes so the buffer mixes early and developed plumes
+    for i, p in enumerate(plumes):
+        p.steps = -(i * episode_steps // batch)
+    buf_rhs = torch.empty(buffer_size, n, dtype=torch.float32, device=dev)
+    buf_p = torch.empty(buffer_size, n, dtype=torch.float32, device=dev)
+    filled, head, generated = 0, 0, 0
+    records: List[dict] = []
+    loss = torch.zeros(1, dtype=torch.float64, device=dev)
+    t0 = time.perf_counter()
+    it = 0
+    with torch.cuda.stream(stream):
+        while generated < pairs:
+            for p in plumes:
+                if p.steps >= episode_steps:
+                    p.restart()
+                pressure, rhs = p.step()
+                if p.steps <= 0:
+                    continue
+                buf_rhs[head].copy_(rhs)
+                buf_p[head].copy_(pressure)
+                head = (head + 1) % buffer_size
+                filled = min(filled + 1, buffer_size)
+                generated += 1
+            if filled < min(warmup_pairs, buffer_size):
+                continue
+            idx = torch.from_numpy(rng.integers(0, filled, size=batch)).to(dev)
+            b_rhs = buf_rhs.index_select(0, idx)
+            b_p = buf_p.index_select(0, idx)
+            network.train_step(b_rhs, b_p, learning_rate, loss)
+            it += 1
+            if log_every and it % log_every == 0:
+                rec = {"iteration": it, "pairs": generated, "loss": float(loss.item()), "seconds": time.perf_counter() - t0}
+                records.append(rec)
+                if log:
+                    log(rec)
+    network.check()
+    return records
+
+
+def solve_iterations(model, ctx, rhs: torch.Tensor, guess: Optional[torch.Tensor], scale: bool = True) -> dict:
+    """PCG statistics of one pressure solve of ``rhs`` on ``model``'s grid from
+    ``guess`` (None: zero), through xs_pressure_solve."""
+    lib = N.lib()
+    g = ctx.native.grid
+    solve = N.XsPressureSolve(N.XS_SOLVER_JACOBI_PCG, int(model.configuration.pressure_max_iterations),
+                              float(model.configuration.pressure_tolerance), None if guess is None else guess.data_ptr(),
+                              1 if scale else 0)
+    n = rhs.numel()
+    ws = torch.empty(lib.xs_projection_workspace_bytes(g), dtype=torch.uint8, device=rhs.device)
+    p = torch.empty(n, dtype=torch.float32, device=rhs.device)
+    N.check("xs_pressure_solve", lib.xs_pressure_solve(ctx.stream_handle, g, C.byref(solve), ctx.native.pressure_anchor,
+                                                       ctx.native.cell_mask, ctx.native.pressure_boundary, rhs.data_ptr(), p.data_ptr(),
+                                                       ws.data_ptr()))
+    st = N.XsSolveStats()
+    N.check("xs_read_solve_stats", lib.xs_read_solve_stats(ctx.stream_handle, C.c_void_p(ws.data_ptr()), C.byref(st)))
+    return st.as_dict()

@@ -11,8 +11,9 @@
  *      jvp_step and vjp_step (solvers/smoke/model.cpp:341-389) over a caller
  *      owned workspace, plus domain construction (model.cpp:32-183).
  *
- * Every function returns an XsStatus and never allocates device memory: the
- * caller owns every buffer, sized with the *_workspace_bytes queries.  All
+ * Every function returns an XsStatus and, except xs_warm_start_create, never
+ * allocates device memory: the caller owns every buffer, sized with the
+ * *_workspace_bytes queries.  All
  * work is enqueued on the given stream; nothing synchronises unless stated.
  * Pointers to cell masks may be NULL, meaning "no colliders" (every cell is
  * fluid); kernels then take the mask-free path.
@@ -97,7 +98,12 @@ typedef struct XsPressureSolve {
     uint32_t max_iterations;  /* PCG cap, or the RBGS sweep count */
     double tolerance;         /* ||b - A p||_2 <= tolerance * ||b||_2, FP64 */
     const float* initial_guess; /* PCG warm start (device, N cells) or NULL */
+    uint32_t scale_guess;     /* 1: start from alpha * guess with the energy-optimal
+                                 alpha = (g.b) / (g.A g); 0: from the guess as given */
 } XsPressureSolve;
+
+/* Opaque handle of the learned warm-start network (no reference counterpart). */
+typedef struct XsWarmStartNet XsWarmStartNet;
 
 /* Written by a pressure solve into device memory (inside the workspace) and
  * read back with xs_read_solve_stats. */
@@ -109,6 +115,7 @@ typedef struct XsSolveStats {
     double rhs_norm;              /* ||b||_2 */
     double initial_residual;      /* ||b - A p0||_2 / ||b||_2 of the accepted start */
     double final_residual;        /* ||b - A p||_2 / ||b||_2, p in FP64 */
+    double guess_scale;           /* alpha applied to the guess (1 if unscaled, 0 if none) */
 } XsSolveStats;
 
 /* ------------------------------------------------------------------------ */
@@ -289,6 +296,11 @@ typedef struct XsSmokeModel {
      * recorded on the step's stream around each pressure solve; NULL: none */
     cudaEvent_t solve_begin;
     cudaEvent_t solve_end;
+    /* learned warm start of the forward pressure solve (NULL: zero guess).
+     * The network's grid times its factor must equal `grid`; the guess is
+     * energy-scaled and PCG falls back to zero when it does not help.  Not
+     * used by the JVP and VJP solves. */
+    XsWarmStartNet* warm_start;
 } XsSmokeModel;
 
 /* State / Control / Parameters (data.ixx:117-134) */
@@ -339,6 +351,11 @@ XsStatus xs_smoke_reduce_metrics(cudaStream_t stream, const XsSmokeModel* model,
 XsStatus xs_smoke_read_solve_stats(cudaStream_t stream, const XsSmokeModel* model, const void* workspace, uint32_t mode,
                                    XsSolveStats* forward_stats, XsSolveStats* adjoint_stats);
 
+/* Device pointers, inside the workspace, of the pressure (FP32 copy of the
+ * solution) and of the right-hand side of the last forward pressure solve:
+ * the (divergence, pressure) pairs the warm-start network trains on. */
+XsStatus xs_smoke_pressure_fields(const XsSmokeModel* model, void* workspace, float** pressure, float** rhs);
+
 /* ------------------------------------------------------------------------ */
 /* learned pressure warm start (no reference counterpart)                    */
 /* ------------------------------------------------------------------------ */
@@ -364,6 +381,43 @@ XsStatus xs_conv3d_weight_grad_bf16(cudaStream_t stream, uint32_t batch, uint32_
                                     uint32_t accumulate, int* error_flag);
 size_t xs_conv3d_weight_grad_scratch_floats(uint32_t batch, uint32_t nx, uint32_t ny, uint32_t nz, uint32_t in_channels,
                                             uint32_t out_channels);
+
+/* The warm-start network: a 4-level U-Net (16/32/64/64 channels, 3x3x3
+ * convolutions on tcgen05, BF16 activations, FP32 accumulation, FP32 master
+ * weights and Adam state) mapping the right-hand side of the pressure system
+ * on its grid (nx x ny x nz cells, each a multiple of 8, every level a valid
+ * xs_conv3d_bf16 shape) to a pressure guess.  `factor` is the ratio of the
+ * fluid grid to the network grid used by xs_warm_start_guess and by a model
+ * that carries the network (1, 2, 3 or 4).  The handle owns its device
+ * memory (one allocation at creation). */
+XsStatus xs_warm_start_create(XsWarmStartNet** net, uint32_t max_batch, uint32_t nx, uint32_t ny, uint32_t nz, uint32_t factor);
+XsStatus xs_warm_start_destroy(XsWarmStartNet* net);
+/* Number of FP32 parameters (layer by layer, each [27][out][in]). */
+size_t xs_warm_start_parameter_count(void);
+/* He-normal initialisation from a seed; resets the Adam state.  Synchronises. */
+XsStatus xs_warm_start_initialize(XsWarmStartNet* net, cudaStream_t stream, uint64_t seed);
+/* Host copies of the FP32 parameters.  set resets the Adam state.  Both synchronise. */
+XsStatus xs_warm_start_set_parameters(XsWarmStartNet* net, cudaStream_t stream, const float* parameters);
+XsStatus xs_warm_start_get_parameters(XsWarmStartNet* net, cudaStream_t stream, float* parameters);
+/* guess[b] = network(rhs[b]) on the network grid, in units of the predicted
+ * pressure's RMS; rhs and guess are [batch][cells] FP32 (device). */
+XsStatus xs_warm_start_predict(XsWarmStartNet* net, cudaStream_t stream, uint32_t batch, const float* rhs, float* guess);
+/* Loss mean_{b,v} (out_b - p_b / rms(p_b))^2 into *loss (device double, may
+ * be NULL) and its gradient with respect to the parameters into gradient
+ * (device, parameter_count floats, may be NULL; the network keeps its own copy). */
+XsStatus xs_warm_start_gradient(XsWarmStartNet* net, cudaStream_t stream, uint32_t batch, const float* rhs, const float* pressure,
+                                float* gradient, double* loss);
+/* One Adam update from the last gradient. */
+XsStatus xs_warm_start_adam_step(XsWarmStartNet* net, cudaStream_t stream, float learning_rate, float beta1, float beta2, float epsilon);
+/* xs_warm_start_gradient followed by Adam (beta 0.9 / 0.999, epsilon 1e-8). */
+XsStatus xs_warm_start_train_step(XsWarmStartNet* net, cudaStream_t stream, uint32_t batch, const float* rhs, const float* pressure,
+                                  float learning_rate, double* loss);
+/* Guess on a fluid grid of factor x the network grid: restriction (sum of
+ * the factor^3 children), network, trilinear prolongation to the fine cell
+ * centres.  guess: cells FP32 (device). */
+XsStatus xs_warm_start_guess(XsWarmStartNet* net, cudaStream_t stream, XsGrid grid, const float* rhs, float* guess);
+/* Synchronises; XS_TIMEOUT if a bounded wait inside a network kernel expired. */
+XsStatus xs_warm_start_status(XsWarmStartNet* net, cudaStream_t stream);
 
 /* Number of kernel launches the library has issued since load (for launch
  * accounting). */

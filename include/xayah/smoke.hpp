@@ -183,6 +183,10 @@ public:
     }
     // Warm start (N device floats) for the following PCG solves; nullptr: zero.
     void set_warm_start(const float* guess) { native_.pressure.initial_guess = guess; }
+    // Learned warm start of the forward pressure solves (a network whose grid
+    // times its factor is this model's grid); nullptr: none.  The guess is
+    // energy-scaled and PCG falls back to zero when it does not help.
+    void set_learned_warm_start(XsWarmStartNet* net) { native_.warm_start = net; }
 
 private:
     ExecutionMode mode_{ExecutionMode::forward};

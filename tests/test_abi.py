@@ -32,14 +32,32 @@ def test_python_signatures_cover_the_header():
     assert declared_functions() <= set(_native.SIGNATURES), set(declared_functions()) - set(_native.SIGNATURES)
 
 
-def test_struct_layouts_match_header():
-    # sizes on x86-64: pointers 8 bytes, doubles 8-aligned
-    assert ctypes.sizeof(_native.XsGrid) == 20
-    assert ctypes.sizeof(_native.XsScalarBoundary) == 48
-    assert ctypes.sizeof(_native.XsVelocityBoundary) == 96
-    assert ctypes.sizeof(_native.XsPressureSolve) == 24
-    assert ctypes.sizeof(_native.XsSolveStats) == 40
-    assert ctypes.sizeof(_native.XsInflow) == 24
+STRUCTS = ["XsGrid", "XsScalarBoundary", "XsVelocityBoundary", "XsPressureSolve", "XsSolveStats", "XsInflow", "XsCollider",
+           "XsSmokeModel", "XsState", "XsControl", "XsParameters", "XsStepCache"]
+
+
+def test_struct_layouts_match_header(tmp_path):
+    """sizeof and every field offset of the ctypes mirrors equal what the C
+    compiler makes of include/diff_smoke.h."""
+    import shutil
+    import subprocess
+    cc = shutil.which("gcc") or "/usr/bin/gcc"
+    lines = ["#include <stdio.h>", "#include <stddef.h>", '#include "diff_smoke.h"', "int main(void) {"]
+    for name in STRUCTS:
+        lines.append(f'printf("{name} %zu\\n", sizeof({name}));')
+        for field, _ in getattr(_native, name)._fields_:
+            lines.append(f'printf("{name}.{field} %zu\\n", offsetof({name}, {field}));')
+    lines.append("return 0; }")
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines))
+    exe = tmp_path / "layout"
+    subprocess.run([cc, "-I", os.path.join(ROOT, "include"), "-I", "/usr/local/cuda/include", str(src), "-o", str(exe)], check=True)
+    want = dict(line.split() for line in subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.splitlines())
+    for name in STRUCTS:
+        cls = getattr(_native, name)
+        assert ctypes.sizeof(cls) == int(want[name]), name
+        for field, _ in cls._fields_:
+            assert getattr(cls, field).offset == int(want[f"{name}.{field}"]), (name, field)
 
 
 def test_status_strings_and_launch_counter_without_gpu():

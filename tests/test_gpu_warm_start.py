@@ -1,0 +1,190 @@
+"""Learned pressure warm start on the GPU: the native network's forward pass,
+loss and parameter gradient against the CPU reference network (PyTorch FP32
+autograd with the GPU's BF16 storage points), restriction / prolongation,
+Adam training, the energy-scaled PCG start with its zero-guess fallback, and
+the network inside a model step."""
+import numpy as np
+import pytest
+
+from common import ROOT  # noqa: F401  (puts the repository on sys.path)
+
+pytestmark = pytest.mark.gpu
+
+SHAPE = (128, 64, 16)  # smallest grid whose coarsest level still tiles by 128 voxels
+
+
+def rel(a, b):
+    a, b = np.asarray(a, np.float64), np.asarray(b, np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-30))
+
+
+def smooth_field(rng, shape, batch):
+    """Random fields with large-scale structure (a sum of a few Gaussians plus noise)."""
+    nx, ny, nz = shape
+    z, y, x = np.meshgrid(np.linspace(0, 1, nz), np.linspace(0, 1, ny), np.linspace(0, 1, nx), indexing="ij")
+    out = np.zeros((batch, nz, ny, nx), np.float32)
+    for b in range(batch):
+        for _ in range(4):
+            c = rng.uniform(0.2, 0.8, 3)
+            s = rng.uniform(0.05, 0.2)
+            out[b] += rng.normal() * np.exp(-((x - c[0]) ** 2 + (y - c[1]) ** 2 + (z - c[2]) ** 2) / (2 * s * s))
+        out[b] += 0.05 * rng.normal(size=(nz, ny, nx))
+    return out
+
+
+@pytest.fixture(scope="module")
+def net_and_data(cuda):
+    import torch
+    from diff_solver_b200.warm_start import WarmStartNetwork
+    rng = np.random.default_rng(3)
+    rhs = smooth_field(rng, SHAPE, 2)
+    p = smooth_field(rng, SHAPE, 2)
+    net = WarmStartNetwork(SHAPE, max_batch=2, factor=2, seed=11)
+    return net, rhs, p, torch.from_numpy(rhs).cuda().reshape(-1), torch.from_numpy(p).cuda().reshape(-1)
+
+
+def test_parameter_layout_matches_reference(net_and_data):
+    from oracle import unet_reference as R
+    net = net_and_data[0]
+    assert net.parameter_count() == R.parameter_count()
+    params = net.parameters()
+    w = R.split_parameters(params)
+    # initialisation: unused input channels of the first layer and unused
+    # output channels of the last one start (and stay) at zero
+    assert np.all(w[0][:, :, 2:] == 0) and np.all(w[11][:, 1:, :] == 0)
+    assert all(np.std(x) > 0 for x in w)
+
+
+def test_forward_matches_reference(net_and_data):
+    import torch
+    from oracle import unet_reference as R
+    net, rhs, _, rhs_d, _ = net_and_data
+    got = net.predict(rhs_d).cpu().numpy().reshape(rhs.shape)
+    torch.cuda.synchronize()
+    net.check()
+    want = R.predict(net.parameters(), rhs)
+    assert rel(got, want) < 2e-2
+
+
+def test_loss_and_gradient_match_reference(net_and_data):
+    from oracle import unet_reference as R
+    net, rhs, p, rhs_d, p_d = net_and_data
+    loss, grad = net.gradient(rhs_d, p_d)
+    net.check()
+    want_loss, want_grad = R.loss_and_gradient(net.parameters(), rhs, p)
+    assert abs(float(loss.item()) - want_loss) / want_loss < 1e-2
+    got = grad.cpu().numpy()
+    assert rel(got, want_grad) < 3e-2
+    off = 0
+    for i, (ci, co, _) in enumerate(R.LAYERS):
+        n = 27 * ci * co
+        g, w = got[off:off + n], want_grad[off:off + n]
+        if i == 0:  # only input channels 0 and 1 carry data
+            g, w = g.reshape(27, co, ci)[:, :, :2], w.reshape(27, co, ci)[:, :, :2]
+        if i == len(R.LAYERS) - 1:  # only output channel 0 is in the loss
+            g, w = g.reshape(27, co, ci)[:, :1], w.reshape(27, co, ci)[:, :1]
+        assert rel(g, w) < 5e-2, (i, rel(g, w))
+        off += n
+
+
+def test_guess_restricts_and_prolongs(net_and_data):
+    import torch
+    from diff_solver_b200 import _native as N
+    from oracle import unet_reference as R
+    net = net_and_data[0]
+    rng = np.random.default_rng(5)
+    fine_shape = tuple(2 * s for s in SHAPE)
+    fine = smooth_field(rng, fine_shape, 1)[0]
+    grid = N.XsGrid(*fine_shape, 1.0 / fine_shape[0], 0.5 / fine_shape[0])
+    got = net.guess(grid, torch.from_numpy(fine).cuda().reshape(-1)).cpu().numpy().reshape(fine.shape)
+    coarse = R.restrict(fine.astype(np.float64), 2).astype(np.float32)
+    want = R.prolong(R.predict(net.parameters(), coarse[None])[0], 2)
+    assert rel(got, want) < 2e-2
+
+
+def test_adam_reduces_the_loss(cuda):
+    import torch
+    from diff_solver_b200.warm_start import WarmStartNetwork
+    rng = np.random.default_rng(9)
+    rhs = torch.from_numpy(smooth_field(rng, SHAPE, 2)).cuda().reshape(-1)
+    p = torch.from_numpy(smooth_field(rng, SHAPE, 2)).cuda().reshape(-1)
+    net = WarmStartNetwork(SHAPE, max_batch=2, seed=1)
+    losses = [float(net.train_step(rhs, p, 1e-3).item()) for _ in range(40)]
+    net.check()
+    assert all(np.isfinite(losses))
+    assert losses[-1] < 0.6 * losses[0], losses[::8]
+
+
+def _plume_problem(res=(32, 32, 32), steps=12):
+    """A developed plume's pressure problem: the model, its context and the
+    right-hand side of its last solve."""
+    import torch
+    from diff_solver_b200.data import plume_configuration
+    from diff_solver_b200.model import ExecutionMode, Model, fill_parameters
+    cfg = plume_configuration(res)
+    m = Model(cfg)
+    ctx = m.allocate_context(ExecutionMode.forward)
+    s, n = m.allocate_state(ctx), m.allocate_state(ctx)
+    c, k = m.allocate_control(ctx), m.allocate_step_cache(ctx)
+    q = fill_parameters(m.allocate_parameters(ctx), 0.0, -0.1, 0.5)
+    g = torch.Generator().manual_seed(0)
+    for t in s.velocity.components():
+        t.copy_((torch.rand(t.shape, generator=g) * 0.02 - 0.01).cuda())
+    for _ in range(steps):
+        m.forward_step(s, c, q, n, k, ctx)
+        s, n = n, s
+    p, b = ctx.pressure_fields()
+    return m, ctx, p.clone(), b.clone()
+
+
+def test_energy_scaled_guess_and_fallback(cuda):
+    import torch
+    from diff_solver_b200.warm_start import solve_iterations
+    m, ctx, p, b = _plume_problem()
+    plain = solve_iterations(m, ctx, b, None)
+    assert plain["status"] == 0 and plain["iterations"] > 10
+    # a multiple of the solution: alpha undoes the factor, nothing left to do
+    st = solve_iterations(m, ctx, b, 2.5 * p)
+    assert st["warm_start_used"] == 1 and abs(st["guess_scale"] - 0.4) < 1e-3
+    assert st["iterations"] <= 0.25 * plain["iterations"] and st["final_residual"] <= 1e-6
+    # unscaled, the same guess is worse than zero and is dropped
+    st = solve_iterations(m, ctx, b, 2.5 * p, scale=False)
+    assert st["warm_start_used"] == 0 and st["guess_scale"] == 0.0 and st["final_residual"] <= 1e-6
+    # noise: scaled towards zero, never worse than the zero guess in the A-norm
+    noise = torch.randn(b.numel(), device=b.device, generator=torch.Generator(device=b.device).manual_seed(2))
+    st = solve_iterations(m, ctx, b, noise)
+    assert st["status"] == 0 and st["final_residual"] <= 1e-6 and abs(st["guess_scale"]) < 0.1
+
+
+def test_learned_warm_start_inside_a_model_step(cuda):
+    """A model carrying the network solves to the same tolerance and gives the
+    same step as the plain solver (both within the 1e-6 residual)."""
+    import torch
+    from diff_solver_b200.data import plume_configuration
+    from diff_solver_b200.model import ExecutionMode, Model, fill_parameters
+    from diff_solver_b200.warm_start import WarmStartNetwork
+    res = (128, 64, 32)
+    cfg = plume_configuration(res)
+    m = Model(cfg)
+    out = {}
+    net = WarmStartNetwork(res, factor=1, seed=4)
+    for name in ("plain", "learned"):
+        ctx = m.allocate_context(ExecutionMode.forward)
+        if name == "learned":
+            ctx.set_learned_warm_start(net)
+        s, n = m.allocate_state(ctx), m.allocate_state(ctx)
+        c, k = m.allocate_control(ctx), m.allocate_step_cache(ctx)
+        q = fill_parameters(m.allocate_parameters(ctx), 0.0, -0.1, 0.5)
+        g = torch.Generator().manual_seed(0)
+        for t in s.velocity.components():
+            t.copy_((torch.rand(t.shape, generator=g) * 0.02 - 0.01).cuda())
+        stats = []
+        for _ in range(6):
+            m.forward_step(s, c, q, n, k, ctx)
+            s, n = n, s
+            stats.append(ctx.read_solve_stats())
+        out[name] = (torch.cat([t.reshape(-1) for t in s.velocity.components()]).cpu().numpy(), stats)
+    net.check()
+    for st in out["learned"][1]:
+        assert st["status"] == 0 and st["final_residual"] <= 1e-6
+    assert rel(out["learned"][0], out["plain"][0]) < 1e-4
