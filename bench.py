@@ -5,9 +5,19 @@ Metric: smoke steps per second on the 256^3 plume (dx = 1/256, dt = dx/2,
 inflow sphere r = 0.08 at (0.5, 0.1, 0.5) setting density = temperature = 1,
 buoyancy +0.5 T - 0.1 rho on v, no confinement, walls with a fixed normal
 velocity on the sides and bottom, open top), pressure by Jacobi-PCG to a
-1e-6 relative residual from a zero guess (plain) or from the learned warm
-start.  One step is Model.forward_step through the C ABI; the rollout starts
-from rest with seeded uniform velocity noise in +-0.01.
+1e-6 relative residual.  One step is Model.forward_step through the C ABI.
+
+The plume first spins up from rest (seeded uniform velocity noise in
++-0.01) for --spinup steps; every arm then starts from that state:
+
+  plain            zero start (the reference's zero-initialised solve)
+  history          Galerkin start from the last 5 forward solutions
+  learned          the warm-start network's guess alone, energy-scaled
+  learned+history  the ring and the network's correction together (headline)
+
+Each arm runs W warm-up steps (which also refill its ring) and K timed steps.
+``value`` is the headline arm's steps/s; every arm's steps/s and PCG
+iterations are in ``arms``.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl product|reference]
 
@@ -33,13 +43,16 @@ sys.path.insert(0, ROOT)
 METRIC = "256^3 smoke steps/s: learned-warm-start vs plain PCG at rel. residual 1e-6"
 UNIT = "steps/s"
 GRID = 256
+HISTORY = 5
+WEIGHTS = os.path.join(ROOT, "diff_solver_b200", "weights", "warm_start_128.npz")
 
 
-def workload_configuration(n=GRID):
+def workload_configuration(n=GRID, history=0):
     from diff_solver_b200.data import plume_configuration
     cfg = plume_configuration((n, n, n), inflow_center=(0.5, 0.1, 0.5), inflow_radius=0.08)
     cfg.pressure_tolerance = 1e-6
     cfg.pressure_max_iterations = 20000
+    cfg.warm_start_history = history
     return cfg
 
 
@@ -175,123 +188,175 @@ def cpu_sample(n=GRID, sample_iterations=8, gpu_iterations=None):
 
 
 # --------------------------------------------------------------------- product
-def product_arm(args, world, rank, local):
+class Rollout:
+    """One execution context of the workload with its own state buffers."""
+
+    def __init__(self, grid, history, network):
+        from diff_solver_b200.model import ExecutionMode, Model, fill_parameters
+        self.model = Model(workload_configuration(grid, history))
+        self.ctx = self.model.allocate_context(ExecutionMode.forward)
+        if network is not None:
+            self.ctx.set_learned_warm_start(network)
+        m = self.model
+        self.cur, self.other = m.allocate_state(self.ctx), m.allocate_state(self.ctx)
+        self.control = m.allocate_control(self.ctx)
+        self.params = fill_parameters(m.allocate_parameters(self.ctx), **PARAMS)
+        self.cache = m.allocate_step_cache(self.ctx)
+
+    def load(self, state):
+        from diff_solver_b200.model import tensors_of
+        for d, s in zip(tensors_of(self.cur), tensors_of(state)):
+            d.copy_(s)
+        self.ctx.reset_warm_start()
+
+    def step(self):
+        self.model.forward_step(self.cur, self.control, self.params, self.other, self.cache, self.ctx)
+        self.cur, self.other = self.other, self.cur
+
+
+def timed_arm(args, world, ro, initial, e2e=False):
+    """W warm-up and K timed steps of one arm from `initial`; per-step solve
+    windows (warm start + PCG) timed by events the step records."""
     import torch
 
     from diff_solver_b200 import _native as N
-    from diff_solver_b200.model import ExecutionMode, Model, fill_parameters
-
-    torch.cuda.set_device(local)
     L = N.lib()
-    cfg = workload_configuration(args.grid)
-    model = Model(cfg)
-    ctx = model.allocate_context(ExecutionMode.forward)
-    stream = ctx.stream
-    n = model.cell_count
-    gen = torch.Generator(device="cuda").manual_seed(0)
-    state = model.allocate_state(ctx)
-    for t in (state.velocity.x, state.velocity.y, state.velocity.z):
-        t.uniform_(-0.01, 0.01, generator=gen)
-    nxt = model.allocate_state(ctx)
-    control = model.allocate_control(ctx)
-    params = fill_parameters(model.allocate_parameters(ctx), **PARAMS)
-    cache = model.allocate_step_cache(ctx)
-    stats_off = L.xs_solve_stats_offset()
-    stats_dev = ctx.workspace[stats_off:stats_off + C.sizeof(N.XsSolveStats)]
-
-    def step(s, o):
-        model.forward_step(s, control, params, o, cache, ctx)
-
-    # warm-up rollout
-    cur, other = state, nxt
-    for _ in range(args.warmup):
-        step(cur, other)
-        cur, other = other, cur
+    ro.load(initial)
+    stream = ro.ctx.stream
+    with torch.cuda.stream(stream):
+        for _ in range(args.warmup):
+            ro.step()
     torch.cuda.synchronize()
-
-    # timed region: K steps, solve kernel timed per step with events
     k_steps = args.steps
+    stats_off = L.xs_solve_stats_offset()
+    stats_dev = ro.ctx.workspace[stats_off:stats_off + C.sizeof(N.XsSolveStats)]
     stats_host = torch.zeros((k_steps, C.sizeof(N.XsSolveStats)), dtype=torch.uint8).pin_memory()
-    solve_events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(k_steps)]
-    for a, b in solve_events:  # create the handles
+    events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(k_steps)]
+    for a, b in events:
         a.record(stream)
         b.record(stream)
-    sampler = ClockSampler(local)
     barrier(world)
     torch.cuda.synchronize()
-    sampler.start()
     launches0 = L.xs_launch_count()
     start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     start.record(stream)
     with torch.cuda.stream(stream):
         for i in range(k_steps):
-            ctx.native.solve_begin = solve_events[i][0].cuda_event
-            ctx.native.solve_end = solve_events[i][1].cuda_event
-            step(cur, other)
+            ro.ctx.native.solve_begin = events[i][0].cuda_event
+            ro.ctx.native.solve_end = events[i][1].cuda_event
+            ro.step()
             stats_host[i].copy_(stats_dev, non_blocking=True)
-            cur, other = other, cur
     end.record(stream)
     torch.cuda.synchronize()
     launches = L.xs_launch_count() - launches0
     barrier(world)
-    clocks = sampler.stop()
-    elapsed_ms = start.elapsed_time(end)
-    elapsed_ms = max_over_ranks(elapsed_ms, world)
+    ro.ctx.native.solve_begin = None
+    ro.ctx.native.solve_end = None
     per_step = [N.XsSolveStats.from_buffer_copy(bytes(stats_host[i].numpy())) for i in range(k_steps)]
-    iterations = [s.iterations for s in per_step]
-    refinements = [s.refinements for s in per_step]
-    residuals = [s.final_residual for s in per_step]
+    out = dict(elapsed_ms=max_over_ranks(start.elapsed_time(end), world), launches=launches,
+               iterations=[s.iterations for s in per_step], refinements=[s.refinements for s in per_step],
+               residuals=[s.final_residual for s in per_step], initial_residuals=[s.initial_residual for s in per_step],
+               solve_ms=[a.elapsed_time(b) for a, b in events])
+    if e2e:
+        out.update(end_to_end(args, world, ro))
+    return out
 
-    # the dominant kernel (persistent PCG), one launch per step, timed by the
-    # events the step recorded around it inside the timed region
-    kernel_ms = [a.elapsed_time(b) for a, b in solve_events]
-    ctx.native.solve_begin = None
-    ctx.native.solve_end = None
 
-    # end to end through the public API with host buffers: every step copies
-    # its control fields from pinned host memory and reads back the metrics
+def end_to_end(args, world, ro):
+    """K steps through the public API with host buffers: every step copies
+    its control fields from pinned host memory and reads back the example
+    metrics."""
+    import torch
+
+    from diff_solver_b200 import _native as N
+    L = N.lib()
+    n = ro.model.cell_count
+    c = ro.control
     host_ctl = [torch.zeros(n, dtype=torch.float32).pin_memory() for _ in range(5)]
-    dev_ctl = [control.density_source.values, control.temperature_source.values, control.external_acceleration.x.values,
-               control.external_acceleration.y.values, control.external_acceleration.z.values]
+    dev_ctl = [c.density_source.values, c.temperature_source.values, c.external_acceleration.x.values, c.external_acceleration.y.values,
+               c.external_acceleration.z.values]
     metrics_dev = torch.zeros(6, dtype=torch.float64, device="cuda")
-    metrics_host = torch.zeros((k_steps, 6), dtype=torch.float64).pin_memory()
+    metrics_host = torch.zeros((args.steps, 6), dtype=torch.float64).pin_memory()
+    stream = ro.ctx.stream
     barrier(world)
     torch.cuda.synchronize()
     e_start, e_end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e_start.record(stream)
     with torch.cuda.stream(stream):
-        for i in range(k_steps):
+        for i in range(args.steps):
             for h, d in zip(host_ctl, dev_ctl):
                 d.copy_(h, non_blocking=True)
-            model.forward_step(cur, control, params, other, cache, ctx)
-            N.check("metrics", L.xs_smoke_reduce_metrics(ctx.stream_handle, C.byref(ctx.native), other.density.values.data_ptr(),
-                                                         other.temperature.values.data_ptr(), N.vec(cache.advected_velocity.components()),
-                                                         N.vec(other.velocity.components()), metrics_dev.data_ptr()))
+            ro.model.forward_step(ro.cur, ro.control, ro.params, ro.other, ro.cache, ro.ctx)
+            N.check("metrics", L.xs_smoke_reduce_metrics(ro.ctx.stream_handle, C.byref(ro.ctx.native), ro.other.density.values.data_ptr(),
+                                                         ro.other.temperature.values.data_ptr(), N.vec(ro.cache.advected_velocity.components()),
+                                                         N.vec(ro.other.velocity.components()), metrics_dev.data_ptr()))
             metrics_host[i].copy_(metrics_dev, non_blocking=True)
-            cur, other = other, cur
+            ro.cur, ro.other = ro.other, ro.cur
     e_end.record(stream)
     torch.cuda.synchronize()
-    e2e_ms = max_over_ranks(e_start.elapsed_time(e_end), world)
-    m_last = metrics_host[-1].numpy()
-    return dict(model=model, elapsed_ms=elapsed_ms, iterations=iterations, refinements=refinements, residuals=residuals,
-                kernel_ms=kernel_ms, launches=launches, clocks=clocks, e2e_ms=e2e_ms,
-                h2d=5 * n * 4, d2h=6 * 8 + 0, metrics=m_last, n=n)
+    return dict(e2e_ms=max_over_ranks(e_start.elapsed_time(e_end), world), h2d=5 * n * 4, d2h=6 * 8, metrics=metrics_host[-1].numpy())
+
+
+def product_run(args, world, rank, local):
+    import torch
+    torch.cuda.set_device(local)
+    network = None
+    if args.grid % 2 == 0 and not args.no_learned:
+        from diff_solver_b200.warm_start import WarmStartNetwork
+        if not os.path.exists(WEIGHTS):
+            raise FileNotFoundError(f"{WEIGHTS} is missing: train it with python -m diff_solver_b200.train_warm_start")
+        network = WarmStartNetwork((args.grid // 2,) * 3, factor=2)
+        network.load(WEIGHTS)
+    # spin-up from rest with the fastest start; its final state opens every arm
+    spin = Rollout(args.grid, HISTORY, network)
+    gen = torch.Generator(device="cuda").manual_seed(0)
+    for t in spin.cur.velocity.components():
+        t.uniform_(-0.01, 0.01, generator=gen)
+    with torch.cuda.stream(spin.ctx.stream):
+        for _ in range(args.spinup):
+            spin.step()
+    torch.cuda.synchronize()
+    from diff_solver_b200.model import tensors_of
+    initial = spin.model.allocate_state(spin.ctx)
+    for d, s in zip(tensors_of(initial), tensors_of(spin.cur)):
+        d.copy_(s)
+    del spin
+    arms = [("plain", 0, None), ("history", HISTORY, None)]
+    if network is not None:
+        arms += [("learned", 0, network), ("learned+history", HISTORY, network)]
+    headline = arms[-1][0]
+    sampler = ClockSampler(local)
+    sampler.start()
+    results = {}
+    for name, history, net in arms:
+        ro = Rollout(args.grid, history, net)
+        results[name] = timed_arm(args, world, ro, initial, e2e=(name == headline))
+        del ro
+        torch.cuda.empty_cache()
+    clocks = sampler.stop()
+    if network is not None:
+        network.check()
+    return results, headline, clocks
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
     ap.add_argument("--steps", type=int, default=5)
-    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--spinup", type=int, default=40, help="steps from rest before the arms start")
     ap.add_argument("--impl", choices=["product", "reference"], default="product")
     ap.add_argument("--grid", type=int, default=GRID)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-learned", action="store_true", help="plain and history arms only")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
     world, rank, local = init_distributed()
-    config = {"workload": f"smoke plume {args.grid}^3, Jacobi-PCG to rel. residual 1e-6, zero guess",
-              "grid": [args.grid] * 3, "cells": args.grid ** 3, "dt": "0.5 dx", "steps_per_replica": args.steps,
+    n = args.grid ** 3
+    config = {"workload": f"smoke plume {args.grid}^3 after a {args.spinup}-step spin-up from rest, Jacobi-PCG to rel. residual 1e-6",
+              "grid": [args.grid] * 3, "cells": n, "dt": "0.5 dx", "steps_per_replica": args.steps, "spinup_steps": args.spinup,
+              "warm_start": f"Galerkin start over the last {HISTORY} solutions + U-Net correction (128^3 network, restriction x2)",
               "l2": "inputs larger than L2 (state 336 MB at 256^3)", "parallelism": f"replicas{world}"}
     if args.impl == "reference":
         if rank == 0:
@@ -303,30 +368,38 @@ def main():
                     "e2e": {"value": cpu["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
             print(json.dumps(line), flush=True)
         return
-    r = product_arm(args, world, rank, local)
+    results, headline, clocks = product_run(args, world, rank, local)
     if rank != 0:
         return
     steps_total = args.steps * world
-    value = steps_total / (r["elapsed_ms"] / 1e3)
+    arms = {}
+    for name, r in results.items():
+        arms[name] = {"steps_per_s": steps_total / (r["elapsed_ms"] / 1e3), "ms_per_step": r["elapsed_ms"] / args.steps,
+                      "pcg_iterations_per_step": r["iterations"], "mean_pcg_iterations": statistics.mean(r["iterations"]),
+                      "solve_ms_per_step": statistics.mean(r["solve_ms"]), "initial_residuals": r["initial_residuals"],
+                      "final_residuals": r["residuals"], "gpu_launches": r["launches"]}
+    h = results[headline]
+    value = arms[headline]["steps_per_s"]
+    # roofline of the dominant kernel (the persistent PCG), from the plain arm
+    # where the solve window holds that kernel alone
+    p = results["plain"]
     peak, peak_kind = measured_peaks()
-    kbytes_each = [pcg_algorithmic_bytes(r["n"], it, rf) for it, rf in zip(r["iterations"], r["refinements"])]
-    kbytes = statistics.mean(kbytes_each)
-    kms = statistics.mean(r["kernel_ms"])
-    achieved = sum(kbytes_each) / (sum(r["kernel_ms"]) / 1e3) / 1e9
+    kbytes_each = [pcg_algorithmic_bytes(n, it, rf) for it, rf in zip(p["iterations"], p["refinements"])]
+    achieved = sum(kbytes_each) / (sum(p["solve_ms"]) / 1e3) / 1e9
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
-            "ms_per_step": r["elapsed_ms"] / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+            "ms_per_step": h["elapsed_ms"] / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 (FP64 CG reductions and iterate)", "data": "synthetic", "config": config,
-            "method": "plain", "pcg_iterations_per_step": r["iterations"], "final_residuals": r["residuals"],
+            "method": headline, "speedup_vs_plain": value / arms["plain"]["steps_per_s"], "arms": arms,
             "roofline": {"bound": "hbm", "kernel": "pcg_kernel", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
-                         "algorithmic_bytes_per_launch": kbytes, "launch_ms": kms,
-                         "iterations_per_launch": statistics.mean(r["iterations"])},
-            "gpu_launches": r["launches"], "clocks": r["clocks"],
-            "e2e": {"value": steps_total / (r["e2e_ms"] / 1e3), "unit": UNIT, "h2d_bytes_per_step": r["h2d"],
-                    "d2h_bytes_per_step": r["d2h"]},
-            "example_metrics_last_step": [float(v) for v in r["metrics"]]}
+                         "algorithmic_bytes_per_launch": statistics.mean(kbytes_each), "launch_ms": statistics.mean(p["solve_ms"]),
+                         "iterations_per_launch": statistics.mean(p["iterations"]), "arm": "plain"},
+            "gpu_launches": h["launches"], "clocks": clocks,
+            "e2e": {"value": steps_total / (h["e2e_ms"] / 1e3), "unit": UNIT, "h2d_bytes_per_step": h["h2d"],
+                    "d2h_bytes_per_step": h["d2h"]},
+            "example_metrics_last_step": [float(v) for v in h["metrics"]]}
     if world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_sample(args.grid, gpu_iterations=int(statistics.mean(r["iterations"])))
+        cpu = cpu_sample(args.grid, gpu_iterations=int(arms["plain"]["mean_pcg_iterations"]))
         line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
     print(json.dumps(line), flush=True)
 

@@ -66,7 +66,7 @@ class XsSmokeModel(C.Structure):
                 ("vorticity_confinement_enabled", C.c_uint32), ("pressure_anchor", C.c_uint32), ("pressure", XsPressureSolve),
                 ("inflows", C.c_void_p), ("inflow_count", C.c_uint32), ("cell_mask", C.c_void_p), ("collider_velocity", XsVector),
                 ("collider_density", C.c_void_p), ("collider_temperature", C.c_void_p), ("solve_begin", C.c_void_p),
-                ("solve_end", C.c_void_p), ("warm_start", C.c_void_p)]
+                ("solve_end", C.c_void_p), ("warm_start", C.c_void_p), ("warm_start_history", C.c_uint32)]
 
 
 class XsState(C.Structure):
@@ -141,7 +141,9 @@ SIGNATURES = {
     "xs_smoke_reduce_metrics": (_S, [_V, C.POINTER(XsSmokeModel), _V, _V, XsVector, XsVector, _V]),
     "xs_smoke_read_solve_stats": (_S, [_V, C.POINTER(XsSmokeModel), _V, C.c_uint32, C.POINTER(XsSolveStats),
                                        C.POINTER(XsSolveStats)]),
-    "xs_smoke_pressure_fields": (_S, [C.POINTER(XsSmokeModel), _V, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
+    "xs_smoke_reset_warm_start": (_S, [_V, C.POINTER(XsSmokeModel), _V]),
+    "xs_smoke_warm_start_fields": (_S, [_V, C.POINTER(XsSmokeModel), _V, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
+    "xs_smoke_pressure_fields":(_S, [C.POINTER(XsSmokeModel), _V, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
     "xs_conv3d_bf16": (_S, [_V, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, _V, _V, _V, _V, C.c_uint32,
                             _V]),
     "xs_conv3d_weight_grad_bf16": (_S, [_V, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, _V, _V, _V, _V,
@@ -155,7 +157,8 @@ SIGNATURES = {
     "xs_warm_start_get_parameters": (_S, [_V, _V, _V]),
     "xs_warm_start_predict": (_S, [_V, _V, C.c_uint32, _V, _V]),
     "xs_warm_start_gradient": (_S, [_V, _V, C.c_uint32, _V, _V, _V, _V]),
-    "xs_warm_start_adam_step": (_S, [_V, _V, C.c_float, C.c_float, C.c_float, C.c_float]),
+    "xs_warm_start_set_loss": (_S, [_V, C.c_uint32, XsScalarBoundary]),
+    "xs_warm_start_adam_step":(_S, [_V, _V, C.c_float, C.c_float, C.c_float, C.c_float]),
     "xs_warm_start_train_step": (_S, [_V, _V, C.c_uint32, _V, _V, C.c_float, _V]),
     "xs_warm_start_guess": (_S, [_V, _V, _G, _V, _V]),
     "xs_warm_start_status": (_S, [_V, _V]),

@@ -71,6 +71,7 @@ XsStatus launch_advect_scalar_jvp(cudaStream_t st, const Grid& g, const uint32_t
 // projection forward with any solver kind (step.cu)
 XsStatus projection_forward(cudaStream_t st, const Grid& g, const XsPressureSolve& solve, uint32_t anchor, const uint32_t* mask,
                             const XsVector& u, const XsScalarBoundary& pb, float* pressure, float* rhs, const XsVector& out,
-                            void* workspace, cudaEvent_t begin = nullptr, cudaEvent_t end = nullptr, struct WarmStartNet* warm_start = nullptr);
+                            void* workspace, cudaEvent_t begin = nullptr, cudaEvent_t end = nullptr, struct WarmStartNet* warm_start = nullptr,
+                            const WarmHistory* history = nullptr);
 
 }  // namespace xs

@@ -64,4 +64,32 @@ XsStatus reverse_rbgs(cudaStream_t stream, const Grid& g, uint32_t sweeps, uint3
 
 XsStatus read_solve_stats(cudaStream_t stream, const void* workspace, const Grid& g, XsSolveStats* out);
 
+// Warm-start subspace: a ring of the last `history` forward solutions plus
+// at most one extra vector (kMaxBasis in all) spanning the Galerkin start.
+constexpr int kMaxBasis = 6;
+struct WarmHistory {
+    float* slots[kMaxBasis];
+    uint32_t history;   // ring slots (0: off)
+    uint32_t* meta;     // device: [0] valid slots, [1] next slot
+    float* start;       // the start vector of the last forward solve (N)
+    float* ring_start;  // the Galerkin start from the ring alone (N)
+    float* residual;    // b - A ring_start (N)
+    double* partials;
+    double* coef;
+};
+size_t warm_history_bytes(const Grid& g, uint32_t history);
+WarmHistory carve_warm_history(void* base, const Grid& g, uint32_t history);
+// out = the A-norm-optimal combination of the valid ring vectors (use_ring)
+// and the n_extra vectors in `extra`, for the right-hand side rhs (+ fixed
+// boundary values).  out must not be one of the combined vectors.
+XsStatus galerkin_combine(cudaStream_t st, const Grid& g, uint32_t anchor, const uint32_t* mask, const XsScalarBoundary& pb, const WarmHistory& h,
+                          bool use_ring, const float* const* extra, int n_extra, const float* rhs, float* out);
+// r = b + fixed boundary values - A x
+XsStatus start_residual(cudaStream_t st, const Grid& g, uint32_t anchor, const uint32_t* mask, const XsScalarBoundary& pb, const float* rhs,
+                        const float* x, float* r);
+// Stores a solution in the next ring slot.
+XsStatus history_push(cudaStream_t st, const Grid& g, const WarmHistory& h, const float* pressure);
+// Empties the ring.
+XsStatus history_reset(cudaStream_t st, const WarmHistory& h);
+
 }  // namespace xs

@@ -16,21 +16,42 @@ namespace xs {
 // the PCG kind the velocity is corrected from the FP64 iterate.
 XsStatus projection_forward(cudaStream_t st, const Grid& g, const XsPressureSolve& solve, uint32_t anchor, const uint32_t* mask,
                             const XsVector& u, const XsScalarBoundary& pb, float* pressure, float* rhs, const XsVector& out,
-                            void* workspace, cudaEvent_t begin, cudaEvent_t end, WarmStartNet* warm_start) {
+                            void* workspace, cudaEvent_t begin, cudaEvent_t end, WarmStartNet* warm_start, const WarmHistory* history) {
     XsStatus s = launch_pressure_rhs(st, g, anchor, mask, u, rhs);
     if (s != XS_OK) return s;
     PressureWorkspace w{};
     if (begin && cudaEventRecord(begin, st) != cudaSuccess) return XS_CUDA_ERROR;
     XsPressureSolve used = solve;
-    if (warm_start && solve.kind == XS_SOLVER_JACOBI_PCG) {
-        // learned guess (inside the timed solve): energy-scaled, with fallback to zero
-        float* guess = nullptr;
+    const bool pcg = solve.kind == XS_SOLVER_JACOBI_PCG;
+    const bool ring = pcg && history && history->history > 0;
+    // warm start (inside the timed solve); PCG falls back to zero whenever the
+    // start is worse than zero:
+    //  * ring of previous solutions: their Galerkin (A-norm-optimal)
+    //    combination x0; with a network, the network maps the residual
+    //    b - A x0 to a correction direction that joins the ring in a second
+    //    Galerkin combination;
+    //  * network alone: its guess for b, scaled by the energy-optimal factor.
+    float* guess = nullptr;
+    if (ring) {
+        const WarmHistory& h = *history;
+        if ((s = galerkin_combine(st, g, anchor, mask, pb, h, true, nullptr, 0, rhs, h.ring_start)) != XS_OK) return s;
+        used.initial_guess = h.ring_start;
+        if (warm_start) {
+            if ((s = start_residual(st, g, anchor, mask, pb, rhs, h.ring_start, h.residual)) != XS_OK) return s;
+            if ((s = warm_start_guess(warm_start, st, g, h.residual, &guess)) != XS_OK) return s;
+            const float* extra[1] = {guess};
+            if ((s = galerkin_combine(st, g, anchor, mask, pb, h, true, extra, 1, rhs, h.start)) != XS_OK) return s;
+            used.initial_guess = h.start;
+        }
+        used.scale_guess = 0u;
+    } else if (warm_start && pcg) {
         if ((s = warm_start_guess(warm_start, st, g, rhs, &guess)) != XS_OK) return s;
         used.initial_guess = guess;
         used.scale_guess = 1u;
     }
     s = solve_pressure(st, g, used, anchor, mask, pb, rhs, nullptr, pressure, nullptr, workspace, &w);
     if (s != XS_OK) return s;
+    if (ring && (s = history_push(st, g, *history, pressure)) != XS_OK) return s;
     if (end && cudaEventRecord(end, st) != cudaSuccess) return XS_CUDA_ERROR;
     if (solve.kind == XS_SOLVER_RED_BLACK_GAUSS_SEIDEL) return launch_project(st, g, mask, u, pressure, out);
     return launch_project64(st, g, mask, u, w.x64, out);
@@ -63,10 +84,11 @@ struct StepWorkspace {
     XsAdjointVector forced_a;
     double* pressure_a;
     double* rhs_a;
+    WarmHistory history;
     size_t bytes;
 };
 
-StepWorkspace carve_step(void* base, const Grid& g, uint32_t mode) {
+StepWorkspace carve_step(void* base, const Grid& g, uint32_t mode, uint32_t history) {
     StepWorkspace w{};
     char* p = static_cast<char*>(base);
     size_t off = 0;
@@ -83,6 +105,8 @@ StepWorkspace carve_step(void* base, const Grid& g, uint32_t mode) {
     w.solver = take(pressure_workspace_bytes(g));
     w.pressure = static_cast<float*>(take(4 * n));
     w.rhs = static_cast<float*>(take(4 * n));
+    // warm-start ring, in every mode at the same place
+    w.history = carve_warm_history(take(warm_history_bytes(g, history)), g, history);
     if (mode == XS_MODE_DIFFERENTIABLE) {
         w.sourced_rho_t = static_cast<float*>(take(4 * n));
         w.sourced_temp_t = static_cast<float*>(take(4 * n));
@@ -109,7 +133,8 @@ StepWorkspace carve_step(void* base, const Grid& g, uint32_t mode) {
 }
 
 bool valid_model(const XsSmokeModel* m) {
-    return m != nullptr && valid_grid(m->grid) && m->inflow_count <= XS_MAX_INFLOWS && (m->inflow_count == 0 || m->inflows != nullptr);
+    return m != nullptr && valid_grid(m->grid) && m->inflow_count <= XS_MAX_INFLOWS && (m->inflow_count == 0 || m->inflows != nullptr) &&
+           m->warm_start_history < static_cast<uint32_t>(kMaxBasis);
 }
 
 XsStatus zero(cudaStream_t st, void* p, size_t bytes) { return check_cuda(cudaMemsetAsync(p, 0, bytes, st)); }
@@ -212,7 +237,7 @@ XsStatus xs_projection_jvp(cudaStream_t stream, XsGrid grid, const XsPressureSol
 
 size_t xs_smoke_workspace_bytes(const XsSmokeModel* model, uint32_t mode) {
     if (!valid_model(model)) return 0;
-    return carve_step(nullptr, make_grid(model->grid), mode).bytes;
+    return carve_step(nullptr, make_grid(model->grid), mode, model->warm_start_history).bytes;
 }
 
 // model.cpp:341-349
@@ -226,7 +251,7 @@ XsStatus xs_smoke_forward_step(cudaStream_t stream, const XsSmokeModel* m, XsSta
         return XS_INVALID_ARGUMENT;
     if (m->vorticity_confinement_enabled && (!cache.vorticity || !parameters.vorticity_confinement)) return XS_INVALID_ARGUMENT;
     const Grid g = make_grid(m->grid);
-    const StepWorkspace w = carve_step(workspace, g, XS_MODE_FORWARD);
+    const StepWorkspace w = carve_step(workspace, g, XS_MODE_FORWARD, m->warm_start_history);
     const InflowSet inflows = make_inflows(m->inflows, m->inflow_count);
     XsStatus s;
     // sources of density and temperature, then buoyancy on the sourced fields
@@ -248,7 +273,7 @@ XsStatus xs_smoke_forward_step(cudaStream_t stream, const XsSmokeModel* m, XsSta
     // projection
     s = projection_forward(stream, g, m->pressure, m->pressure_anchor, m->cell_mask, cache.advected_velocity, m->pressure_boundary,
                            w.pressure, w.rhs, next_state.velocity, w.solver, m->solve_begin, m->solve_end,
-                           reinterpret_cast<WarmStartNet*>(m->warm_start));
+                           reinterpret_cast<WarmStartNet*>(m->warm_start), &w.history);
     if (s != XS_OK) return s;
     // scalar advection of the sourced fields through the projected velocity
     return launch_advect_scalar_pair(stream, g, m->cell_mask, m->collider_density, m->collider_temperature, cache.sourced_density,
@@ -267,7 +292,7 @@ XsStatus xs_smoke_jvp_step(cudaStream_t stream, const XsSmokeModel* m, XsState s
     if (m->vorticity_confinement_enabled && (!cache.vorticity || !parameters.vorticity_confinement || !pt.vorticity_confinement))
         return XS_INVALID_ARGUMENT;
     const Grid g = make_grid(m->grid);
-    const StepWorkspace w = carve_step(workspace, g, XS_MODE_DIFFERENTIABLE);
+    const StepWorkspace w = carve_step(workspace, g, XS_MODE_DIFFERENTIABLE, m->warm_start_history);
     const InflowSet inflows = make_inflows(m->inflows, m->inflow_count);
     XsStatus s;
     s = launch_source_jvp_pair(stream, g, m->cell_mask, st.density, st.temperature, ct.density_source, ct.temperature_source, inflows,
@@ -315,7 +340,7 @@ XsStatus xs_smoke_vjp_step(cudaStream_t stream, const XsSmokeModel* m, XsState s
     if (m->vorticity_confinement_enabled && (!cache.vorticity || !parameters.vorticity_confinement || !qa.vorticity_confinement))
         return XS_INVALID_ARGUMENT;
     const Grid g = make_grid(m->grid);
-    const StepWorkspace w = carve_step(workspace, g, XS_MODE_DIFFERENTIABLE);
+    const StepWorkspace w = carve_step(workspace, g, XS_MODE_DIFFERENTIABLE, m->warm_start_history);
     const InflowSet inflows = make_inflows(m->inflows, m->inflow_count);
     const uint64_t n = cell_count(g), f0 = face_count(g, 0), f1 = face_count(g, 1), f2 = face_count(g, 2);
     XsStatus s;
@@ -382,7 +407,7 @@ XsStatus xs_smoke_read_solve_stats(cudaStream_t stream, const XsSmokeModel* mode
                                    XsSolveStats* forward_stats, XsSolveStats* adjoint_stats) {
     (void)mode;
     if (!valid_model(model) || !workspace) return XS_INVALID_ARGUMENT;
-    const StepWorkspace w = carve_step(const_cast<void*>(workspace), make_grid(model->grid), XS_MODE_FORWARD);
+    const StepWorkspace w = carve_step(const_cast<void*>(workspace), make_grid(model->grid), XS_MODE_FORWARD, model->warm_start_history);
     XsSolveStats st{};
     const XsStatus s = xs_read_solve_stats(stream, w.solver, &st);
     if (forward_stats) *forward_stats = st;
@@ -390,9 +415,27 @@ XsStatus xs_smoke_read_solve_stats(cudaStream_t stream, const XsSmokeModel* mode
     return s;
 }
 
+XsStatus xs_smoke_warm_start_fields(cudaStream_t stream, const XsSmokeModel* model, void* workspace, float** ring_start, float** residual) {
+    if (!valid_model(model) || !workspace || model->warm_start_history == 0) return XS_INVALID_ARGUMENT;
+    const Grid g = make_grid(model->grid);
+    const StepWorkspace w = carve_step(workspace, g, XS_MODE_FORWARD, model->warm_start_history);
+    const XsStatus s = start_residual(stream, g, model->pressure_anchor, model->cell_mask, model->pressure_boundary, w.rhs, w.history.ring_start,
+                                      w.history.residual);
+    if (s != XS_OK) return s;
+    if (ring_start) *ring_start = w.history.ring_start;
+    if (residual) *residual = w.history.residual;
+    return XS_OK;
+}
+
+XsStatus xs_smoke_reset_warm_start(cudaStream_t stream, const XsSmokeModel* model, void* workspace) {
+    if (!valid_model(model) || !workspace) return XS_INVALID_ARGUMENT;
+    const StepWorkspace w = carve_step(workspace, make_grid(model->grid), XS_MODE_FORWARD, model->warm_start_history);
+    return history_reset(stream, w.history);
+}
+
 XsStatus xs_smoke_pressure_fields(const XsSmokeModel* model, void* workspace, float** pressure, float** rhs) {
     if (!valid_model(model) || !workspace) return XS_INVALID_ARGUMENT;
-    const StepWorkspace w = carve_step(workspace, make_grid(model->grid), XS_MODE_FORWARD);
+    const StepWorkspace w = carve_step(workspace, make_grid(model->grid), XS_MODE_FORWARD, model->warm_start_history);
     if (pressure) *pressure = w.pressure;
     if (rhs) *rhs = w.rhs;
     return XS_OK;

@@ -24,7 +24,12 @@
 // rescales the guess by the energy-optimal factor, so only the shape
 // matters); output channels 1..15 receive no gradient and stay unused.
 //
-// Training loss: mean over samples and voxels of (out_0 - p / rms(p))^2.
+// Training losses (xs_warm_start_set_loss):
+//   0: mean over samples and voxels of (out_0 - p / rms(p))^2;
+//   1: energy loss, mean over samples of 1 - (g.Ap)^2 / ((g.Ag)(p.Ap)) with
+//      g = out_0 and A the pressure operator of the training grid: the
+//      squared relative A-norm error of the energy-optimally scaled guess,
+//      which is what PCG started from that guess has left to remove.
 #include <cuda_bf16.h>
 
 #include <cmath>
@@ -274,6 +279,105 @@ __global__ void loss_final_kernel(const double* __restrict__ partial, uint32_t c
     if (threadIdx.x == 0) *loss = acc[0] / denom;
 }
 
+// ----------------------------------------------------- energy (A-norm) loss
+// The pressure operator on the network grid (no solids): diag counts the
+// in-domain or periodic neighbours plus the fixed-value boundary faces,
+// zero-gradient faces drop out; (A u)_c = diag u_c - sum of neighbours.
+template <class Load>
+__device__ __forceinline__ float apply_operator(const Load& u, int x, int y, int z, int X, int Y, int Z, const XsScalarBoundary& pb) {
+    const int c[3] = {x, y, z}, n[3] = {X, Y, Z};
+    float diag = 0.0f, acc = 0.0f;
+#pragma unroll
+    for (int d = 0; d < 3; ++d) {
+#pragma unroll
+        for (int side = 0; side < 2; ++side) {
+            int q[3] = {c[0], c[1], c[2]};
+            q[d] += side ? 1 : -1;
+            if (q[d] < 0 || q[d] >= n[d]) {
+                if (periodic(pb, d)) {
+                    q[d] = side ? 0 : n[d] - 1;
+                } else {
+                    if (pb.modes[2 * d + side] == 0u) diag += 1.0f;
+                    continue;
+                }
+            }
+            acc += u(q[0], q[1], q[2]);
+            diag += 1.0f;
+        }
+    }
+    return diag * u(x, y, z) - acc;
+}
+
+struct EnergyArgs {
+    const __nv_bfloat16* out;  // network output, channel 0 at stride 16
+    const float* p;            // target pressure (any scale)
+    int X, Y, Z;
+    XsScalarBoundary pb;
+    uint64_t per_sample;
+};
+
+// Per sample: S1 = g.At, S2 = g.Ag, S3 = t.At, as block partials.
+__global__ void energy_sums_kernel(EnergyArgs a, double* __restrict__ partial) {
+    __shared__ double red[4 * 32];
+    const uint64_t base = static_cast<uint64_t>(blockIdx.y) * a.per_sample;
+    auto G = [&](int x, int y, int z) { return __bfloat162float(a.out[(base + (static_cast<uint64_t>(z) * a.Y + y) * a.X + x) * 16]); };
+    auto T = [&](int x, int y, int z) { return a.p[base + (static_cast<uint64_t>(z) * a.Y + y) * a.X + x]; };
+    double s[3] = {0.0, 0.0, 0.0};
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < a.per_sample; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const int x = static_cast<int>(i % a.X), y = static_cast<int>((i / a.X) % a.Y), z = static_cast<int>(i / (static_cast<uint64_t>(a.X) * a.Y));
+        const double at = apply_operator(T, x, y, z, a.X, a.Y, a.Z, a.pb), ag = apply_operator(G, x, y, z, a.X, a.Y, a.Z, a.pb);
+        const double g = G(x, y, z), t = T(x, y, z);
+        s[0] += g * at;
+        s[1] += g * ag;
+        s[2] += t * at;
+    }
+    block_sum<3>(s, red);
+    if (threadIdx.x == 0)
+        for (int k = 0; k < 3; ++k) partial[(static_cast<uint64_t>(blockIdx.y) * gridDim.x + blockIdx.x) * 3 + k] = s[k];
+}
+
+// Per sample: alpha = S1/S2 (the energy-optimal scale of the guess), loss
+// 1 - S1^2/(S2 S3) (the squared relative A-norm error of alpha g), gradient
+// factor -2 alpha / (S3 batch).  coef[2b] = alpha, coef[2b+1] = factor.
+__global__ void energy_final_kernel(const double* __restrict__ partial, uint32_t blocks, uint32_t batch, double* __restrict__ coef, double* loss) {
+    __shared__ double lb[64];
+    const uint32_t b = threadIdx.x;
+    if (b < batch) {
+        double s[3] = {0.0, 0.0, 0.0};
+        for (uint32_t i = 0; i < blocks; ++i)
+            for (int k = 0; k < 3; ++k) s[k] += partial[(static_cast<uint64_t>(b) * blocks + i) * 3 + k];
+        const bool ok = s[1] > 0.0 && s[2] > 0.0;
+        const double alpha = ok ? s[0] / s[1] : 0.0;
+        coef[2 * b] = alpha;
+        coef[2 * b + 1] = ok ? -2.0 * alpha / (s[2] * batch) : 0.0;
+        lb[b] = ok ? 1.0 - s[0] * s[0] / (s[1] * s[2]) : 1.0;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        double acc = 0.0;
+        for (uint32_t i = 0; i < batch; ++i) acc += lb[i];
+        *loss = acc / batch;
+    }
+}
+
+// g_out[v] = {factor_b (A t - alpha_b A g)_v, 0, ..., 0}
+__global__ void energy_grad_kernel(EnergyArgs a, uint32_t batch, const double* __restrict__ coef, __nv_bfloat16* __restrict__ g_out) {
+    const uint64_t total = a.per_sample * batch;
+    for (uint64_t v = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; v < total; v += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const uint64_t b = v / a.per_sample, i = v % a.per_sample;
+        const uint64_t base = b * a.per_sample;
+        auto G = [&](int x, int y, int z) { return __bfloat162float(a.out[(base + (static_cast<uint64_t>(z) * a.Y + y) * a.X + x) * 16]); };
+        auto T = [&](int x, int y, int z) { return a.p[base + (static_cast<uint64_t>(z) * a.Y + y) * a.X + x]; };
+        const int x = static_cast<int>(i % a.X), y = static_cast<int>((i / a.X) % a.Y), z = static_cast<int>(i / (static_cast<uint64_t>(a.X) * a.Y));
+        const float at = apply_operator(T, x, y, z, a.X, a.Y, a.Z, a.pb), ag = apply_operator(G, x, y, z, a.X, a.Y, a.Z, a.pb);
+        const float d = static_cast<float>(coef[2 * b + 1] * (static_cast<double>(at) - coef[2 * b] * static_cast<double>(ag)));
+        float o[8] = {d, 0, 0, 0, 0, 0, 0, 0};
+        store8(g_out + v * 16, o);
+        const float z8[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+        store8(g_out + v * 16 + 8, z8);
+    }
+}
+
 struct LayerTable {
     uint32_t offset[kLayers + 1];
     uint16_t cin[kLayers], cout[kLayers];
@@ -394,8 +498,11 @@ struct WarmStartNet {
     int* error = nullptr;
     float* coarse_rhs = nullptr;  // restriction of a fine right-hand side (factor > 1)
     float* fine_guess = nullptr;  // prolonged guess on the fine grid
+    double* coef = nullptr;       // energy loss: per-sample alpha and gradient factor
     uint64_t adam_steps = 0;
     LayerTable table{};
+    uint32_t loss_kind = 0;       // 0: normalised L2, 1: energy (A-norm)
+    XsScalarBoundary loss_boundary{};
 };
 
 namespace {
@@ -577,10 +684,11 @@ XsStatus xs_warm_start_create(XsWarmStartNet** out, uint32_t max_batch, uint32_t
     for (int a = 0; a < A_COUNT; ++a) take(reinterpret_cast<void**>(&n->act[a]), voxels(n->level[kActLevel[a]]) * kActChannels[a] * 2);
     for (int g = 0; g < G_COUNT; ++g) take(reinterpret_cast<void**>(&n->gbuf[g]), voxels(n->level[kGradLevel[g]]) * kGradChannels[g] * 2);
     take(reinterpret_cast<void**>(&n->wgrad_scratch), scratch * 4);
-    take(reinterpret_cast<void**>(&n->partial), sizeof(double) * kStatBlocks * max_batch);
+    take(reinterpret_cast<void**>(&n->partial), sizeof(double) * 3 * kStatBlocks * max_batch);
     take(reinterpret_cast<void**>(&n->inv_rms_in), 4 * max_batch);
     take(reinterpret_cast<void**>(&n->inv_rms_p), 4 * max_batch);
     take(reinterpret_cast<void**>(&n->loss), sizeof(double));
+    take(reinterpret_cast<void**>(&n->coef), sizeof(double) * 2 * max_batch);
     take(reinterpret_cast<void**>(&n->error), sizeof(int));
     take(reinterpret_cast<void**>(&n->coarse_rhs), voxels(at_level(*n, 0, 1)) * 4);
     take(reinterpret_cast<void**>(&n->fine_guess), fine_cells * 4);
@@ -666,16 +774,37 @@ XsStatus xs_warm_start_gradient(XsWarmStartNet* net, cudaStream_t stream, uint32
     const uint64_t per = voxels(at_level(*n, 0, 1));
     XsStatus s = prepare_input(*n, stream, rhs, batch);
     if (s == XS_OK) s = forward(*n, stream, batch);
-    if (s == XS_OK) s = sample_inv_rms(*n, stream, pressure, per, batch, n->inv_rms_p);
     if (s != XS_OK) return s;
-    const double denom = static_cast<double>(per) * batch;
-    loss_kernel<<<dim3(kStatBlocks, batch), 256, 0, stream>>>(n->act[A_OUT], pressure, n->inv_rms_p, per, static_cast<float>(2.0 / denom),
-                                                             n->gbuf[G_OUT], n->partial);
-    if ((s = check_launch()) != XS_OK) return s;
-    loss_final_kernel<<<1, 256, 0, stream>>>(n->partial, kStatBlocks * batch, denom, loss ? loss : n->loss);
-    if ((s = check_launch()) != XS_OK) return s;
+    if (n->loss_kind == 1) {
+        const VolumeShape l0 = at_level(*n, 0, 1);
+        EnergyArgs ea{n->act[A_OUT], pressure, static_cast<int>(l0.x), static_cast<int>(l0.y), static_cast<int>(l0.z), n->loss_boundary, per};
+        energy_sums_kernel<<<dim3(kStatBlocks, batch), 256, 0, stream>>>(ea, n->partial);
+        if ((s = check_launch()) != XS_OK) return s;
+        energy_final_kernel<<<1, 64, 0, stream>>>(n->partial, kStatBlocks, batch, n->coef, loss ? loss : n->loss);
+        if ((s = check_launch()) != XS_OK) return s;
+        energy_grad_kernel<<<grid_for(per * batch), 256, 0, stream>>>(ea, batch, n->coef, n->gbuf[G_OUT]);
+        if ((s = check_launch()) != XS_OK) return s;
+    } else {
+        if ((s = sample_inv_rms(*n, stream, pressure, per, batch, n->inv_rms_p)) != XS_OK) return s;
+        const double denom = static_cast<double>(per) * batch;
+        loss_kernel<<<dim3(kStatBlocks, batch), 256, 0, stream>>>(n->act[A_OUT], pressure, n->inv_rms_p, per, static_cast<float>(2.0 / denom),
+                                                                 n->gbuf[G_OUT], n->partial);
+        if ((s = check_launch()) != XS_OK) return s;
+        loss_final_kernel<<<1, 256, 0, stream>>>(n->partial, kStatBlocks * batch, denom, loss ? loss : n->loss);
+        if ((s = check_launch()) != XS_OK) return s;
+    }
     if ((s = backward(*n, stream, batch)) != XS_OK) return s;
     if (gradient) return check_cuda(cudaMemcpyAsync(gradient, n->grad, parameter_count() * 4, cudaMemcpyDeviceToDevice, stream));
+    return XS_OK;
+}
+
+XsStatus xs_warm_start_set_loss(XsWarmStartNet* net, uint32_t kind, XsScalarBoundary pressure_boundary) {
+    WarmStartNet* n = reinterpret_cast<WarmStartNet*>(net);
+    if (!n || kind > 1) return XS_INVALID_ARGUMENT;
+    for (int f = 0; f < 6; ++f)
+        if (pressure_boundary.modes[f] > 2u) return XS_INVALID_ARGUMENT;
+    n->loss_kind = kind;
+    n->loss_boundary = pressure_boundary;
     return XS_OK;
 }
 

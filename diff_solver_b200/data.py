@@ -150,6 +150,9 @@ class Configuration:
     pressure_tolerance: float = 1.0e-6
     pressure_max_iterations: int = 4000
     warm_start: WarmStart = WarmStart.none
+    # previous forward solutions kept for the Galerkin start of the next
+    # forward PCG solve (0..5; 0: off)
+    warm_start_history: int = 0
 
 
 def plume_configuration(n=(64, 64, 64), cell_size=None, inflow_center=(0.5, 0.1, 0.5), inflow_radius=0.08,

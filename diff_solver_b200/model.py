@@ -145,6 +145,12 @@ class ExecutionContext:
         self._warm_start = guess
         self.native.pressure.initial_guess = None if guess is None else guess.data_ptr()
 
+    def reset_warm_start(self) -> None:
+        """Forgets the previous solutions of the Galerkin warm start (a new
+        trajectory starts)."""
+        N.check("xs_smoke_reset_warm_start", N.lib().xs_smoke_reset_warm_start(self.stream_handle, C.byref(self.native),
+                                                                                 C.c_void_p(self.workspace.data_ptr())))
+
     def set_inflow(self, index: int, center=None, radius=None) -> None:
         """Moves or resizes inflow ``index`` for the following steps (the
         inflow table travels to the device with every launch)."""
@@ -170,15 +176,22 @@ class ExecutionContext:
         p, b = C.c_void_p(), C.c_void_p()
         N.check("xs_smoke_pressure_fields", N.lib().xs_smoke_pressure_fields(C.byref(self.native), C.c_void_p(self.workspace.data_ptr()),
                                                                                C.byref(p), C.byref(b)))
+        return self._workspace_view(p), self._workspace_view(b)
+
+    def warm_start_fields(self):
+        """(x0, b - A x0) of the last forward solve, x0 the Galerkin start from
+        the ring of previous solutions (configuration.warm_start_history > 0),
+        as device tensors viewing the workspace."""
+        x, r = C.c_void_p(), C.c_void_p()
+        N.check("xs_smoke_warm_start_fields", N.lib().xs_smoke_warm_start_fields(self.stream_handle, C.byref(self.native),
+                                                                                   C.c_void_p(self.workspace.data_ptr()), C.byref(x),
+                                                                                   C.byref(r)))
+        return self._workspace_view(x), self._workspace_view(r)
+
+    def _workspace_view(self, ptr):
         n = int(self.native.grid.nx) * int(self.native.grid.ny) * int(self.native.grid.nz)
-        base = self.workspace.data_ptr()
-        flat = self.workspace.view(torch.uint8)
-
-        def view(ptr):
-            off = ptr.value - base
-            return flat[off:off + 4 * n].view(torch.float32)
-
-        return view(p), view(b)
+        off = ptr.value - self.workspace.data_ptr()
+        return self.workspace[off:off + 4 * n].view(torch.float32)
 
 
 def _grid(cfg: Configuration) -> N.XsGrid:
@@ -276,9 +289,13 @@ class Model:
         m.collider_velocity = N.vec(cv.components()) if has_colliders else N.XsVector(None, None, None)
         m.collider_density = cd.data_ptr() if has_colliders else None
         m.collider_temperature = ct.data_ptr() if has_colliders else None
+        m.warm_start_history = int(cfg.warm_start_history)
         ctx.native = m
         nbytes = L.xs_smoke_workspace_bytes(C.byref(m), int(mode))
+        if nbytes == 0:
+            raise ValueError("invalid model configuration (grid, inflows or warm-start history)")
         ctx.workspace = torch.empty(nbytes, dtype=torch.uint8, device=dev)
+        ctx.reset_warm_start()
         return ctx
 
     # ------------------------------------------------------------ allocation

@@ -119,6 +119,14 @@ class WarmStartNetwork:
                                                                          pressure.contiguous().data_ptr(), grad.data_ptr(), loss.data_ptr()))
         return loss, grad
 
+    def set_loss(self, kind: str, pressure_boundary: Optional[N.XsScalarBoundary] = None) -> None:
+        """``"l2"``: mean (out - p / rms(p))^2; ``"energy"``: the squared
+        relative A-norm error of the energy-optimally scaled guess, with A the
+        pressure operator of the network grid under ``pressure_boundary``."""
+        k = {"l2": 0, "energy": 1}[kind]
+        pb = pressure_boundary if pressure_boundary is not None else N.XsScalarBoundary()
+        N.check("xs_warm_start_set_loss", N.lib().xs_warm_start_set_loss(self.handle, k, pb))
+
     def adam_step(self, learning_rate: float, beta1: float = 0.9, beta2: float = 0.999, epsilon: float = 1e-8) -> None:
         N.check("xs_warm_start_adam_step", N.lib().xs_warm_start_adam_step(self.handle, self.stream_handle, learning_rate, beta1, beta2,
                                                                            epsilon))
@@ -161,13 +169,14 @@ class PlumeSampler:
 class _Plume:
     """One running plume simulation that yields a (rhs, pressure) pair per step."""
 
-    def __init__(self, resolution, rng: np.random.Generator, sampler: PlumeSampler, stream):
+    def __init__(self, resolution, rng: np.random.Generator, sampler: PlumeSampler, stream, history: int = 0):
         from .data import plume_configuration
         from .model import ExecutionMode, Model, fill_parameters
         self.rng = rng
         self.sampler = sampler
         centre, radius, buoyancy = sampler.draw(rng)
         cfg = plume_configuration(tuple(resolution), inflow_center=centre, inflow_radius=radius)
+        cfg.warm_start_history = int(history)
         self.model = Model(cfg)
         self.ctx = self.model.allocate_context(ExecutionMode.forward, stream=stream)
         self.state = self.model.allocate_state(self.ctx)
@@ -187,6 +196,7 @@ class _Plume:
                 t.zero_()
             for t in self.state.velocity.components():
                 t.copy_((torch.rand(t.shape, generator=g) * 0.02 - 0.01).to(t.device))
+        self.ctx.reset_warm_start()
         self.steps = 0
 
     def restart(self):
@@ -205,13 +215,18 @@ class _Plume:
 
 def train_on_plumes(network: WarmStartNetwork, pairs: int = 20000, batch: int = 8, learning_rate: float = 1e-3,
                     buffer_size: int = 256, episode_steps: int = 200, warmup_pairs: int = 64, seed: int = 0,
-                    log: Optional[Callable[[dict], None]] = None, log_every: int = 50) -> List[dict]:
-    """Trains ``network`` on ``pairs`` (rhs, pressure) pairs generated by the
-    plain PCG solver on its own grid: ``batch`` plumes run side by side, each
-    step adds their pairs to a replay buffer of ``buffer_size`` pairs in device
-    memory, and one Adam step runs on ``batch`` pairs drawn from the buffer.
-    A plume restarts with new random parameters after ``episode_steps``
-    steps.  Returns the logged records."""
+                    log: Optional[Callable[[dict], None]] = None, log_every: int = 50, loss: str = "energy",
+                    history: int = 0) -> List[dict]:
+    """Trains ``network`` on ``pairs`` pairs generated by the PCG solver on
+    its own grid: ``batch`` plumes run side by side, each step adds their
+    pairs to a replay buffer of ``buffer_size`` pairs in device memory, and
+    one Adam step runs on ``batch`` pairs drawn from the buffer.  A plume
+    restarts with new random parameters after ``episode_steps`` steps.
+
+    With ``history`` = 0 the pairs are (rhs, pressure) of plain solves; with
+    a ring of ``history`` previous solutions they are (b - A x0, p - x0), x0
+    the ring's Galerkin start: the correction the network supplies when it
+    serves a model that keeps a ring.  Returns the logged records."""
     if network.max_batch < batch:
         raise ValueError(f"the network was created for batches of at most {network.max_batch}")
     rng = np.random.default_rng(seed)
@@ -219,7 +234,8 @@ def train_on_plumes(network: WarmStartNetwork, pairs: int = 20000, batch: int = 
     stream = network.stream
     n = network.cells
     dev = torch.device("cuda")
-    plumes = [_Plume(network.shape, rng, sampler, stream) for _ in range(batch)]
+    plumes = [_Plume(network.shape, rng, sampler, stream, history=history) for _ in range(batch)]
+    network.set_loss(loss, plumes[0].ctx.native.pressure_boundary)
     # stagger the episodes so the buffer mixes early and developed plumes
     for i, p in enumerate(plumes):
         p.steps = -(i * episode_steps // batch)
@@ -238,8 +254,13 @@ def train_on_plumes(network: WarmStartNetwork, pairs: int = 20000, batch: int = 
                 pressure, rhs = p.step()
                 if p.steps <= 0:
                     continue
-                buf_rhs[head].copy_(rhs)
-                buf_p[head].copy_(pressure)
+                if history:
+                    x0, r0 = p.ctx.warm_start_fields()
+                    buf_rhs[head].copy_(r0)
+                    torch.sub(pressure, x0, out=buf_p[head])
+                else:
+                    buf_rhs[head].copy_(rhs)
+                    buf_p[head].copy_(pressure)
                 head = (head + 1) % buffer_size
                 filled = min(filled + 1, buffer_size)
                 generated += 1
@@ -257,6 +278,62 @@ def train_on_plumes(network: WarmStartNetwork, pairs: int = 20000, batch: int = 
                     log(rec)
     network.check()
     return records
+
+
+def evaluate_on_plume(network: WarmStartNetwork, resolution: Sequence[int], steps: int = 100, every: int = 10,
+                      centre=(0.5, 0.1, 0.5), radius: float = 0.08, buoyancy: float = 0.5, seed: int = 1234) -> List[dict]:
+    """Runs the plain-PCG plume on ``resolution`` (the network grid times its
+    factor) for ``steps`` steps and, every ``every`` steps, solves that
+    step's pressure problem again from the network's energy-scaled guess.
+    Returns one record per evaluated step: the plain and the learned PCG
+    iteration counts and the learned start's relative residual."""
+    rng = np.random.default_rng(seed)
+    sampler = PlumeSampler(centre_low=tuple(centre), centre_high=tuple(centre), radius=(radius, radius), buoyancy=(buoyancy, buoyancy))
+    stream = network.stream
+    plume = _Plume(resolution, rng, sampler, stream)
+    grid = plume.ctx.native.grid
+    out: List[dict] = []
+    with torch.cuda.stream(stream):
+        for s in range(1, steps + 1):
+            _, rhs = plume.step()
+            if s % every:
+                continue
+            plain = plume.ctx.read_solve_stats()
+            learned = solve_iterations(plume.model, plume.ctx, rhs, network.guess(grid, rhs))
+            out.append({"step": s, "plain_iterations": plain["iterations"], "learned_iterations": learned["iterations"],
+                        "learned_initial_residual": learned["initial_residual"], "warm_start_used": learned["warm_start_used"],
+                        "guess_scale": learned["guess_scale"], "learned_final_residual": learned["final_residual"]})
+    network.check()
+    return out
+
+
+def evaluate_arms(network: Optional[WarmStartNetwork], resolution: Sequence[int], steps: int = 100, history: int = 4,
+                  centre=(0.5, 0.1, 0.5), radius: float = 0.08, buoyancy: float = 0.5, seed: int = 1234) -> dict:
+    """Runs the same plume side by side with the forward solve started from
+    zero ("plain"), from the Galerkin combination of the last ``history``
+    solutions ("history"), from the learned guess alone ("learned") and from
+    both ("learned+history"), and returns each arm's per-step PCG iteration
+    counts.  The arms' states agree within the solver tolerance."""
+    sampler = PlumeSampler(centre_low=tuple(centre), centre_high=tuple(centre), radius=(radius, radius), buoyancy=(buoyancy, buoyancy))
+    stream = network.stream if network is not None else torch.cuda.current_stream()
+    arms = {"plain": (0, False), "history": (history, False)}
+    if network is not None:
+        arms.update({"learned": (0, True), "learned+history": (history, True)})
+    plumes = {}
+    for name, (h, learned) in arms.items():
+        p = _Plume(resolution, np.random.default_rng(seed), sampler, stream, history=h)
+        if learned:
+            p.ctx.set_learned_warm_start(network)
+        plumes[name] = p
+    out = {name: [] for name in arms}
+    with torch.cuda.stream(stream):
+        for _ in range(steps):
+            for name, p in plumes.items():
+                p.step()
+                out[name].append(int(p.ctx.read_solve_stats()["iterations"]))
+    if network is not None:
+        network.check()
+    return out
 
 
 def solve_iterations(model, ctx, rhs: torch.Tensor, guess: Optional[torch.Tensor], scale: bool = True) -> dict:

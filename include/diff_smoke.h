@@ -301,6 +301,13 @@ typedef struct XsSmokeModel {
      * energy-scaled and PCG falls back to zero when it does not help.  Not
      * used by the JVP and VJP solves. */
     XsWarmStartNet* warm_start;
+    /* number of previous forward solutions kept in the workspace (0..5; 0:
+     * off).  The forward PCG then starts from the A-norm-optimal (Galerkin)
+     * combination of those solutions and the learned guess, if any.  The ring
+     * is part of the workspace (xs_smoke_workspace_bytes counts it) and is
+     * emptied by xs_smoke_reset_warm_start, which must run once after the
+     * workspace is allocated. */
+    uint32_t warm_start_history;
 } XsSmokeModel;
 
 /* State / Control / Parameters (data.ixx:117-134) */
@@ -356,6 +363,17 @@ XsStatus xs_smoke_read_solve_stats(cudaStream_t stream, const XsSmokeModel* mode
  * the (divergence, pressure) pairs the warm-start network trains on. */
 XsStatus xs_smoke_pressure_fields(const XsSmokeModel* model, void* workspace, float** pressure, float** rhs);
 
+/* With a ring of previous solutions: device pointers, inside the workspace,
+ * of the ring's Galerkin start x0 of the last forward solve and of its
+ * residual b - A x0 (recomputed on the stream by this call): with the
+ * solution, the (residual, correction) pairs the network learns when it
+ * serves a model that keeps a ring. */
+XsStatus xs_smoke_warm_start_fields(cudaStream_t stream, const XsSmokeModel* model, void* workspace, float** ring_start, float** residual);
+
+/* Empties the ring of previous solutions (model->warm_start_history > 0):
+ * after allocating the workspace and when a new trajectory starts. */
+XsStatus xs_smoke_reset_warm_start(cudaStream_t stream, const XsSmokeModel* model, void* workspace);
+
 /* ------------------------------------------------------------------------ */
 /* learned pressure warm start (no reference counterpart)                    */
 /* ------------------------------------------------------------------------ */
@@ -407,6 +425,12 @@ XsStatus xs_warm_start_predict(XsWarmStartNet* net, cudaStream_t stream, uint32_
  * (device, parameter_count floats, may be NULL; the network keeps its own copy). */
 XsStatus xs_warm_start_gradient(XsWarmStartNet* net, cudaStream_t stream, uint32_t batch, const float* rhs, const float* pressure,
                                 float* gradient, double* loss);
+/* Training loss: kind 0 (default) the normalised L2 loss above; kind 1 the
+ * energy loss mean_b 1 - (g.Ap)^2 / ((g.Ag)(p.Ap)) with g = output channel 0
+ * and A the 7-point pressure operator of the network grid under
+ * pressure_boundary (no solids): the squared relative A-norm error of the
+ * energy-optimally scaled guess.  Takes effect at the next gradient. */
+XsStatus xs_warm_start_set_loss(XsWarmStartNet* net, uint32_t kind, XsScalarBoundary pressure_boundary);
 /* One Adam update from the last gradient. */
 XsStatus xs_warm_start_adam_step(XsWarmStartNet* net, cudaStream_t stream, float learning_rate, float beta1, float beta2, float epsilon);
 /* xs_warm_start_gradient followed by Adam (beta 0.9 / 0.999, epsilon 1e-8). */

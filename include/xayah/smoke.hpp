@@ -91,6 +91,8 @@ struct Configuration {
     PressureSolver pressure_solver{PressureSolver::jacobi_pcg};
     double pressure_tolerance{1.0e-6};
     std::uint32_t pressure_max_iterations{4000u};
+    // previous forward solutions kept for the Galerkin warm start (0..5; 0: off)
+    std::uint32_t warm_start_history{0u};
 };
 
 // ------------------------------------------------------------- data.ixx:85-204
@@ -257,7 +259,11 @@ public:
         m.collider_velocity = colliders ? view(ctx.domain.collider_velocity) : XsVector{nullptr, nullptr, nullptr};
         m.collider_density = colliders ? ctx.domain.collider_density.values.data : nullptr;
         m.collider_temperature = colliders ? ctx.domain.collider_temperature.values.data : nullptr;
-        ctx.workspace_ = cuda::Buffer<unsigned char>(ctx.resource, xs_smoke_workspace_bytes(&m, static_cast<std::uint32_t>(mode)));
+        m.warm_start_history = configuration.warm_start_history;
+        const std::size_t bytes = xs_smoke_workspace_bytes(&m, static_cast<std::uint32_t>(mode));
+        if (bytes == 0) throw std::invalid_argument("invalid smoke configuration");
+        ctx.workspace_ = cuda::Buffer<unsigned char>(ctx.resource, bytes);
+        check(xs_smoke_reset_warm_start(ctx.resource->stream(), &m, ctx.workspace_.data), "xs_smoke_reset_warm_start");
         ctx.resource->synchronize();
         return ctx;
     }

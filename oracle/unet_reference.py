@@ -85,10 +85,38 @@ def forward(weights, x0, bf16=True):
     return _conv(d0, w[11], False, bf16)
 
 
-def loss_and_gradient(flat_params: np.ndarray, rhs: np.ndarray, pressure: np.ndarray, bf16=True):
-    """Loss mean (out_0 - p / rms(p))^2 and its gradient (flat, FP32), with
-    the weights rounded to BF16 as the GPU uses them.  rhs, pressure:
-    [B, Z, Y, X]."""
+def apply_operator(u, modes):
+    """The 7-point pressure operator without solids on u [B, Z, Y, X]; modes
+    of the faces x-, x+, y-, y+, z-, z+ (0 fixed value, 1 zero gradient,
+    2 periodic): diag counts in-domain or periodic neighbours plus fixed
+    faces; (A u) = diag u - sum of neighbours."""
+    diag = torch.zeros_like(u)
+    acc = torch.zeros_like(u)
+    for d, axis in ((0, 3), (1, 2), (2, 1)):
+        periodic = modes[2 * d] == 2 and modes[2 * d + 1] == 2
+        n = u.shape[axis]
+        for side in (0, 1):
+            if periodic:
+                acc = acc + torch.roll(u, shifts=-1 if side else 1, dims=axis)
+                diag = diag + 1.0
+                continue
+            idx = torch.arange(n)
+            inside = ((idx + 1 < n) if side else (idx - 1 >= 0)).to(u.dtype)
+            shape = [1, 1, 1, 1]
+            shape[axis] = n
+            inside = inside.view(shape)
+            nb = torch.roll(u, shifts=-1 if side else 1, dims=axis) * inside
+            acc = acc + nb
+            diag = diag + inside + ((1.0 - inside) if modes[2 * d + side] == 0 else 0.0)
+    return diag * u - acc
+
+
+def loss_and_gradient(flat_params: np.ndarray, rhs: np.ndarray, pressure: np.ndarray, bf16=True, kind="l2", modes=None):
+    """Loss and its gradient (flat, FP32), with the weights rounded to BF16
+    as the GPU uses them.  rhs, pressure: [B, Z, Y, X].  kind "l2": mean
+    (out_0 - p / rms(p))^2; kind "energy": mean over samples of
+    1 - (g.Ap)^2 / ((g.Ag)(p.Ap)) with g = out_0 and A the operator of
+    ``modes``."""
     p = torch.from_numpy(np.asarray(flat_params, dtype=np.float32))
     pb = p.to(torch.bfloat16).float() if bf16 else p.clone()
     pb.requires_grad_(True)
@@ -97,9 +125,18 @@ def loss_and_gradient(flat_params: np.ndarray, rhs: np.ndarray, pressure: np.nda
     out = forward(w, x0, bf16)[:, 0]
     t = torch.from_numpy(pressure).double()
     b = t.shape[0]
-    rms = torch.sqrt((t.reshape(b, -1) ** 2).mean(dim=1))
-    target = (t / rms.view(b, 1, 1, 1)).float()
-    loss = ((out - target) ** 2).mean()
+    if kind == "energy":
+        g = out.double()
+        at = apply_operator(t, modes)
+        ag = apply_operator(g, modes)
+        s1 = (g * at).reshape(b, -1).sum(1)
+        s2 = (g * ag).reshape(b, -1).sum(1)
+        s3 = (t * at).reshape(b, -1).sum(1)
+        loss = (1.0 - s1 * s1 / (s2 * s3)).mean()
+    else:
+        rms = torch.sqrt((t.reshape(b, -1) ** 2).mean(dim=1))
+        target = (t / rms.view(b, 1, 1, 1)).float()
+        loss = ((out - target) ** 2).mean()
     loss.backward()
     return float(loss.detach()), pb.grad.numpy().copy()
 

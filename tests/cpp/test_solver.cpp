@@ -8,6 +8,7 @@
 
 #include "xayah/smoke.hpp"
 #include "xayah/solver.hpp"
+#include "xayah/warm_start.hpp"
 
 using namespace xayah;
 
@@ -129,11 +130,33 @@ int main() {
             for (std::size_t i = 0; i < g.size(); ++i) rhs += g[i] * vhost[a][i];
         }
         const XsSolveStats st = ctx.solve_stats();
+
+        // learned warm start on a grid the network tiles (128 x 64 x 32, network at factor 1)
+        smoke::Configuration wc = plume();
+        wc.resolution = {128u, 64u, 32u};
+        wc.cell_size = 1.0F / 128.0F;
+        wc.time_step = 0.5F * wc.cell_size;
+        wc.vorticity_confinement_enabled = false;
+        wc.pressure_tolerance = 1.0e-6;
+        const smoke::Model wmodel{wc};
+        smoke::ExecutionContext wctx = wmodel.allocate_context(smoke::ExecutionMode::forward);
+        smoke::WarmStartNetwork net(128u, 64u, 32u, 1u, 1u, 3u, wctx.resource->stream());
+        wctx.set_learned_warm_start(net.native());
+        smoke::State w0 = wmodel.allocate_state(wctx);
+        smoke::Parameters wp = wmodel.allocate_parameters(wctx);
+        wctx.resource->copy_from_host(wp.density_buoyancy.data, &values[1], 4);
+        wctx.resource->copy_from_host(wp.temperature_buoyancy.data, &values[2], 4);
+        std::vector<smoke::Control> wcontrols;
+        for (int i = 0; i < 3; ++i) wcontrols.push_back(wmodel.allocate_control(wctx));
+        auto wtraj = solver::simulate(wmodel, wctx, w0, std::span<const smoke::Control>{wcontrols}, wp, solver::TapeMode::recompute_step_cache);
+        net.check_status();
+        const XsSolveStats wst = wctx.solve_stats();
         std::printf("{\"forward_checkpoint_vs_store_all\": %.3e, \"vjp_recompute_vs_store_all\": %.3e, "
                     "\"vjp_checkpoint_vs_store_all\": %.3e, \"dot_jvp\": %.12e, \"dot_vjp\": %.12e, \"checkpoints\": %zu, "
-                    "\"last_solve_status\": %u, \"last_solve_residual\": %.3e}\n",
+                    "\"last_solve_status\": %u, \"last_solve_residual\": %.3e, \"warm_solve_status\": %u, "
+                    "\"warm_solve_residual\": %.3e, \"warm_states\": %zu}\n",
                     forward_diff, max_rel(gu_rec, gu_all), max_rel(gu_chk, gu_all), lhs, rhs, chk.states.size(), st.status,
-                    st.final_residual);
+                    st.final_residual, wst.status, wst.final_residual, wtraj.states.size());
         return 0;
     } catch (const std::exception& e) {
         std::fprintf(stderr, "test_solver failed: %s\n", e.what());

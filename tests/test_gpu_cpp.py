@@ -37,3 +37,5 @@ def test_cpp_solver_tape_modes_agree(cuda):
     assert out["checkpoints"] == 3  # steps 0, 4, 6
     assert out["last_solve_status"] == 0
     assert abs(out["dot_jvp"] - out["dot_vjp"]) <= 1e-4 * max(abs(out["dot_jvp"]), 1e-12), out
+    # a model carrying the (untrained) learned warm start still solves to 1e-6
+    assert out["warm_solve_status"] == 0 and out["warm_solve_residual"] <= 1e-6 and out["warm_states"] == 4

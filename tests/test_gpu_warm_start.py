@@ -87,6 +87,29 @@ def test_loss_and_gradient_match_reference(net_and_data):
         off += n
 
 
+@pytest.mark.parametrize("modes", [(1, 1, 1, 0, 1, 1), (2, 2, 0, 1, 2, 2)])
+def test_energy_loss_and_gradient_match_reference(cuda, modes):
+    """The energy (A-norm) loss: plume boundaries (open top) and a periodic
+    variant, against autograd through the reference operator."""
+    import torch
+    from diff_solver_b200 import _native as N
+    from diff_solver_b200.warm_start import WarmStartNetwork
+    from oracle import unet_reference as R
+    rng = np.random.default_rng(21)
+    rhs = smooth_field(rng, SHAPE, 2)
+    p = smooth_field(rng, SHAPE, 2)
+    net = WarmStartNetwork(SHAPE, max_batch=2, seed=5)
+    pb = N.XsScalarBoundary()
+    pb.modes[:] = list(modes)
+    net.set_loss("energy", pb)
+    loss, grad = net.gradient(torch.from_numpy(rhs).cuda().reshape(-1), torch.from_numpy(p).cuda().reshape(-1))
+    net.check()
+    want_loss, want_grad = R.loss_and_gradient(net.parameters(), rhs, p, kind="energy", modes=modes)
+    assert 0.0 <= want_loss <= 1.0
+    assert abs(float(loss.item()) - want_loss) < 1e-2 * max(want_loss, 1e-3)
+    assert rel(grad.cpu().numpy(), want_grad) < 3e-2
+
+
 def test_guess_restricts_and_prolongs(net_and_data):
     import torch
     from diff_solver_b200 import _native as N
@@ -154,6 +177,61 @@ def test_energy_scaled_guess_and_fallback(cuda):
     noise = torch.randn(b.numel(), device=b.device, generator=torch.Generator(device=b.device).manual_seed(2))
     st = solve_iterations(m, ctx, b, noise)
     assert st["status"] == 0 and st["final_residual"] <= 1e-6 and abs(st["guess_scale"]) < 0.1
+
+
+def _rollout(cfg, steps, network=None, seed=0):
+    import torch
+    from diff_solver_b200.model import ExecutionMode, Model, fill_parameters
+    m = Model(cfg)
+    ctx = m.allocate_context(ExecutionMode.forward)
+    if network is not None:
+        ctx.set_learned_warm_start(network)
+    s, n = m.allocate_state(ctx), m.allocate_state(ctx)
+    c, k = m.allocate_control(ctx), m.allocate_step_cache(ctx)
+    q = fill_parameters(m.allocate_parameters(ctx), 0.0, -0.1, 0.5)
+    g = torch.Generator().manual_seed(seed)
+    for t in s.velocity.components():
+        t.copy_((torch.rand(t.shape, generator=g) * 0.02 - 0.01).cuda())
+    stats = []
+    for _ in range(steps):
+        m.forward_step(s, c, q, n, k, ctx)
+        s, n = n, s
+        stats.append(ctx.read_solve_stats())
+    vel = torch.cat([t.reshape(-1) for t in s.velocity.components()]).cpu().numpy()
+    return vel, stats, ctx
+
+
+def test_galerkin_history_start(cuda):
+    """Previous solutions as a Galerkin start: same steps within the solver
+    tolerance, far fewer iterations once the ring holds solutions, and a
+    reset ring starts from zero again."""
+    from diff_solver_b200.data import plume_configuration
+    cfg = plume_configuration((64, 64, 64))
+    plain, plain_stats, _ = _rollout(cfg, 24)
+    cfg.warm_start_history = 4
+    warm, warm_stats, ctx = _rollout(cfg, 24)
+    assert all(s["status"] == 0 and s["final_residual"] <= 1e-6 for s in warm_stats)
+    assert warm_stats[0]["iterations"] == plain_stats[0]["iterations"]  # empty ring: zero start
+    late_plain = np.mean([s["iterations"] for s in plain_stats[8:]])
+    late_warm = np.mean([s["iterations"] for s in warm_stats[8:]])
+    assert late_warm < 0.6 * late_plain, (late_warm, late_plain)
+    assert rel(warm, plain) < 1e-4
+    ctx.reset_warm_start()
+
+
+def test_galerkin_history_with_learned_guess(cuda):
+    from diff_solver_b200.data import plume_configuration
+    from diff_solver_b200.warm_start import WarmStartNetwork
+    res = (128, 64, 32)
+    cfg = plume_configuration(res)
+    plain, plain_stats, _ = _rollout(cfg, 8)
+    cfg.warm_start_history = 3
+    net = WarmStartNetwork(res, factor=1, seed=4)
+    warm, warm_stats, _ = _rollout(cfg, 8, network=net)
+    net.check()
+    assert all(s["status"] == 0 and s["final_residual"] <= 1e-6 for s in warm_stats)
+    assert rel(warm, plain) < 1e-4
+    assert sum(s["iterations"] for s in warm_stats) < sum(s["iterations"] for s in plain_stats)
 
 
 def test_learned_warm_start_inside_a_model_step(cuda):

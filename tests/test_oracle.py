@@ -111,3 +111,27 @@ def test_tangent_and_adjoint_are_transposes(name):
     if cfg.vorticity_confinement_enabled:
         rhs += v_par["vorticity_confinement"] * padj.vorticity_confinement
     assert abs(lhs - rhs) <= 1e-9 * max(abs(lhs), 1.0), (lhs, rhs)
+
+
+def test_network_reference_operator_matches_the_c_oracle():
+    """The 7-point operator of the warm-start network's energy loss (oracle/
+    unet_reference.py) is the pressure matrix the C oracle restates from the
+    reference's red-black Gauss-Seidel, on grids without solids."""
+    import torch
+    from common import scenario
+    from oracle import binding as ob
+    from oracle import unet_reference as R
+    checked = 0
+    for name in ("plume", "periodic", "fixed_values"):
+        cfg = scenario(name, (12, 10, 8))
+        P = ob.Problem(cfg, "f64", solver="pcg", iterations=10, tolerance=1e-8)
+        if P.anchor < 12 * 10 * 8:  # an anchored (all-Neumann) problem drops one row
+            continue
+        rng = np.random.default_rng(1)
+        u = rng.normal(size=12 * 10 * 8)
+        want = P.apply_operator(u)
+        modes = [int(f.mode) for f in cfg.pressure_boundary.faces()]
+        got = R.apply_operator(torch.from_numpy(u.reshape(1, 8, 10, 12)), modes).numpy().reshape(-1)
+        np.testing.assert_allclose(got, want, rtol=1e-12, atol=1e-12)
+        checked += 1
+    assert checked >= 2
