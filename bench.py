@@ -47,9 +47,17 @@ HISTORY = 5
 WEIGHTS = os.path.join(ROOT, "diff_solver_b200", "weights", "warm_start_128.npz")
 
 
-def workload_configuration(n=GRID, history=0):
+def grid_shape(spec):
+    """'256' -> (256, 256, 256); '512,512,256' -> (512, 512, 256)."""
+    v = [int(s) for s in str(spec).split(",")]
+    return tuple(v * 3) if len(v) == 1 else tuple(v)
+
+
+def workload_configuration(shape=(GRID,) * 3, history=0):
+    """dx = 1 / nx; the inflow sits at x = 0.5, y = 0.1 and the middle of z."""
     from diff_solver_b200.data import plume_configuration
-    cfg = plume_configuration((n, n, n), inflow_center=(0.5, 0.1, 0.5), inflow_radius=0.08)
+    nx, ny, nz = shape
+    cfg = plume_configuration((nx, ny, nz), inflow_center=(0.5, 0.1, 0.5 * nz / nx), inflow_radius=0.08)
     cfg.pressure_tolerance = 1e-6
     cfg.pressure_max_iterations = 20000
     cfg.warm_start_history = history
@@ -155,7 +163,7 @@ def max_over_ranks(value, world):
 
 
 # --------------------------------------------------------------------- CPU
-def cpu_sample(n=GRID, sample_iterations=8, gpu_iterations=None):
+def cpu_sample(shape=(GRID,) * 3, sample_iterations=8, gpu_iterations=None):
     """The FP64 oracle step on the host cores: one step with the PCG capped at
     0 and at `sample_iterations` iterations; the step time at the GPU's
     iteration count is t0 + k * (t_k - t0) / sample_iterations."""
@@ -163,7 +171,7 @@ def cpu_sample(n=GRID, sample_iterations=8, gpu_iterations=None):
     from oracle import binding as ob
     threads = os.cpu_count() or 1
     ob.set_threads(threads)
-    cfg = workload_configuration(n)
+    cfg = workload_configuration(shape)
     rng = np.random.default_rng(0)
     P0 = ob.Problem(cfg, "f64", solver="pcg", iterations=0, tolerance=1e-6)
     st = ob.zeros_state(P0.res, np.float64)
@@ -181,7 +189,7 @@ def cpu_sample(n=GRID, sample_iterations=8, gpu_iterations=None):
     k = gpu_iterations if gpu_iterations is not None else 1400
     seconds = t0 + k * per_iteration
     return {"value": 1.0 / seconds, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"FP64 oracle forward step at {n}^3 on {threads} threads: one step with 0 and one with {sample_iterations} "
+            "sample": f"FP64 oracle forward step at {'x'.join(map(str, shape))} on {threads} threads: one step with 0 and one with {sample_iterations} "
                       f"PCG iterations ({t0:.2f} s, {tk:.2f} s), projected to {k} iterations per step "
                       f"({per_iteration * 1e3:.1f} ms per iteration)",
             "seconds_per_step": seconds}
@@ -301,14 +309,15 @@ def product_run(args, world, rank, local):
     import torch
     torch.cuda.set_device(local)
     network = None
-    if args.grid % 2 == 0 and not args.no_learned:
+    if not args.no_learned:
         from diff_solver_b200.warm_start import WarmStartNetwork
         if not os.path.exists(WEIGHTS):
             raise FileNotFoundError(f"{WEIGHTS} is missing: train it with python -m diff_solver_b200.train_warm_start")
-        network = WarmStartNetwork((args.grid // 2,) * 3, factor=2)
+        # trained at 128^3, applied fully convolutionally on the grid restricted x2
+        network = WarmStartNetwork(tuple(s // 2 for s in args.shape), factor=2)
         network.load(WEIGHTS)
     # spin-up from rest with the fastest start; its final state opens every arm
-    spin = Rollout(args.grid, HISTORY, network)
+    spin = Rollout(args.shape, HISTORY, network)
     gen = torch.Generator(device="cuda").manual_seed(0)
     for t in spin.cur.velocity.components():
         t.uniform_(-0.01, 0.01, generator=gen)
@@ -329,7 +338,7 @@ def product_run(args, world, rank, local):
     sampler.start()
     results = {}
     for name, history, net in arms:
-        ro = Rollout(args.grid, history, net)
+        ro = Rollout(args.shape, history, net)
         results[name] = timed_arm(args, world, ro, initial, e2e=(name == headline))
         del ro
         torch.cuda.empty_cache()
@@ -346,21 +355,24 @@ def main():
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--spinup", type=int, default=40, help="steps from rest before the arms start")
     ap.add_argument("--impl", choices=["product", "reference"], default="product")
-    ap.add_argument("--grid", type=int, default=GRID)
+    ap.add_argument("--grid", default=str(GRID), help="N for N^3, or nx,ny,nz")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="plain and history arms only")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
+    args.shape = grid_shape(args.grid)
     world, rank, local = init_distributed()
-    n = args.grid ** 3
-    config = {"workload": f"smoke plume {args.grid}^3 after a {args.spinup}-step spin-up from rest, Jacobi-PCG to rel. residual 1e-6",
-              "grid": [args.grid] * 3, "cells": n, "dt": "0.5 dx", "steps_per_replica": args.steps, "spinup_steps": args.spinup,
-              "warm_start": f"Galerkin start over the last {HISTORY} solutions + U-Net correction (128^3 network, restriction x2)",
-              "l2": "inputs larger than L2 (state 336 MB at 256^3)", "parallelism": f"replicas{world}"}
+    n = args.shape[0] * args.shape[1] * args.shape[2]
+    name = "x".join(map(str, args.shape))
+    config = {"workload": f"smoke plume {name} after a {args.spinup}-step spin-up from rest, Jacobi-PCG to rel. residual 1e-6",
+              "grid": list(args.shape), "cells": n, "dt": "0.5 dx", "steps_per_replica": args.steps, "spinup_steps": args.spinup,
+              "warm_start": f"Galerkin start over the last {HISTORY} solutions + U-Net correction (network trained at 128^3, "
+                            f"applied on the grid restricted x2)",
+              "l2": f"inputs larger than L2 (state {n * 21 * 4 / 1e6:.0f} MB)", "parallelism": f"replicas{world}"}
     if args.impl == "reference":
         if rank == 0:
-            cpu = cpu_sample(args.grid, gpu_iterations=None)
+            cpu = cpu_sample(args.shape, gpu_iterations=None)
             line = {"impl": "reference", "metric": METRIC, "value": cpu["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
                     "warmup": args.warmup, "ms_per_step": 1e3 * cpu["seconds_per_step"], "higher_is_better": True,
                     "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
@@ -399,7 +411,7 @@ def main():
                     "d2h_bytes_per_step": h["d2h"]},
             "example_metrics_last_step": [float(v) for v in h["metrics"]]}
     if world == 1 and not args.no_cpu_baseline:
-        cpu = cpu_sample(args.grid, gpu_iterations=int(arms["plain"]["mean_pcg_iterations"]))
+        cpu = cpu_sample(args.shape, gpu_iterations=int(arms["plain"]["mean_pcg_iterations"]))
         line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
     print(json.dumps(line), flush=True)
 
