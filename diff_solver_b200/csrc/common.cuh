@@ -196,6 +196,30 @@ __device__ __forceinline__ void grid_coordinates(const Vec3& p, float h, int axi
     gz = p.z / h - (axis == 2 ? 0.0f : 0.5f);
 }
 
+// True when the 2x2x2 stencil with lower corner (x0, y0, z0) lies inside an
+// array whose rows run to lx, ly, lz with no boundary rule involved: then
+// load_scalar / load_face return plain array elements, and the stencil is
+// read with 32-bit offsets and no per-node boundary logic (the same values,
+// so the same results).  lx etc. are the array extents, or the wrap period
+// on a periodic axis.
+__device__ __forceinline__ bool interior_stencil(int x0, int y0, int z0, int lx, int ly, int lz) {
+    return static_cast<unsigned>(x0) + 1u < static_cast<unsigned>(lx) && static_cast<unsigned>(y0) + 1u < static_cast<unsigned>(ly) &&
+           static_cast<unsigned>(z0) + 1u < static_cast<unsigned>(lz) && x0 >= 0 && y0 >= 0 && z0 >= 0;
+}
+
+__device__ __forceinline__ void load_stencil(const float* __restrict__ v, int x0, int y0, int z0, int ex, int ey, float (&v8)[2][2][2]) {
+    const uint32_t sy = static_cast<uint32_t>(ex), sz = static_cast<uint32_t>(ex) * static_cast<uint32_t>(ey);
+    const float* c = v + (static_cast<uint32_t>(x0) + sy * static_cast<uint32_t>(y0) + sz * static_cast<uint32_t>(z0));
+    v8[0][0][0] = __ldg(c);
+    v8[0][0][1] = __ldg(c + 1);
+    v8[0][1][0] = __ldg(c + sy);
+    v8[0][1][1] = __ldg(c + sy + 1);
+    v8[1][0][0] = __ldg(c + sz);
+    v8[1][0][1] = __ldg(c + sz + 1);
+    v8[1][1][0] = __ldg(c + sz + sy);
+    v8[1][1][1] = __ldg(c + sz + sy + 1);
+}
+
 // operators.cu:136-164
 template <bool kGradient>
 __device__ __forceinline__ Sample sample_scalar(const float* __restrict__ v, const Vec3& p, const Grid& g, const XsScalarBoundary& b) {
@@ -203,6 +227,9 @@ __device__ __forceinline__ Sample sample_scalar(const float* __restrict__ v, con
     grid_coordinates(p, g.h, -1, gx, gy, gz);
     const int x0 = static_cast<int>(floorf(gx)), y0 = static_cast<int>(floorf(gy)), z0 = static_cast<int>(floorf(gz));
     float v8[2][2][2];
+    if (interior_stencil(x0, y0, z0, g.nx, g.ny, g.nz))
+        load_stencil(v, x0, y0, z0, g.nx, g.ny, v8);
+    else
 #pragma unroll
     for (int dz = 0; dz < 2; ++dz)
 #pragma unroll
@@ -221,6 +248,10 @@ __device__ __forceinline__ Sample sample_face(const float* __restrict__ v, int a
     grid_coordinates(p, g.h, axis, gx, gy, gz);
     const int x0 = static_cast<int>(floorf(gx)), y0 = static_cast<int>(floorf(gy)), z0 = static_cast<int>(floorf(gz));
     float v8[2][2][2];
+    const int ex = extent(g, axis, 0), ey = extent(g, axis, 1), ez = extent(g, axis, 2);
+    if (interior_stencil(x0, y0, z0, periodic(b, 0) ? g.nx : ex, periodic(b, 1) ? g.ny : ey, periodic(b, 2) ? g.nz : ez))
+        load_stencil(v, x0, y0, z0, ex, ey, v8);
+    else
 #pragma unroll
     for (int dz = 0; dz < 2; ++dz)
 #pragma unroll
