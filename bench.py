@@ -390,6 +390,15 @@ def main():
                       "pcg_iterations_per_step": r["iterations"], "mean_pcg_iterations": statistics.mean(r["iterations"]),
                       "solve_ms_per_step": statistics.mean(r["solve_ms"]), "initial_residuals": r["initial_residuals"],
                       "final_residuals": r["residuals"], "gpu_launches": r["launches"]}
+    # whole-step roofline: B_step = 4 (8 N + 8 F) + 40 N k bytes per step (the
+    # scope table's count: fused stages once, 10 floats per cell per CG iteration)
+    nx, ny, nz = args.shape
+    faces = (nx + 1) * ny * nz + nx * (ny + 1) * nz + nx * ny * (nz + 1)
+    peak_gbs, _ = measured_peaks()
+    for name, a in arms.items():
+        b_step = 4.0 * (8 * n + 8 * faces) + 40.0 * n * a["mean_pcg_iterations"]
+        a["step_roofline"] = {"bytes_per_step": b_step, "achieved_gbs": b_step / (a["ms_per_step"] / 1e3) / 1e9,
+                              "frac": b_step / (a["ms_per_step"] / 1e3) / 1e9 / peak_gbs}
     h = results[headline]
     value = arms[headline]["steps_per_s"]
     # roofline of the dominant kernel (the persistent PCG), from the plain arm

@@ -141,7 +141,7 @@ SIGNATURES = {
     "xs_smoke_reduce_metrics": (_S, [_V, C.POINTER(XsSmokeModel), _V, _V, XsVector, XsVector, _V]),
     "xs_smoke_read_solve_stats": (_S, [_V, C.POINTER(XsSmokeModel), _V, C.c_uint32, C.POINTER(XsSolveStats),
                                        C.POINTER(XsSolveStats)]),
-    "xs_smoke_reset_warm_start": (_S, [_V, C.POINTER(XsSmokeModel), _V]),
+    "xs_smoke_reset_warm_start": (_S, [_V, C.POINTER(XsSmokeModel), _V, C.c_uint32]),
     "xs_smoke_warm_start_fields": (_S, [_V, C.POINTER(XsSmokeModel), _V, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
     "xs_smoke_pressure_fields":(_S, [C.POINTER(XsSmokeModel), _V, C.POINTER(C.c_void_p), C.POINTER(C.c_void_p)]),
     "xs_conv3d_bf16": (_S, [_V, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, C.c_uint32, _V, _V, _V, _V, C.c_uint32,

@@ -364,7 +364,7 @@ XsStatus launch_constrain_vjp(cudaStream_t st, const Grid& g, const uint32_t* ma
 // or reverse-swept (RBGS kind), and the divergence transpose is added.
 XsStatus projection_vjp(cudaStream_t st, const Grid& g, const XsPressureSolve& solve, uint32_t anchor, const uint32_t* mask,
                         const XsAdjointVector& oa, const XsScalarBoundary& pb, double* pa, double* ra, const XsAdjointVector& ua,
-                        void* workspace) {
+                        void* workspace, const WarmHistory* history) {
     project_reverse_cells_kernel<<<blocks_for(cell_count(g)), kBlock, 0, st>>>(g, mask, oa, pa);
     if (check_launch() != XS_OK) return XS_CUDA_ERROR;
     XsStatus s;
@@ -374,7 +374,17 @@ XsStatus projection_vjp(cudaStream_t st, const Grid& g, const XsPressureSolve& s
     } else {
         XsPressureSolve adj = solve;
         adj.initial_guess = nullptr;
+        adj.scale_guess = 0u;
+        const bool ring = history && history->history > 0;
+        if (ring) {
+            // successive adjoint solves of a reverse pass are close: Galerkin
+            // start from the ring of previous adjoint solutions
+            if ((s = galerkin_combine(st, g, anchor, mask, pb, *history, true, nullptr, 0, nullptr, history->ring_start, pa)) != XS_OK)
+                return s;
+            adj.initial_guess = history->ring_start;
+        }
         s = solve_pressure(st, g, adj, anchor, mask, pb, nullptr, pa, nullptr, ra, workspace, nullptr);
+        if (s == XS_OK && ring) s = history_push(st, g, *history, nullptr, ra);
     }
     if (s != XS_OK) return s;
     const uint64_t f0 = face_count(g, 0), f1 = face_count(g, 1), f2 = face_count(g, 2);

@@ -49,7 +49,7 @@ XsStatus launch_constrain_vjp(cudaStream_t st, const Grid& g, const uint32_t* ma
                               const XsAdjointVector& ua);
 XsStatus projection_vjp(cudaStream_t st, const Grid& g, const XsPressureSolve& solve, uint32_t anchor, const uint32_t* mask,
                         const XsAdjointVector& oa, const XsScalarBoundary& pb, double* pa, double* ra, const XsAdjointVector& ua,
-                        void* workspace);
+                        void* workspace, const WarmHistory* history = nullptr);
 
 // tangent.cu
 XsStatus launch_source_jvp_pair(cudaStream_t st, const Grid& g, const uint32_t* mask, const float* rho_t, const float* temp_t,

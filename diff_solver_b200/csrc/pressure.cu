@@ -890,23 +890,37 @@ struct BasisArgs {
     const float* v[M];
     uint32_t history;      // the first `history` entries of v are ring slots
     const uint32_t* meta;  // [0] valid ring vectors, [1] next slot
-    const float* rhs;
+    const float* rhs;      // forward right-hand side (fixed boundary values added), or
+    const double* rhs_d;   // adjoint right-hand side (FP64, no fixed values)
     double* partials;      // [gridDim.x][M(M+1)/2 + M]
 };
 
+// The ring's vectors ordered newest first: ptr[j] for j < history is the j-th
+// newest valid solution (null past the valid count); entries past the ring
+// are the extra vectors.  The basis spans the same space but uses successive
+// differences of the ring, b_0 = r_0, b_j = r_{j-1} - r_j: consecutive
+// solutions are nearly collinear, their differences far less so, which keeps
+// the scaled Gram matrix well conditioned.
 template <int M>
-__device__ __forceinline__ void basis_valid(const BasisArgs<M>& a, bool (&valid)[M]) {
-    const uint32_t count = a.history > 0 ? min(a.meta[0], a.history) : 0u;
+__device__ __forceinline__ void basis_order(const BasisArgs<M>& a, const float* (&ptr)[M], uint32_t& count) {
+    count = a.history > 0 ? min(a.meta[0], a.history) : 0u;
+    const uint32_t head = a.history > 0 ? min(a.meta[1], a.history - 1) : 0u;
 #pragma unroll
-    for (int i = 0; i < M; ++i) valid[i] = i < static_cast<int>(a.history) ? static_cast<uint32_t>(i) < count : a.v[i] != nullptr;
+    for (int j = 0; j < M; ++j) {
+        if (j < static_cast<int>(a.history))
+            ptr[j] = static_cast<uint32_t>(j) < count ? a.v[(head + 2 * a.history - 1 - j) % a.history] : nullptr;
+        else
+            ptr[j] = a.v[j];
+    }
 }
 
 template <int M>
 __global__ void __launch_bounds__(256) basis_gram_kernel(BasisArgs<M> a) {
     constexpr int K = M * (M + 1) / 2 + M;
     __shared__ double red[K * 32];
-    bool valid[M];
-    basis_valid(a, valid);
+    const float* ptr[M];
+    uint32_t count;
+    basis_order(a, ptr, count);
     const Grid& g = a.op.g;
     const uint64_t n = cell_count(g);
     double acc[K];
@@ -917,19 +931,26 @@ __global__ void __launch_bounds__(256) basis_gram_kernel(BasisArgs<M> a) {
         decode(i, g.nx, g.ny, x, y, z);
         CellStencil s;
         if (!stencil(a.op, x, y, z, i, s)) continue;
-        const double b = static_cast<double>(a.rhs[i]) + static_cast<double>(s.fixed_sum);
+        const double b = a.rhs_d ? a.rhs_d[i] : static_cast<double>(a.rhs[i]) + static_cast<double>(s.fixed_sum);
+        double rv[M], ar[M];  // raw vectors and their A products
+#pragma unroll
+        for (int j = 0; j < M; ++j) {
+            rv[j] = 0.0;
+            ar[j] = 0.0;
+            if (ptr[j] == nullptr) continue;
+            rv[j] = ptr[j][i];
+            double q = s.diag * rv[j];
+#pragma unroll
+            for (int f = 0; f < 6; ++f)
+                if ((s.conn >> f) & 1u) { const uint64_t nb = s.nb[f]; if (nb != a.op.anchor) q -= static_cast<double>(ptr[j][nb]); }
+            ar[j] = q;
+        }
         double vi[M], av[M];
 #pragma unroll
         for (int j = 0; j < M; ++j) {
-            vi[j] = 0.0;
-            av[j] = 0.0;
-            if (!valid[j]) continue;
-            vi[j] = a.v[j][i];
-            double q = s.diag * vi[j];
-#pragma unroll
-            for (int f = 0; f < 6; ++f)
-                if ((s.conn >> f) & 1u) { const uint64_t nb = s.nb[f]; if (nb != a.op.anchor) q -= static_cast<double>(a.v[j][nb]); }
-            av[j] = q;
+            const bool diff = j > 0 && j < static_cast<int>(a.history) && static_cast<uint32_t>(j) < count;
+            vi[j] = diff ? rv[j - 1] - rv[j] : rv[j];
+            av[j] = diff ? ar[j - 1] - ar[j] : ar[j];
         }
         int k = 0;
 #pragma unroll
@@ -1003,17 +1024,25 @@ __global__ void basis_solve_kernel(const double* __restrict__ partials, uint32_t
 
 template <int M>
 __global__ void basis_combine_kernel(BasisArgs<M> a, const double* __restrict__ coef, float* __restrict__ x0) {
-    bool valid[M];
-    basis_valid(a, valid);
+    const float* ptr[M];
+    uint32_t count;
+    basis_order(a, ptr, count);
+    // coefficients of the raw vectors: sum_j w_j b_j with b_0 = r_0 and
+    // b_j = r_{j-1} - r_j on the ring gives r_j the weight
+    // (j == 0 ? w_0 : -w_j) + w_{j+1} (if b_{j+1} is a ring difference)
     double w[M];
 #pragma unroll
-    for (int j = 0; j < M; ++j) w[j] = valid[j] ? coef[j] : 0.0;
+    for (int j = 0; j < M; ++j) {
+        if (ptr[j] == nullptr) { w[j] = 0.0; continue; }
+        if (j >= static_cast<int>(a.history)) { w[j] = coef[j]; continue; }
+        w[j] = (j == 0 ? coef[0] : -coef[j]) + (static_cast<uint32_t>(j + 1) < count ? coef[j + 1] : 0.0);
+    }
     const uint64_t n = cell_count(a.op.g);
     for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         double acc = 0.0;
 #pragma unroll
         for (int j = 0; j < M; ++j)
-            if (w[j] != 0.0) acc += w[j] * static_cast<double>(a.v[j][i]);
+            if (w[j] != 0.0) acc += w[j] * static_cast<double>(ptr[j][i]);
         x0[i] = static_cast<float>(acc);
     }
 }
@@ -1042,11 +1071,12 @@ struct HistorySlots {
     float* s[kMaxBasis];
 };
 
-// slot[meta[1]] = pressure
-__global__ void history_push_kernel(const float* __restrict__ pressure, uint64_t n, HistorySlots slots, uint32_t history, const uint32_t* meta) {
+// slot[meta[1]] = pressure (rounded to FP32)
+template <class T>
+__global__ void history_push_kernel(const T* __restrict__ pressure, uint64_t n, HistorySlots slots, uint32_t history, const uint32_t* meta) {
     float* dst = slots.s[min(meta[1], history - 1)];
     for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
-        dst[i] = pressure[i];
+        dst[i] = static_cast<float>(pressure[i]);
 }
 
 __global__ void history_advance_kernel(uint32_t history, uint32_t* meta) {
@@ -1087,7 +1117,7 @@ WarmHistory carve_warm_history(void* base, const Grid& g, uint32_t history) {
 
 template <int M>
 XsStatus galerkin_m(cudaStream_t st, const Operator& op, const WarmHistory& h, uint32_t ring, const float* const* extra, int n_extra,
-                    const float* rhs, float* out) {
+                    const float* rhs, const double* rhs_d, float* out) {
     BasisArgs<M> a{};
     a.op = op;
     for (uint32_t i = 0; i < ring; ++i) a.v[i] = h.slots[i];
@@ -1095,6 +1125,7 @@ XsStatus galerkin_m(cudaStream_t st, const Operator& op, const WarmHistory& h, u
     a.history = ring;
     a.meta = h.meta;
     a.rhs = rhs;
+    a.rhs_d = rhs_d;
     a.partials = h.partials;
     const uint64_t n = cell_count(op.g);
     const unsigned blocks = static_cast<unsigned>(std::min<uint64_t>((n + 255) / 256, kGramBlocks));
@@ -1108,18 +1139,18 @@ XsStatus galerkin_m(cudaStream_t st, const Operator& op, const WarmHistory& h, u
 }
 
 XsStatus galerkin_combine(cudaStream_t st, const Grid& g, uint32_t anchor, const uint32_t* mask, const XsScalarBoundary& pb, const WarmHistory& h,
-                          bool use_ring, const float* const* extra, int n_extra, const float* rhs, float* out) {
+                          bool use_ring, const float* const* extra, int n_extra, const float* rhs, float* out, const double* rhs_d) {
     const uint32_t ring = use_ring ? h.history : 0u;
     const uint32_t m = ring + static_cast<uint32_t>(n_extra);
-    if (m == 0 || m > static_cast<uint32_t>(kMaxBasis) || !h.meta || !out) return XS_INVALID_ARGUMENT;
-    const Operator op{g, mask, anchor, pb, true};
+    if (m == 0 || m > static_cast<uint32_t>(kMaxBasis) || !h.meta || !out || (!rhs && !rhs_d)) return XS_INVALID_ARGUMENT;
+    const Operator op{g, mask, anchor, pb, rhs_d == nullptr};
     switch (m) {
-        case 1: return galerkin_m<1>(st, op, h, ring, extra, n_extra, rhs, out);
-        case 2: return galerkin_m<2>(st, op, h, ring, extra, n_extra, rhs, out);
-        case 3: return galerkin_m<3>(st, op, h, ring, extra, n_extra, rhs, out);
-        case 4: return galerkin_m<4>(st, op, h, ring, extra, n_extra, rhs, out);
-        case 5: return galerkin_m<5>(st, op, h, ring, extra, n_extra, rhs, out);
-        default: return galerkin_m<kMaxBasis>(st, op, h, ring, extra, n_extra, rhs, out);
+        case 1: return galerkin_m<1>(st, op, h, ring, extra, n_extra, rhs, rhs_d, out);
+        case 2: return galerkin_m<2>(st, op, h, ring, extra, n_extra, rhs, rhs_d, out);
+        case 3: return galerkin_m<3>(st, op, h, ring, extra, n_extra, rhs, rhs_d, out);
+        case 4: return galerkin_m<4>(st, op, h, ring, extra, n_extra, rhs, rhs_d, out);
+        case 5: return galerkin_m<5>(st, op, h, ring, extra, n_extra, rhs, rhs_d, out);
+        default: return galerkin_m<kMaxBasis>(st, op, h, ring, extra, n_extra, rhs, rhs_d, out);
     }
 }
 
@@ -1131,13 +1162,16 @@ XsStatus start_residual(cudaStream_t st, const Grid& g, uint32_t anchor, const u
     return check_launch();
 }
 
-XsStatus history_push(cudaStream_t st, const Grid& g, const WarmHistory& h, const float* pressure) {
+XsStatus history_push(cudaStream_t st, const Grid& g, const WarmHistory& h, const float* pressure, const double* pressure64) {
     if (h.history == 0) return XS_OK;
     HistorySlots slots{};
     for (uint32_t i = 0; i < h.history; ++i) slots.s[i] = h.slots[i];
     const uint64_t n = cell_count(g);
-    history_push_kernel<<<static_cast<unsigned>(std::min<uint64_t>((n + 255) / 256, 148 * 16)), 256, 0, st>>>(pressure, n, slots, h.history,
-                                                                                                            h.meta);
+    const unsigned blocks = static_cast<unsigned>(std::min<uint64_t>((n + 255) / 256, 148 * 16));
+    if (pressure64)
+        history_push_kernel<double><<<blocks, 256, 0, st>>>(pressure64, n, slots, h.history, h.meta);
+    else
+        history_push_kernel<float><<<blocks, 256, 0, st>>>(pressure, n, slots, h.history, h.meta);
     XsStatus s = check_launch();
     if (s != XS_OK) return s;
     history_advance_kernel<<<1, 1, 0, st>>>(h.history, h.meta);

@@ -81,14 +81,15 @@ size_t warm_history_bytes(const Grid& g, uint32_t history);
 WarmHistory carve_warm_history(void* base, const Grid& g, uint32_t history);
 // out = the A-norm-optimal combination of the valid ring vectors (use_ring)
 // and the n_extra vectors in `extra`, for the right-hand side rhs (+ fixed
-// boundary values).  out must not be one of the combined vectors.
+// boundary values), or for the FP64 adjoint right-hand side rhs_d (no fixed
+// values) when given.  out must not be one of the combined vectors.
 XsStatus galerkin_combine(cudaStream_t st, const Grid& g, uint32_t anchor, const uint32_t* mask, const XsScalarBoundary& pb, const WarmHistory& h,
-                          bool use_ring, const float* const* extra, int n_extra, const float* rhs, float* out);
+                          bool use_ring, const float* const* extra, int n_extra, const float* rhs, float* out, const double* rhs_d = nullptr);
 // r = b + fixed boundary values - A x
 XsStatus start_residual(cudaStream_t st, const Grid& g, uint32_t anchor, const uint32_t* mask, const XsScalarBoundary& pb, const float* rhs,
                         const float* x, float* r);
-// Stores a solution in the next ring slot.
-XsStatus history_push(cudaStream_t st, const Grid& g, const WarmHistory& h, const float* pressure);
+// Stores a solution (FP32, or FP64 rounded to FP32) in the next ring slot.
+XsStatus history_push(cudaStream_t st, const Grid& g, const WarmHistory& h, const float* pressure, const double* pressure64 = nullptr);
 // Empties the ring.
 XsStatus history_reset(cudaStream_t st, const WarmHistory& h);
 

@@ -85,6 +85,7 @@ struct StepWorkspace {
     double* pressure_a;
     double* rhs_a;
     WarmHistory history;
+    WarmHistory adjoint_history;  // ring of previous adjoint pressure solutions
     size_t bytes;
 };
 
@@ -127,6 +128,7 @@ StepWorkspace carve_step(void* base, const Grid& g, uint32_t mode, uint32_t hist
         w.forced_a = fadj();
         w.pressure_a = static_cast<double*>(take(8 * n));
         w.rhs_a = static_cast<double*>(take(8 * n));
+        w.adjoint_history = carve_warm_history(take(warm_history_bytes(g, history)), g, history);
     }
     w.bytes = off;
     return w;
@@ -366,7 +368,7 @@ XsStatus xs_smoke_vjp_step(cudaStream_t stream, const XsSmokeModel* m, XsState s
     if (s != XS_OK) return s;
     // projection
     s = projection_vjp(stream, g, m->pressure, m->pressure_anchor, m->cell_mask, w.projected_a, m->pressure_boundary, w.pressure_a, w.rhs_a,
-                       w.advected_a, w.solver);
+                       w.advected_a, w.solver, &w.adjoint_history);
     if (s != XS_OK) return s;
     // velocity evolution: constrain, advect, integrate (operators.cpp:152-156)
     s = launch_constrain_vjp(stream, g, m->cell_mask, w.advected_a, m->velocity_boundary, w.raw_a);
@@ -427,10 +429,12 @@ XsStatus xs_smoke_warm_start_fields(cudaStream_t stream, const XsSmokeModel* mod
     return XS_OK;
 }
 
-XsStatus xs_smoke_reset_warm_start(cudaStream_t stream, const XsSmokeModel* model, void* workspace) {
-    if (!valid_model(model) || !workspace) return XS_INVALID_ARGUMENT;
-    const StepWorkspace w = carve_step(workspace, make_grid(model->grid), XS_MODE_FORWARD, model->warm_start_history);
-    return history_reset(stream, w.history);
+XsStatus xs_smoke_reset_warm_start(cudaStream_t stream, const XsSmokeModel* model, void* workspace, uint32_t mode) {
+    if (!valid_model(model) || !workspace || mode > XS_MODE_DIFFERENTIABLE) return XS_INVALID_ARGUMENT;
+    const StepWorkspace w = carve_step(workspace, make_grid(model->grid), mode, model->warm_start_history);
+    const XsStatus s = history_reset(stream, w.history);
+    if (s != XS_OK || mode != XS_MODE_DIFFERENTIABLE) return s;
+    return history_reset(stream, w.adjoint_history);
 }
 
 XsStatus xs_smoke_pressure_fields(const XsSmokeModel* model, void* workspace, float** pressure, float** rhs) {

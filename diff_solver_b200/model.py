@@ -149,7 +149,7 @@ class ExecutionContext:
         """Forgets the previous solutions of the Galerkin warm start (a new
         trajectory starts)."""
         N.check("xs_smoke_reset_warm_start", N.lib().xs_smoke_reset_warm_start(self.stream_handle, C.byref(self.native),
-                                                                                 C.c_void_p(self.workspace.data_ptr())))
+                                                                                 C.c_void_p(self.workspace.data_ptr()), int(self.mode)))
 
     def set_inflow(self, index: int, center=None, radius=None) -> None:
         """Moves or resizes inflow ``index`` for the following steps (the

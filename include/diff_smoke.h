@@ -370,9 +370,12 @@ XsStatus xs_smoke_pressure_fields(const XsSmokeModel* model, void* workspace, fl
  * serves a model that keeps a ring. */
 XsStatus xs_smoke_warm_start_fields(cudaStream_t stream, const XsSmokeModel* model, void* workspace, float** ring_start, float** residual);
 
-/* Empties the ring of previous solutions (model->warm_start_history > 0):
- * after allocating the workspace and when a new trajectory starts. */
-XsStatus xs_smoke_reset_warm_start(cudaStream_t stream, const XsSmokeModel* model, void* workspace);
+/* Empties the rings of previous solutions (model->warm_start_history > 0):
+ * after allocating the workspace and when a new trajectory starts.  A
+ * differentiable workspace (mode) also keeps a ring of previous adjoint
+ * pressure solutions, which starts the adjoint solves of a reverse pass the
+ * same way; both are emptied. */
+XsStatus xs_smoke_reset_warm_start(cudaStream_t stream, const XsSmokeModel* model, void* workspace, uint32_t mode);
 
 /* ------------------------------------------------------------------------ */
 /* learned pressure warm start (no reference counterpart)                    */

@@ -263,7 +263,8 @@ public:
         const std::size_t bytes = xs_smoke_workspace_bytes(&m, static_cast<std::uint32_t>(mode));
         if (bytes == 0) throw std::invalid_argument("invalid smoke configuration");
         ctx.workspace_ = cuda::Buffer<unsigned char>(ctx.resource, bytes);
-        check(xs_smoke_reset_warm_start(ctx.resource->stream(), &m, ctx.workspace_.data), "xs_smoke_reset_warm_start");
+        check(xs_smoke_reset_warm_start(ctx.resource->stream(), &m, ctx.workspace_.data, static_cast<std::uint32_t>(mode)),
+              "xs_smoke_reset_warm_start");
         ctx.resource->synchronize();
         return ctx;
     }
