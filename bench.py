@@ -388,6 +388,7 @@ def main():
     for name, r in results.items():
         arms[name] = {"steps_per_s": steps_total / (r["elapsed_ms"] / 1e3), "ms_per_step": r["elapsed_ms"] / args.steps,
                       "pcg_iterations_per_step": r["iterations"], "mean_pcg_iterations": statistics.mean(r["iterations"]),
+                      "refinement_passes_per_step": r["refinements"],
                       "solve_ms_per_step": statistics.mean(r["solve_ms"]), "initial_residuals": r["initial_residuals"],
                       "final_residuals": r["residuals"], "gpu_launches": r["launches"]}
     # whole-step roofline: B_step = 4 (8 N + 8 F) + 40 N k bytes per step (the

@@ -384,7 +384,7 @@ XsStatus projection_vjp(cudaStream_t st, const Grid& g, const XsPressureSolve& s
             adj.initial_guess = history->ring_start;
         }
         s = solve_pressure(st, g, adj, anchor, mask, pb, nullptr, pa, nullptr, ra, workspace, nullptr);
-        if (s == XS_OK && ring) s = history_push(st, g, *history, nullptr, ra);
+        if (s == XS_OK && ring) s = history_push(st, g, anchor, mask, pb, *history, nullptr, ra);
     }
     if (s != XS_OK) return s;
     const uint64_t f0 = face_count(g, 0), f1 = face_count(g, 1), f2 = face_count(g, 2);

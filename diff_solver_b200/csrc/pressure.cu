@@ -893,6 +893,8 @@ struct BasisArgs {
     const float* rhs;      // forward right-hand side (fixed boundary values added), or
     const double* rhs_d;   // adjoint right-hand side (FP64, no fixed values)
     double* partials;      // [gridDim.x][M(M+1)/2 + M]
+    const float* w[M];     // A v, zero on inactive cells
+    uint32_t fixed_terms;  // the forward b has non-zero fixed boundary values
 };
 
 // The ring's vectors ordered newest first: ptr[j] for j < history is the j-th
@@ -902,48 +904,50 @@ struct BasisArgs {
 // solutions are nearly collinear, their differences far less so, which keeps
 // the scaled Gram matrix well conditioned.
 template <int M>
-__device__ __forceinline__ void basis_order(const BasisArgs<M>& a, const float* (&ptr)[M], uint32_t& count) {
+__device__ __forceinline__ void basis_order(const BasisArgs<M>& a, const float* (&ptr)[M], uint32_t& count, const float* (*wptr)[M] = nullptr) {
     count = a.history > 0 ? min(a.meta[0], a.history) : 0u;
     const uint32_t head = a.history > 0 ? min(a.meta[1], a.history - 1) : 0u;
 #pragma unroll
     for (int j = 0; j < M; ++j) {
-        if (j < static_cast<int>(a.history))
-            ptr[j] = static_cast<uint32_t>(j) < count ? a.v[(head + 2 * a.history - 1 - j) % a.history] : nullptr;
-        else
-            ptr[j] = a.v[j];
+        const bool ring = j < static_cast<int>(a.history);
+        const uint32_t slot = ring ? (head + 2 * a.history - 1 - j) % a.history : static_cast<uint32_t>(j);
+        const bool valid = ring ? static_cast<uint32_t>(j) < count : a.v[j] != nullptr;
+        ptr[j] = valid ? a.v[slot] : nullptr;
+        if (wptr) (*wptr)[j] = valid ? a.w[slot] : nullptr;
     }
 }
 
+// Fixed boundary values entering b at cell i (non-zero only next to a
+// fixed-value face; the solver adds the same sum).
+__device__ __forceinline__ double boundary_fixed_sum(const Operator& op, uint64_t i) {
+    int x, y, z;
+    decode(i, op.g.nx, op.g.ny, x, y, z);
+    CellStencil s;
+    stencil(op, x, y, z, i, s);
+    return s.fixed_sum;
+}
+
+// Streams the vectors and their stored A products: no stencil work here.
 template <int M>
 __global__ void __launch_bounds__(256) basis_gram_kernel(BasisArgs<M> a) {
     constexpr int K = M * (M + 1) / 2 + M;
     __shared__ double red[K * 32];
     const float* ptr[M];
+    const float* wptr[M];
     uint32_t count;
-    basis_order(a, ptr, count);
-    const Grid& g = a.op.g;
-    const uint64_t n = cell_count(g);
+    basis_order(a, ptr, count, &wptr);
+    const uint64_t n = cell_count(a.op.g);
     double acc[K];
 #pragma unroll
     for (int k = 0; k < K; ++k) acc[k] = 0.0;
     for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
-        int x, y, z;
-        decode(i, g.nx, g.ny, x, y, z);
-        CellStencil s;
-        if (!stencil(a.op, x, y, z, i, s)) continue;
-        const double b = a.rhs_d ? a.rhs_d[i] : static_cast<double>(a.rhs[i]) + static_cast<double>(s.fixed_sum);
+        double b = a.rhs_d ? a.rhs_d[i] : static_cast<double>(a.rhs[i]);
+        if (a.fixed_terms) b += boundary_fixed_sum(a.op, i);
         double rv[M], ar[M];  // raw vectors and their A products
 #pragma unroll
         for (int j = 0; j < M; ++j) {
-            rv[j] = 0.0;
-            ar[j] = 0.0;
-            if (ptr[j] == nullptr) continue;
-            rv[j] = ptr[j][i];
-            double q = s.diag * rv[j];
-#pragma unroll
-            for (int f = 0; f < 6; ++f)
-                if ((s.conn >> f) & 1u) { const uint64_t nb = s.nb[f]; if (nb != a.op.anchor) q -= static_cast<double>(ptr[j][nb]); }
-            ar[j] = q;
+            rv[j] = ptr[j] ? static_cast<double>(__ldg(ptr[j] + i)) : 0.0;
+            ar[j] = wptr[j] ? static_cast<double>(__ldg(wptr[j] + i)) : 0.0;
         }
         double vi[M], av[M];
 #pragma unroll
@@ -1071,12 +1075,38 @@ struct HistorySlots {
     float* s[kMaxBasis];
 };
 
-// slot[meta[1]] = pressure (rounded to FP32)
+// (A u)_i of the FP32 rounding of u on the active cells, 0 elsewhere
 template <class T>
-__global__ void history_push_kernel(const T* __restrict__ pressure, uint64_t n, HistorySlots slots, uint32_t history, const uint32_t* meta) {
-    float* dst = slots.s[min(meta[1], history - 1)];
-    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+__device__ __forceinline__ float apply_at(const Operator& op, const T* __restrict__ u, uint64_t i) {
+    int x, y, z;
+    decode(i, op.g.nx, op.g.ny, x, y, z);
+    CellStencil s;
+    if (!stencil(op, x, y, z, i, s)) return 0.0f;
+    double q = s.diag * static_cast<double>(static_cast<float>(u[i]));
+#pragma unroll
+    for (int f = 0; f < 6; ++f)
+        if ((s.conn >> f) & 1u) { const uint64_t nb = s.nb[f]; if (nb != op.anchor) q -= static_cast<double>(static_cast<float>(u[nb])); }
+    return static_cast<float>(q);
+}
+
+// slot[meta[1]] = pressure (rounded to FP32), product[meta[1]] = A slot
+template <class T>
+__global__ void history_push_kernel(Operator op, const T* __restrict__ pressure, HistorySlots slots, HistorySlots products, uint32_t history,
+                                    const uint32_t* meta) {
+    const uint32_t k = min(meta[1], history - 1);
+    float* dst = slots.s[k];
+    float* prod = products.s[k];
+    const uint64_t n = cell_count(op.g);
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         dst[i] = static_cast<float>(pressure[i]);
+        prod[i] = apply_at(op, pressure, i);
+    }
+}
+
+__global__ void apply_operator_kernel(Operator op, const float* __restrict__ u, float* __restrict__ out) {
+    const uint64_t n = cell_count(op.g);
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
+        out[i] = apply_at(op, u, i);
 }
 
 __global__ void history_advance_kernel(uint32_t history, uint32_t* meta) {
@@ -1087,7 +1117,7 @@ __global__ void history_advance_kernel(uint32_t history, uint32_t* meta) {
 size_t warm_history_bytes(const Grid& g, uint32_t history) {
     if (history == 0) return 0;
     const size_t n = cell_count(g);
-    return align_up(256, 256) + (history + 3) * align_up(n * 4, 256) +
+    return align_up(256, 256) + (2 * history + 4) * align_up(n * 4, 256) +
            align_up(sizeof(double) * kGramBlocks * (kMaxBasis * (kMaxBasis + 1) / 2 + kMaxBasis), 256) + 256;
 }
 
@@ -1102,7 +1132,11 @@ WarmHistory carve_warm_history(void* base, const Grid& g, uint32_t history) {
     for (uint32_t i = 0; i < history; ++i) {
         h.slots[i] = reinterpret_cast<float*>(p + off);
         off += align_up(n * 4, 256);
+        h.products[i] = reinterpret_cast<float*>(p + off);
+        off += align_up(n * 4, 256);
     }
+    h.extra_product = reinterpret_cast<float*>(p + off);
+    off += align_up(n * 4, 256);
     h.start = reinterpret_cast<float*>(p + off);
     off += align_up(n * 4, 256);
     h.ring_start = reinterpret_cast<float*>(p + off);
@@ -1120,18 +1154,31 @@ XsStatus galerkin_m(cudaStream_t st, const Operator& op, const WarmHistory& h, u
                     const float* rhs, const double* rhs_d, float* out) {
     BasisArgs<M> a{};
     a.op = op;
-    for (uint32_t i = 0; i < ring; ++i) a.v[i] = h.slots[i];
-    for (int i = 0; i < n_extra; ++i) a.v[ring + i] = extra[i];
+    for (uint32_t i = 0; i < ring; ++i) {
+        a.v[i] = h.slots[i];
+        a.w[i] = h.products[i];
+    }
+    const uint64_t n = cell_count(op.g);
+    const unsigned grid = static_cast<unsigned>(std::min<uint64_t>((n + 255) / 256, 148 * 16));
+    XsStatus s;
+    for (int i = 0; i < n_extra; ++i) {  // at most one extra vector (one product buffer)
+        a.v[ring + i] = extra[i];
+        a.w[ring + i] = h.extra_product;
+        apply_operator_kernel<<<grid, 256, 0, st>>>(op, extra[i], h.extra_product);
+        if ((s = check_launch()) != XS_OK) return s;
+    }
     a.history = ring;
     a.meta = h.meta;
     a.rhs = rhs;
     a.rhs_d = rhs_d;
     a.partials = h.partials;
-    const uint64_t n = cell_count(op.g);
+    a.fixed_terms = 0u;
+    if (!rhs_d)
+        for (int f = 0; f < 6; ++f)
+            if (op.pb.modes[f] == 0u && op.pb.values[f] != 0.0f) a.fixed_terms = 1u;
     const unsigned blocks = static_cast<unsigned>(std::min<uint64_t>((n + 255) / 256, kGramBlocks));
     basis_gram_kernel<M><<<blocks, 256, 0, st>>>(a);
-    XsStatus s = check_launch();
-    if (s != XS_OK) return s;
+    if ((s = check_launch()) != XS_OK) return s;
     basis_solve_kernel<M><<<1, 64, 0, st>>>(h.partials, blocks, h.coef);
     if ((s = check_launch()) != XS_OK) return s;
     basis_combine_kernel<M><<<static_cast<unsigned>(std::min<uint64_t>((n + 255) / 256, 148 * 16)), 256, 0, st>>>(a, h.coef, out);
@@ -1142,7 +1189,7 @@ XsStatus galerkin_combine(cudaStream_t st, const Grid& g, uint32_t anchor, const
                           bool use_ring, const float* const* extra, int n_extra, const float* rhs, float* out, const double* rhs_d) {
     const uint32_t ring = use_ring ? h.history : 0u;
     const uint32_t m = ring + static_cast<uint32_t>(n_extra);
-    if (m == 0 || m > static_cast<uint32_t>(kMaxBasis) || !h.meta || !out || (!rhs && !rhs_d)) return XS_INVALID_ARGUMENT;
+    if (m == 0 || m > static_cast<uint32_t>(kMaxBasis) || n_extra > 1 || !h.meta || !out || (!rhs && !rhs_d)) return XS_INVALID_ARGUMENT;
     const Operator op{g, mask, anchor, pb, rhs_d == nullptr};
     switch (m) {
         case 1: return galerkin_m<1>(st, op, h, ring, extra, n_extra, rhs, rhs_d, out);
@@ -1162,16 +1209,21 @@ XsStatus start_residual(cudaStream_t st, const Grid& g, uint32_t anchor, const u
     return check_launch();
 }
 
-XsStatus history_push(cudaStream_t st, const Grid& g, const WarmHistory& h, const float* pressure, const double* pressure64) {
+XsStatus history_push(cudaStream_t st, const Grid& g, uint32_t anchor, const uint32_t* mask, const XsScalarBoundary& pb, const WarmHistory& h,
+                      const float* pressure, const double* pressure64) {
     if (h.history == 0) return XS_OK;
-    HistorySlots slots{};
-    for (uint32_t i = 0; i < h.history; ++i) slots.s[i] = h.slots[i];
+    HistorySlots slots{}, products{};
+    for (uint32_t i = 0; i < h.history; ++i) {
+        slots.s[i] = h.slots[i];
+        products.s[i] = h.products[i];
+    }
+    const Operator op{g, mask, anchor, pb, pressure64 == nullptr};
     const uint64_t n = cell_count(g);
     const unsigned blocks = static_cast<unsigned>(std::min<uint64_t>((n + 255) / 256, 148 * 16));
     if (pressure64)
-        history_push_kernel<double><<<blocks, 256, 0, st>>>(pressure64, n, slots, h.history, h.meta);
+        history_push_kernel<double><<<blocks, 256, 0, st>>>(op, pressure64, slots, products, h.history, h.meta);
     else
-        history_push_kernel<float><<<blocks, 256, 0, st>>>(pressure, n, slots, h.history, h.meta);
+        history_push_kernel<float><<<blocks, 256, 0, st>>>(op, pressure, slots, products, h.history, h.meta);
     XsStatus s = check_launch();
     if (s != XS_OK) return s;
     history_advance_kernel<<<1, 1, 0, st>>>(h.history, h.meta);

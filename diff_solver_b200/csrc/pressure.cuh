@@ -69,11 +69,13 @@ XsStatus read_solve_stats(cudaStream_t stream, const void* workspace, const Grid
 constexpr int kMaxBasis = 6;
 struct WarmHistory {
     float* slots[kMaxBasis];
+    float* products[kMaxBasis];  // A slot, computed when the slot is written
     uint32_t history;   // ring slots (0: off)
     uint32_t* meta;     // device: [0] valid slots, [1] next slot
     float* start;       // the start vector of the last forward solve (N)
     float* ring_start;  // the Galerkin start from the ring alone (N)
     float* residual;    // b - A ring_start (N)
+    float* extra_product;  // A of the extra vector of a combination (N)
     double* partials;
     double* coef;
 };
@@ -88,8 +90,10 @@ XsStatus galerkin_combine(cudaStream_t st, const Grid& g, uint32_t anchor, const
 // r = b + fixed boundary values - A x
 XsStatus start_residual(cudaStream_t st, const Grid& g, uint32_t anchor, const uint32_t* mask, const XsScalarBoundary& pb, const float* rhs,
                         const float* x, float* r);
-// Stores a solution (FP32, or FP64 rounded to FP32) in the next ring slot.
-XsStatus history_push(cudaStream_t st, const Grid& g, const WarmHistory& h, const float* pressure, const double* pressure64 = nullptr);
+// Stores a solution (FP32, or FP64 rounded to FP32) in the next ring slot,
+// with its product by the operator.
+XsStatus history_push(cudaStream_t st, const Grid& g, uint32_t anchor, const uint32_t* mask, const XsScalarBoundary& pb, const WarmHistory& h,
+                      const float* pressure, const double* pressure64 = nullptr);
 // Empties the ring.
 XsStatus history_reset(cudaStream_t st, const WarmHistory& h);
 

@@ -51,7 +51,7 @@ XsStatus projection_forward(cudaStream_t st, const Grid& g, const XsPressureSolv
     }
     s = solve_pressure(st, g, used, anchor, mask, pb, rhs, nullptr, pressure, nullptr, workspace, &w);
     if (s != XS_OK) return s;
-    if (ring && (s = history_push(st, g, *history, pressure)) != XS_OK) return s;
+    if (ring && (s = history_push(st, g, anchor, mask, pb, *history, pressure)) != XS_OK) return s;
     if (end && cudaEventRecord(end, st) != cudaSuccess) return XS_CUDA_ERROR;
     if (solve.kind == XS_SOLVER_RED_BLACK_GAUSS_SEIDEL) return launch_project(st, g, mask, u, pressure, out);
     return launch_project64(st, g, mask, u, w.x64, out);

@@ -266,6 +266,24 @@ def test_galerkin_history_with_learned_guess(cuda):
     assert sum(s["iterations"] for s in warm_stats) < sum(s["iterations"] for s in plain_stats)
 
 
+def test_trained_network_gain(cuda):
+    """What the committed network (trained at 128^3 on 20k plume pairs) gains
+    on the held-out benchmark plume at 128^3: fewer PCG iterations than the
+    zero start on its own, and fewer than the Galerkin history alone when it
+    corrects the history's start."""
+    import os
+    from diff_solver_b200.warm_start import WarmStartNetwork, evaluate_arms
+    weights = os.path.join(ROOT, "diff_solver_b200", "weights", "warm_start_128.npz")
+    net = WarmStartNetwork((128, 128, 128), factor=1)
+    net.load(weights)
+    arms = evaluate_arms(net, (128, 128, 128), steps=40, history=5)
+    late = {k: float(np.mean(v[20:])) for k, v in arms.items()}
+    print(late)
+    assert late["learned"] < 0.99 * late["plain"], late
+    assert late["learned+history"] < 0.9 * late["history"], late
+    assert late["history"] < 0.6 * late["plain"], late
+
+
 def test_learned_warm_start_inside_a_model_step(cuda):
     """A model carrying the network solves to the same tolerance and gives the
     same step as the plain solver (both within the 1e-6 residual)."""
