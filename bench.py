@@ -311,11 +311,11 @@ def product_run(args, world, rank, local):
     network = None
     if not args.no_learned:
         from diff_solver_b200.warm_start import WarmStartNetwork
-        if not os.path.exists(WEIGHTS):
-            raise FileNotFoundError(f"{WEIGHTS} is missing: train it with python -m diff_solver_b200.train_warm_start")
+        if not os.path.exists(args.weights):
+            raise FileNotFoundError(f"{args.weights} is missing: train it with python -m diff_solver_b200.train_warm_start")
         # trained at 128^3, applied fully convolutionally on the grid restricted x2
         network = WarmStartNetwork(tuple(s // 2 for s in args.shape), factor=2)
-        network.load(WEIGHTS)
+        network.load(args.weights)
     # spin-up from rest with the fastest start; its final state opens every arm
     spin = Rollout(args.shape, HISTORY, network)
     gen = torch.Generator(device="cuda").manual_seed(0)
@@ -351,13 +351,16 @@ def product_run(args, world, rank, local):
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    ap.add_argument("--steps", type=int, default=5)
+    # the warm-started arms' iteration counts vary from step to step (120-550 at
+    # 256^3): 20 timed steps per arm keep the mean within a few per cent
+    ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
     ap.add_argument("--spinup", type=int, default=40, help="steps from rest before the arms start")
     ap.add_argument("--impl", choices=["product", "reference"], default="product")
     ap.add_argument("--grid", default=str(GRID), help="N for N^3, or nx,ny,nz")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="plain and history arms only")
+    ap.add_argument("--weights", default=WEIGHTS, help="warm-start network parameters (.npz)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3

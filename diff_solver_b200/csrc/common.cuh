@@ -62,12 +62,16 @@ __host__ __device__ __forceinline__ uint64_t idx3(int x, int y, int z, int nx, i
     return static_cast<uint64_t>(x) + static_cast<uint64_t>(nx) * (static_cast<uint64_t>(y) + static_cast<uint64_t>(ny) * z);
 }
 
-// operators.cu:49-54
+// operators.cu:49-54.  Every cell or face index of a valid grid is below
+// 2^32 (the extents' product with +1 on each axis is checked on the host), so
+// the divisions run in 32 bits (64-bit integer division is a long software
+// sequence on the GPU).
 __device__ __forceinline__ void decode(uint64_t i, int nx, int ny, int& x, int& y, int& z) {
-    const uint64_t yz = i / static_cast<uint64_t>(nx);
-    x = static_cast<int>(i - yz * nx);
-    const uint64_t zz = yz / static_cast<uint64_t>(ny);
-    y = static_cast<int>(yz - zz * ny);
+    const uint32_t i32 = static_cast<uint32_t>(i);
+    const uint32_t yz = i32 / static_cast<uint32_t>(nx);
+    x = static_cast<int>(i32 - yz * static_cast<uint32_t>(nx));
+    const uint32_t zz = yz / static_cast<uint32_t>(ny);
+    y = static_cast<int>(yz - zz * static_cast<uint32_t>(ny));
     z = static_cast<int>(zz);
 }
 

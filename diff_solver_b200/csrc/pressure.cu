@@ -442,12 +442,15 @@ __device__ void spmv_fast(const PcgArgs& a, const FastGeom& f, int k, float beta
         int32_t left, right;
         float4 d;
         x_geom(f, x0, rg.dyz, left, right, d);
-        float4 po;
+        float4 po, ev;
         float4 c;
         if (kFirst) {
             c = ld4(pnew + i);
         } else {
+            // every load of the group is issued before the first store (the
+            // compiler cannot move the e load across the p store by itself)
             po = ld4(pold + i);
+            ev = ld4(a.e + i);
             c = axpy4(ld4(zv + i), beta, po);
         }
         float4 s = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
@@ -471,8 +474,7 @@ __device__ void spmv_fast(const PcgArgs& a, const FastGeom& f, int k, float beta
         }
         if (!kFirst) {
             st4(pnew + i, c);
-            const float4 e = ld4(a.e + i);
-            st4(a.e + i, axpy4(e, alpha_prev, po));
+            st4(a.e + i, axpy4(ev, alpha_prev, po));
         }
         st4(a.q + i, qv);
         pq += static_cast<double>(c.x) * qv.x + static_cast<double>(c.y) * qv.y + static_cast<double>(c.z) * qv.z +
@@ -881,7 +883,7 @@ XsStatus reverse_rbgs(cudaStream_t stream, const Grid& g, uint32_t sweeps, uint3
 // slot live on the device) and optionally one extra vector (the learned
 // guess).  Dependent vectors are dropped by an LDL^T of the Jacobi-scaled
 // Gram matrix that skips pivots below kBasisPivot.
-constexpr int kGramBlocks = 148 * 4;
+constexpr int kGramBlocks = 148 * 3;  // one wave at 3 blocks per SM
 constexpr double kBasisPivot = 1e-11;
 
 template <int M>
@@ -929,7 +931,7 @@ __device__ __forceinline__ double boundary_fixed_sum(const Operator& op, uint64_
 
 // Streams the vectors and their stored A products: no stencil work here.
 template <int M>
-__global__ void __launch_bounds__(256) basis_gram_kernel(BasisArgs<M> a) {
+__global__ void __launch_bounds__(256, 3) basis_gram_kernel(BasisArgs<M> a) {
     constexpr int K = M * (M + 1) / 2 + M;
     __shared__ double red[K * 32];
     const float* ptr[M];

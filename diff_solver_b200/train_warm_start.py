@@ -41,8 +41,12 @@ def main(argv=None) -> int:
     ap.add_argument("--eval-arms-steps", type=int, default=0,
                     help="steps of the side-by-side run of the plain, history, learned and learned+history starts (0: skip)")
     ap.add_argument("--history", type=int, default=4, help="previous solutions in the Galerkin start of that run")
+    ap.add_argument("--fine-factor", type=int, default=1,
+                    help="generate the pairs on a grid this many times finer and restrict them to the network grid")
     ap.add_argument("--train-history", type=int, default=0,
                     help="train on (residual, correction) pairs of a ring of this many previous solutions (0: (rhs, pressure))")
+    ap.add_argument("--time-inference", action="store_true",
+                    help="only time the network: guess on a grid twice as fine, then predict on its own grid (3 warm-up + 10 timed each)")
     args = ap.parse_args(argv)
 
     import torch
@@ -52,6 +56,33 @@ def main(argv=None) -> int:
     def emit(rec):
         print(json.dumps(rec), flush=True)
 
+    if args.time_inference:
+        from . import _native as N
+        shape = (args.grid,) * 3
+        net = WarmStartNetwork(shape, factor=2)
+        if args.init:
+            net.load(args.init)
+        fine = tuple(2 * s for s in shape)
+        rhs = torch.randn(fine[0] * fine[1] * fine[2], device="cuda")
+        small = torch.randn(shape[0] * shape[1] * shape[2], device="cuda")
+        grid = N.XsGrid(*fine, 1.0 / fine[0], 0.5 / fine[0])
+        for _ in range(3):
+            net.guess(grid, rhs)
+            net.predict(small)
+        torch.cuda.synchronize()
+        ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+        ev[0].record()
+        for _ in range(10):
+            net.guess(grid, rhs)
+        ev[1].record()
+        for _ in range(10):
+            net.predict(small)
+        ev[2].record()
+        torch.cuda.synchronize()
+        net.check()
+        emit({"network_grid": shape, "guess_ms": ev[0].elapsed_time(ev[1]) / 10, "predict_ms": ev[1].elapsed_time(ev[2]) / 10})
+        return 0
+
     shape = (args.grid,) * 3
     net = WarmStartNetwork(shape, max_batch=args.batch, factor=1, seed=args.seed)
     if args.init:
@@ -60,7 +91,8 @@ def main(argv=None) -> int:
     records = []
     if args.pairs > 0:
         records = train_on_plumes(net, pairs=args.pairs, batch=args.batch, learning_rate=args.lr, buffer_size=args.buffer,
-                                  episode_steps=args.episode, seed=args.seed, log=emit, loss=args.loss, history=args.train_history)
+                                  episode_steps=args.episode, seed=args.seed, log=emit, loss=args.loss, history=args.train_history,
+                                  fine_factor=args.fine_factor)
     train_s = time.perf_counter() - t0
     emit({"trained_pairs": args.pairs, "seconds": train_s})
     summary = {"pairs": args.pairs, "train_seconds": train_s, "final_loss": records[-1]["loss"] if records else None}

@@ -216,17 +216,21 @@ class _Plume:
 def train_on_plumes(network: WarmStartNetwork, pairs: int = 20000, batch: int = 8, learning_rate: float = 1e-3,
                     buffer_size: int = 256, episode_steps: int = 200, warmup_pairs: int = 64, seed: int = 0,
                     log: Optional[Callable[[dict], None]] = None, log_every: int = 50, loss: str = "energy",
-                    history: int = 0) -> List[dict]:
-    """Trains ``network`` on ``pairs`` pairs generated by the PCG solver on
-    its own grid: ``batch`` plumes run side by side, each step adds their
-    pairs to a replay buffer of ``buffer_size`` pairs in device memory, and
-    one Adam step runs on ``batch`` pairs drawn from the buffer.  A plume
-    restarts with new random parameters after ``episode_steps`` steps.
+                    history: int = 0, fine_factor: int = 1) -> List[dict]:
+    """Trains ``network`` on ``pairs`` pairs generated by the PCG solver:
+    ``batch`` plumes run side by side, each step adds their pairs to a replay
+    buffer of ``buffer_size`` pairs in device memory, and one Adam step runs
+    on ``batch`` pairs drawn from the buffer.  A plume restarts with new
+    random parameters after ``episode_steps`` steps.
 
     With ``history`` = 0 the pairs are (rhs, pressure) of plain solves; with
     a ring of ``history`` previous solutions they are (b - A x0, p - x0), x0
     the ring's Galerkin start: the correction the network supplies when it
-    serves a model that keeps a ring.  Returns the logged records."""
+    serves a model that keeps a ring.  With ``fine_factor`` f > 1 the plumes
+    run on a grid f times the network's and both members of a pair are
+    restricted to the network grid by summing the f^3 children (the
+    restriction the solver applies to the network's input).  Returns the
+    logged records."""
     if network.max_batch < batch:
         raise ValueError(f"the network was created for batches of at most {network.max_batch}")
     rng = np.random.default_rng(seed)
@@ -234,7 +238,15 @@ def train_on_plumes(network: WarmStartNetwork, pairs: int = 20000, batch: int = 
     stream = network.stream
     n = network.cells
     dev = torch.device("cuda")
-    plumes = [_Plume(network.shape, rng, sampler, stream, history=history) for _ in range(batch)]
+    f = int(fine_factor)
+    fine_shape = tuple(f * s for s in network.shape)
+    plumes = [_Plume(fine_shape, rng, sampler, stream, history=history) for _ in range(batch)]
+
+    def coarse(v):
+        if f == 1:
+            return v
+        nx, ny, nz = network.shape
+        return v.view(nz, f, ny, f, nx, f).sum(dim=(1, 3, 5)).reshape(-1)
     network.set_loss(loss, plumes[0].ctx.native.pressure_boundary)
     # stagger the episodes so the buffer mixes early and developed plumes
     for i, p in enumerate(plumes):
@@ -256,11 +268,11 @@ def train_on_plumes(network: WarmStartNetwork, pairs: int = 20000, batch: int = 
                     continue
                 if history:
                     x0, r0 = p.ctx.warm_start_fields()
-                    buf_rhs[head].copy_(r0)
-                    torch.sub(pressure, x0, out=buf_p[head])
+                    buf_rhs[head].copy_(coarse(r0))
+                    buf_p[head].copy_(coarse(pressure - x0))
                 else:
-                    buf_rhs[head].copy_(rhs)
-                    buf_p[head].copy_(pressure)
+                    buf_rhs[head].copy_(coarse(rhs))
+                    buf_p[head].copy_(coarse(pressure))
                 head = (head + 1) % buffer_size
                 filled = min(filled + 1, buffer_size)
                 generated += 1
