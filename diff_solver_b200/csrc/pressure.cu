@@ -55,6 +55,8 @@ PressureWorkspace carve_pressure_workspace(void* base, const Grid& g) {
     w.p1 = static_cast<float*>(take(sizeof(float) * n));
     w.q = static_cast<float*>(take(sizeof(float) * n));
     w.e = static_cast<float*>(take(sizeof(float) * n));
+    w.s = static_cast<float*>(take(sizeof(float) * n));
+    w.y = static_cast<float*>(take(sizeof(float) * n));
     w.bytes = off;
     return w;
 }
@@ -204,6 +206,8 @@ struct PcgArgs {
     float* p[2];
     float* q;
     float* e;
+    float* s;             // smoothed residual (smooth != 0)
+    float* y;             // smoothed correction (smooth != 0)
     float* pressure_out;  // FP32 copy of the solution (null: none)
     double* solution_out; // FP64 copy of the solution (null: none)
     double* partials;
@@ -212,6 +216,7 @@ struct PcgArgs {
     uint32_t max_iterations;
     FastGeom fast;
     uint32_t use_fast;
+    uint32_t smooth;      // minimal-residual smoothing of the iterates (warm starts)
 };
 
 enum ResidualMode { kFromZero = 0, kFromGuess = 1, kFromX64 = 2 };
@@ -255,6 +260,7 @@ __device__ void residual_phase(const PcgArgs& a, int mode, double (&v)[3], doubl
         const bool act = stencil(a.op, x, y, z, i, s);
         if (!act) {
             a.z[i] = 0.0f; a.p[0][i] = 0.0f; a.e[i] = 0.0f;
+            if (a.smooth) { a.s[i] = 0.0f; a.y[i] = 0.0f; }
             if (mode != kFromX64) a.x64[i] = 0.0;
             if (a.pressure_out) a.pressure_out[i] = 0.0f;
             if (a.solution_out) a.solution_out[i] = 0.0;
@@ -285,6 +291,10 @@ __device__ void residual_phase(const PcgArgs& a, int mode, double (&v)[3], doubl
         a.z[i] = zf;
         a.p[0][i] = zf;
         a.e[i] = 0.0f;
+        if (a.smooth) {  // the smoothed sequence starts at the pass' start
+            a.s[i] = zf * s.diag;
+            a.y[i] = 0.0f;
+        }
         if (a.pressure_out) a.pressure_out[i] = static_cast<float>(xi);
         if (a.solution_out) a.solution_out[i] = xi;
         v[0] += b * b;
@@ -295,7 +305,10 @@ __device__ void residual_phase(const PcgArgs& a, int mode, double (&v)[3], doubl
 
 // Iteration k: p_k = z + beta p_{k-1} (k > 0), q = A p_k, e += alpha_{k-1} p_{k-1};
 // partial p_k.q.
-__device__ void spmv_phase(const PcgArgs& a, int k, float beta, float alpha_prev, double& pq) {
+// With smoothing (k > 0): s_k = s_{k-1} + eta (r_k - s_{k-1}) and
+// y_k = y_{k-1} + eta (e_k - y_{k-1}), r_k = z_k diag, e_k the updated e.
+template <bool kSmooth>
+__device__ void spmv_phase(const PcgArgs& a, int k, float beta, float alpha_prev, float eta, bool smooth, double& pq) {
     const Grid& g = a.op.g;
     const uint64_t n = cell_count(g);
     const float* pold = a.p[(k + 1) & 1];
@@ -320,13 +333,20 @@ __device__ void spmv_phase(const PcgArgs& a, int k, float beta, float alpha_prev
                 if ((s.conn >> f) & 1u) acc += pnew[s.nb[f]];
         } else {
             const float po = pold[i];
-            pc = a.z[i] + beta * po;
+            const float zc = a.z[i];
+            pc = zc + beta * po;
             acc = 0.0f;
 #pragma unroll
             for (int f = 0; f < 6; ++f)
                 if ((s.conn >> f) & 1u) { const uint64_t j = s.nb[f]; acc += a.z[j] + beta * pold[j]; }
             pnew[i] = pc;
-            a.e[i] += alpha_prev * po;
+            const float en = a.e[i] + alpha_prev * po;
+            a.e[i] = en;
+            if (kSmooth && smooth) {
+                const float sv = a.s[i], yv = a.y[i];
+                a.s[i] = sv + eta * (zc * s.diag - sv);
+                a.y[i] = yv + eta * (en - yv);
+            }
         }
         const float qv = s.diag * pc - acc;
         a.q[i] = qv;
@@ -335,10 +355,13 @@ __device__ void spmv_phase(const PcgArgs& a, int k, float beta, float alpha_prev
 }
 
 // z -= alpha q / diag; partial {r.z, r.r} with r = z diag.
-__device__ void update_phase(const PcgArgs& a, float alpha, double (&v)[2]) {
+// z -= alpha q / diag; partial {r.z, r.r, s.r, s.s} with r = z diag (the last
+// two with smoothing only).
+template <bool kSmooth>
+__device__ void update_phase(const PcgArgs& a, float alpha, bool smooth, double (&v)[4]) {
     const Grid& g = a.op.g;
     const uint64_t n = cell_count(g);
-    v[0] = v[1] = 0.0;
+    v[0] = v[1] = v[2] = v[3] = 0.0;
     for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         int x, y, z;
         decode(i, g.nx, g.ny, x, y, z);
@@ -349,6 +372,11 @@ __device__ void update_phase(const PcgArgs& a, float alpha, double (&v)[2]) {
         const double r = static_cast<double>(zn) * s.diag;
         v[0] += r * static_cast<double>(zn);
         v[1] += r * r;
+        if (kSmooth && smooth) {
+            const double sv = a.s[i];
+            v[2] += sv * r;
+            v[3] += sv * sv;
+        }
     }
 }
 
@@ -359,6 +387,18 @@ __device__ void fold_phase(const PcgArgs& a, int k, float alpha) {
     const float* pk = a.p[k & 1];
     for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         a.x64[i] += static_cast<double>(a.e[i]) + static_cast<double>(alpha) * static_cast<double>(pk[i]);
+    }
+}
+
+// The smoothed iterate: x64 += y_k + eta (e_k + alpha p_k - y_k).
+__device__ void fold_smoothed_phase(const PcgArgs& a, int k, float alpha, double eta) {
+    const Grid& g = a.op.g;
+    const uint64_t n = cell_count(g);
+    const float* pk = a.p[k & 1];
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        const double xk = static_cast<double>(a.e[i]) + static_cast<double>(alpha) * static_cast<double>(pk[i]);
+        const double yk = a.y[i];
+        a.x64[i] += yk + eta * (xk - yk);
     }
 }
 
@@ -424,8 +464,8 @@ __device__ __forceinline__ float4 axpy4(const float4& a, float b, const float4& 
 }
 
 // spmv_phase for the fast path.
-template <bool kFirst>
-__device__ void spmv_fast(const PcgArgs& a, const FastGeom& f, int k, float beta, float alpha_prev, double& pq) {
+template <bool kFirst, bool kSmooth>
+__device__ void spmv_fast(const PcgArgs& a, const FastGeom& f, int k, float beta, float alpha_prev, float eta, bool smooth, double& pq) {
     const float* zv = a.z;
     const float* pold = a.p[(k + 1) & 1];
     float* pnew = a.p[k & 1];
@@ -442,7 +482,7 @@ __device__ void spmv_fast(const PcgArgs& a, const FastGeom& f, int k, float beta
         int32_t left, right;
         float4 d;
         x_geom(f, x0, rg.dyz, left, right, d);
-        float4 po, ev;
+        float4 po, ev, zc, sv, yv;
         float4 c;
         if (kFirst) {
             c = ld4(pnew + i);
@@ -451,7 +491,12 @@ __device__ void spmv_fast(const PcgArgs& a, const FastGeom& f, int k, float beta
             // compiler cannot move the e load across the p store by itself)
             po = ld4(pold + i);
             ev = ld4(a.e + i);
-            c = axpy4(ld4(zv + i), beta, po);
+            zc = ld4(zv + i);
+            if (kSmooth && smooth) {
+                sv = ld4(a.s + i);
+                yv = ld4(a.y + i);
+            }
+            c = axpy4(zc, beta, po);
         }
         float4 s = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 #pragma unroll
@@ -474,7 +519,14 @@ __device__ void spmv_fast(const PcgArgs& a, const FastGeom& f, int k, float beta
         }
         if (!kFirst) {
             st4(pnew + i, c);
-            st4(a.e + i, axpy4(ev, alpha_prev, po));
+            const float4 en = axpy4(ev, alpha_prev, po);
+            st4(a.e + i, en);
+            if (kSmooth && smooth) {  // s += eta (z diag - s); y += eta (e - y)
+                st4(a.s + i, make_float4(sv.x + eta * (zc.x * d.x - sv.x), sv.y + eta * (zc.y * d.y - sv.y), sv.z + eta * (zc.z * d.z - sv.z),
+                                         sv.w + eta * (zc.w * d.w - sv.w)));
+                st4(a.y + i, make_float4(yv.x + eta * (en.x - yv.x), yv.y + eta * (en.y - yv.y), yv.z + eta * (en.z - yv.z),
+                                         yv.w + eta * (en.w - yv.w)));
+            }
         }
         st4(a.q + i, qv);
         pq += static_cast<double>(c.x) * qv.x + static_cast<double>(c.y) * qv.y + static_cast<double>(c.z) * qv.z +
@@ -485,8 +537,9 @@ __device__ void spmv_fast(const PcgArgs& a, const FastGeom& f, int k, float beta
 // update_phase for the fast path.  (Recomputing q = A p_k here instead of
 // storing it saves 4 B/cell, but measured slower on B200: 183 vs 167 ms per
 // 1329-iteration solve at 256^3, from the extra stencil loads and spills.)
-__device__ void update_fast(const PcgArgs& a, const FastGeom& f, float alpha, double (&v)[2]) {
-    v[0] = v[1] = 0.0;
+template <bool kSmooth>
+__device__ void update_fast(const PcgArgs& a, const FastGeom& f, float alpha, bool smooth, double (&v)[4]) {
+    v[0] = v[1] = v[2] = v[3] = 0.0;
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < f.groups; t += gridDim.x * blockDim.x) {
         const uint32_t i = 4u * t;
         const uint32_t row = fastdiv(i, f.dnx);
@@ -499,6 +552,8 @@ __device__ void update_fast(const PcgArgs& a, const FastGeom& f, float alpha, do
         x_geom(f, x0, rg.dyz, left, right, d);
         float4 zz = ld4(a.z + i);
         const float4 q = ld4(a.q + i);
+        float4 sv;
+        if (kSmooth && smooth) sv = ld4(a.s + i);
         zz.x -= alpha * q.x / d.x;
         zz.y -= alpha * q.y / d.y;
         zz.z -= alpha * q.z / d.z;
@@ -508,12 +563,17 @@ __device__ void update_fast(const PcgArgs& a, const FastGeom& f, float alpha, do
                      r3 = static_cast<double>(zz.w) * d.w;
         v[0] += r0 * zz.x + r1 * zz.y + r2 * zz.z + r3 * zz.w;
         v[1] += r0 * r0 + r1 * r1 + r2 * r2 + r3 * r3;
+        if (kSmooth && smooth) {
+            v[2] += r0 * sv.x + r1 * sv.y + r2 * sv.z + r3 * sv.w;
+            v[3] += static_cast<double>(sv.x) * sv.x + static_cast<double>(sv.y) * sv.y + static_cast<double>(sv.z) * sv.z +
+                    static_cast<double>(sv.w) * sv.w;
+        }
     }
 }
 
 constexpr uint32_t kMaxRefinements = 4;
 
-template <bool kFast>
+template <bool kFast, bool kSmooth>
 __global__ void __launch_bounds__(kBlock, 4) pcg_kernel(PcgArgs a) {
     __shared__ double red[4 * 32];
     SolverState* st = a.st;
@@ -540,6 +600,12 @@ __global__ void __launch_bounds__(kBlock, 4) pcg_kernel(PcgArgs a) {
     }
     const double initial = bb > 0.0 ? sqrt(rr / bb) : 0.0;
     const double target2 = a.tol * a.tol * bb;
+    // Smoothing pays off from a good start (relative residual below 0.1:
+    // 2-4x fewer iterations measured at 128^3); from a poor one it saves a
+    // few per cent of the iterations for 16 more bytes per cell and
+    // iteration.  A dropped guess, or one no better than zero (an empty
+    // history), makes this the plain solve.
+    const bool smooth_run = kSmooth && warm != 0u && rr < 0.01 * bb;
     uint32_t iterations = 0, refinements = 0;
     uint32_t status = XS_OK;
     while (true) {
@@ -550,37 +616,57 @@ __global__ void __launch_bounds__(kBlock, 4) pcg_kernel(PcgArgs a) {
             status = XS_OK;
             break;
         }
-        // one CG pass on the current residual (z, p0 set, e = 0)
+        // one CG pass on the current residual (z, p0 set, e = 0; with smoothing
+        // s = r, y = 0).  Minimal-residual smoothing (Schoenauer; Zhou and
+        // Walker): y_k = y_{k-1} + eta_k (x_k - y_{k-1}) with eta_k minimising
+        // the norm of s_k = b - A y_k.  From a warm start the CG residual
+        // plateaus just above the tolerance for many iterations while the
+        // smoothed residual crosses it far earlier; the pass ends when
+        // either does and keeps the iterate whose residual did.
         int k = 0;
-        float beta = 0.0f, alpha = 0.0f;
-        bool broke = false;
+        float beta = 0.0f, alpha = 0.0f, eta = 0.0f;
+        double eta_final = 0.0;
+        bool broke = false, smoothed = false;
         while (true) {
             double pq[1];
             if (kFast) {
-                if (k == 0) spmv_fast<true>(a, a.fast, k, beta, alpha, pq[0]);
-                else spmv_fast<false>(a, a.fast, k, beta, alpha, pq[0]);
+                if (k == 0) spmv_fast<true, kSmooth>(a, a.fast, k, beta, alpha, eta, smooth_run, pq[0]);
+                else spmv_fast<false, kSmooth>(a, a.fast, k, beta, alpha, eta, smooth_run, pq[0]);
             } else {
-                spmv_phase(a, k, beta, alpha, pq[0]);
+                spmv_phase<kSmooth>(a, k, beta, alpha, eta, smooth_run, pq[0]);
             }
             if (!grid_reduce<1>(st, a.partials, pq, red)) return;
             if (!(pq[0] > 0.0) || !isfinite(pq[0])) { broke = true; break; }
             alpha = static_cast<float>(rz / pq[0]);
-            double v2[2];
-            if (kFast) update_fast(a, a.fast, alpha, v2);
-            else update_phase(a, alpha, v2);
-            if (!grid_reduce<2>(st, a.partials, v2, red)) return;
+            double v4[4];
+            if (kFast) update_fast<kSmooth>(a, a.fast, alpha, smooth_run, v4);
+            else update_phase<kSmooth>(a, alpha, smooth_run, v4);
+            if (!grid_reduce<4>(st, a.partials, v4, red)) return;
             ++iterations;
-            beta = static_cast<float>(v2[0] / rz);
-            rz = v2[0];
-            if (!isfinite(v2[1])) { broke = true; break; }
-            if (v2[1] <= target2 || iterations >= a.max_iterations) break;
+            beta = static_cast<float>(v4[0] / rz);
+            rz = v4[0];
+            if (!isfinite(v4[1])) { broke = true; break; }
+            if (v4[1] <= target2 || iterations >= a.max_iterations) break;
+            if (smooth_run) {
+                // s.s, s.r, r.r -> eta and the norm of the next smoothed residual
+                const double den = v4[1] - 2.0 * v4[2] + v4[3];
+                const double e = den > 0.0 ? (v4[3] - v4[2]) / den : 0.0;
+                const double ss = v4[3] + 2.0 * e * (v4[2] - v4[3]) + e * e * den;
+                eta = static_cast<float>(e);
+                if (ss <= target2 && isfinite(ss)) {
+                    smoothed = true;
+                    eta_final = e;
+                    break;
+                }
+            }
             ++k;
         }
         if (broke) {
             status = XS_NUMERICAL_ERROR;
             break;
         }
-        fold_phase(a, k, alpha);
+        if (smoothed) fold_smoothed_phase(a, k, alpha, eta_final);
+        else fold_phase(a, k, alpha);
         if (!grid_barrier(st, a.partials, red)) return;
         residual_phase(a, kFromX64, v3);
         if (!grid_reduce<3>(st, a.partials, v3, red)) return;
@@ -773,10 +859,16 @@ XsStatus device_limits(DeviceLimits& out) {
     if (dev != cached_device) {
         DeviceLimits l;
         if (cudaDeviceGetAttribute(&l.sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return XS_CUDA_ERROR;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&l.pcg_blocks_per_sm, pcg_kernel<false>, kBlock, 0) != cudaSuccess)
+        // the smoothing variants have the same register cap (launch bounds);
+        // the smaller occupancy of the two sizes both grids
+        int a0 = 0, a1 = 0, b0 = 0, b1 = 0;
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a0, pcg_kernel<false, false>, kBlock, 0) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a1, pcg_kernel<false, true>, kBlock, 0) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, pcg_kernel<true, false>, kBlock, 0) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, pcg_kernel<true, true>, kBlock, 0) != cudaSuccess)
             return XS_CUDA_ERROR;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&l.pcg_fast_blocks_per_sm, pcg_kernel<true>, kBlock, 0) != cudaSuccess)
-            return XS_CUDA_ERROR;
+        l.pcg_blocks_per_sm = std::min(a0, a1);
+        l.pcg_fast_blocks_per_sm = std::min(b0, b1);
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&l.rbgs_blocks_per_sm, rbgs_kernel, kBlock, 0) != cudaSuccess) return XS_CUDA_ERROR;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&l.rev_blocks_per_sm, rbgs_reverse_kernel, kBlock, 0) != cudaSuccess)
             return XS_CUDA_ERROR;
@@ -830,6 +922,11 @@ XsStatus solve_pressure(cudaStream_t stream, const Grid& g, const XsPressureSolv
     a.rhs_d = rhs_d;
     a.guess = solve.initial_guess;
     a.scale_guess = solve.scale_guess;
+    // residual smoothing pays off from warm starts (2-4x fewer iterations at
+    // 128^3); from zero it saves ~4 % of the iterations for 44 % more traffic
+    a.smooth = solve.initial_guess != nullptr ? 1u : 0u;
+    a.s = w.s;
+    a.y = w.y;
     a.x64 = w.x64;
     a.z = w.z;
     a.p[0] = w.p0;
@@ -860,8 +957,12 @@ XsStatus solve_pressure(cudaStream_t stream, const Grid& g, const XsPressureSolv
             f.kind[face] = per ? 2u : (pb.modes[face] == 0u ? 1u : 0u);
         }
     }
-    if (a.use_fast) return launch_cooperative(pcg_kernel<true>, persistent_blocks(lim.pcg_fast_blocks_per_sm, lim.sms, n / 4), a, stream);
-    return launch_cooperative(pcg_kernel<false>, persistent_blocks(lim.pcg_blocks_per_sm, lim.sms, n), a, stream);
+    const unsigned fast_blocks = persistent_blocks(lim.pcg_fast_blocks_per_sm, lim.sms, n / 4);
+    const unsigned blocks = persistent_blocks(lim.pcg_blocks_per_sm, lim.sms, n);
+    if (a.use_fast)
+        return a.smooth ? launch_cooperative(pcg_kernel<true, true>, fast_blocks, a, stream)
+                        : launch_cooperative(pcg_kernel<true, false>, fast_blocks, a, stream);
+    return a.smooth ? launch_cooperative(pcg_kernel<false, true>, blocks, a, stream) : launch_cooperative(pcg_kernel<false, false>, blocks, a, stream);
 }
 
 XsStatus reverse_rbgs(cudaStream_t stream, const Grid& g, uint32_t sweeps, uint32_t anchor, const uint32_t* mask,

@@ -27,6 +27,8 @@ struct PressureWorkspace {
     float* p1;
     float* q;
     float* e;     // FP32 correction of the current CG pass
+    float* s;     // minimal-residual smoothed residual (warm starts)
+    float* y;     // smoothed correction (warm starts)
     size_t bytes;
 };
 

@@ -38,7 +38,7 @@ constexpr size_t round256(size_t v) { return (v + 255) / 256 * 256; }
 constexpr uint64_t kStaticMaxCells = XS_STATIC_SOLVE_MAX_CELLS;
 // Same carving as carve_pressure_workspace for the largest admitted grid.
 constexpr size_t kStaticBytes = round256(sizeof(SolverState)) + round256(sizeof(double) * kPartialSlots * kMaxPersistentBlocks) +
-                                round256(sizeof(double) * kStaticMaxCells) + 5 * round256(sizeof(float) * kStaticMaxCells);
+                                round256(sizeof(double) * kStaticMaxCells) + 7 * round256(sizeof(float) * kStaticMaxCells);
 
 static __device__ __align__(256) unsigned char g_static_scratch[kStaticBytes];
 

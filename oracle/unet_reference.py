@@ -100,7 +100,7 @@ def apply_operator(u, modes):
                 acc = acc + torch.roll(u, shifts=-1 if side else 1, dims=axis)
                 diag = diag + 1.0
                 continue
-            idx = torch.arange(n)
+            idx = torch.arange(n, device=u.device)
             inside = ((idx + 1 < n) if side else (idx - 1 >= 0)).to(u.dtype)
             shape = [1, 1, 1, 1]
             shape[axis] = n
