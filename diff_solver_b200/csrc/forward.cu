@@ -195,7 +195,9 @@ __global__ void constrain_kernel(Grid g, FaceSpace fs, const uint32_t* __restric
 // Advection and constraint fused (operators.cu:381-388 then :466-481): the
 // constrained output is written directly; a periodic face at the upper end
 // takes the advected value of its wrapped partner at coordinate 0.
-__global__ void advect_constrain_kernel(Grid g, FaceSpace fs, const uint32_t* __restrict__ mask, XsVector col, XsVector u,
+// Latency-bound on its ~56 L1 gathers per face: the launch bounds trade a few
+// registers for a fourth resident block per SM.
+__global__ void __launch_bounds__(kBlock, 4) advect_constrain_kernel(Grid g, FaceSpace fs, const uint32_t* __restrict__ mask, XsVector col, XsVector u,
                                         XsVelocityBoundary b, XsVector out) {
     const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= fs.total()) return;
@@ -234,7 +236,7 @@ __global__ void advect_scalar_kernel(Grid g, const uint32_t* __restrict__ mask, 
 
 // Density and temperature advected along one shared trace (the reference
 // traces twice, model.cpp:347-348).
-__global__ void advect_scalar_pair_kernel(Grid g, const uint32_t* __restrict__ mask, const float* __restrict__ col_rho,
+__global__ void __launch_bounds__(kBlock, 5) advect_scalar_pair_kernel(Grid g, const uint32_t* __restrict__ mask, const float* __restrict__ col_rho,
                                           const float* __restrict__ col_temp, const float* __restrict__ src_rho,
                                           const float* __restrict__ src_temp, XsVector u, XsScalarBoundary rb,
                                           XsScalarBoundary tb, XsVelocityBoundary vb, float* __restrict__ out_rho,
