@@ -303,12 +303,17 @@ __device__ void residual_phase(const PcgArgs& a, int mode, double (&v)[3], doubl
     }
 }
 
+// Smoothing state of a CG pass: off, starting (this spmv begins the smoothed
+// sequence at the current iterate), or active.
+enum SmoothMode { kSmoothOff = 0, kSmoothStart = 1, kSmoothActive = 2 };
+
 // Iteration k: p_k = z + beta p_{k-1} (k > 0), q = A p_k, e += alpha_{k-1} p_{k-1};
 // partial p_k.q.
-// With smoothing (k > 0): s_k = s_{k-1} + eta (r_k - s_{k-1}) and
-// y_k = y_{k-1} + eta (e_k - y_{k-1}), r_k = z_k diag, e_k the updated e.
+// With smoothing active (k > 0): s_k = s_{k-1} + eta (r_k - s_{k-1}) and
+// y_k = y_{k-1} + eta (e_k - y_{k-1}), r_k = z_k diag, e_k the updated e;
+// starting: s_k = r_k, y_k = e_k.
 template <bool kSmooth>
-__device__ void spmv_phase(const PcgArgs& a, int k, float beta, float alpha_prev, float eta, bool smooth, double& pq) {
+__device__ void spmv_phase(const PcgArgs& a, int k, float beta, float alpha_prev, float eta, int smooth, double& pq) {
     const Grid& g = a.op.g;
     const uint64_t n = cell_count(g);
     const float* pold = a.p[(k + 1) & 1];
@@ -342,10 +347,13 @@ __device__ void spmv_phase(const PcgArgs& a, int k, float beta, float alpha_prev
             pnew[i] = pc;
             const float en = a.e[i] + alpha_prev * po;
             a.e[i] = en;
-            if (kSmooth && smooth) {
+            if (kSmooth && smooth == kSmoothActive) {
                 const float sv = a.s[i], yv = a.y[i];
                 a.s[i] = sv + eta * (zc * s.diag - sv);
                 a.y[i] = yv + eta * (en - yv);
+            } else if (kSmooth && smooth == kSmoothStart) {
+                a.s[i] = zc * s.diag;
+                a.y[i] = en;
             }
         }
         const float qv = s.diag * pc - acc;
@@ -463,17 +471,41 @@ __device__ __forceinline__ float4 axpy4(const float4& a, float b, const float4& 
     return make_float4(fmaf(b, x.x, a.x), fmaf(b, x.y, a.y), fmaf(b, x.z, a.z), fmaf(b, x.w, a.w));
 }
 
-// spmv_phase for the fast path.
+// spmv_phase for the fast path.  The centre vectors of the thread's next
+// group are loaded before this group's stores (software prefetch, as in
+// update_fast); the stores go to p_k, e, q, s and y, none of which this
+// phase reads at another group.
 template <bool kFirst, bool kSmooth>
-__device__ void spmv_fast(const PcgArgs& a, const FastGeom& f, int k, float beta, float alpha_prev, float eta, bool smooth, double& pq) {
+__device__ void spmv_fast(const PcgArgs& a, const FastGeom& f, int k, float beta, float alpha_prev, float eta, int smooth, double& pq) {
     const float* zv = a.z;
     const float* pold = a.p[(k + 1) & 1];
     float* pnew = a.p[k & 1];
     pq = 0.0;
     auto value4 = [&](uint32_t j) -> float4 { return kFirst ? ld4(pnew + j) : axpy4(ld4(zv + j), beta, ld4(pold + j)); };
     auto value1 = [&](uint32_t j) -> float { return kFirst ? pnew[j] : fmaf(beta, pold[j], zv[j]); };
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < f.groups; t += gridDim.x * blockDim.x) {
+    const bool active = kSmooth && smooth == kSmoothActive;
+    const float4 zero4 = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+    float4 pn = zero4, en_next = zero4, zn = zero4, sn = zero4, yn = zero4;  // the next group's centre values
+    auto fetch = [&](uint32_t j) {
+        if (kFirst) {
+            pn = ld4(pnew + j);
+        } else {
+            pn = ld4(pold + j);
+            en_next = ld4(a.e + j);
+            zn = ld4(zv + j);
+            if (active) {
+                sn = ld4(a.s + j);
+                yn = ld4(a.y + j);
+            }
+        }
+    };
+    const uint32_t stride = gridDim.x * blockDim.x;
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t < f.groups) fetch(4u * t);
+    for (; t < f.groups; t += stride) {
         const uint32_t i = 4u * t;
+        const float4 po = pn, ev = en_next, zc = zn, sv = sn, yv = yn;
+        if (t + stride < f.groups) fetch(i + 4u * stride);
         const uint32_t row = fastdiv(i, f.dnx);
         const uint32_t x0 = i - row * f.nx;
         const uint32_t z = fastdiv(row, f.dny);
@@ -482,22 +514,7 @@ __device__ void spmv_fast(const PcgArgs& a, const FastGeom& f, int k, float beta
         int32_t left, right;
         float4 d;
         x_geom(f, x0, rg.dyz, left, right, d);
-        float4 po, ev, zc, sv, yv;
-        float4 c;
-        if (kFirst) {
-            c = ld4(pnew + i);
-        } else {
-            // every load of the group is issued before the first store (the
-            // compiler cannot move the e load across the p store by itself)
-            po = ld4(pold + i);
-            ev = ld4(a.e + i);
-            zc = ld4(zv + i);
-            if (kSmooth && smooth) {
-                sv = ld4(a.s + i);
-                yv = ld4(a.y + i);
-            }
-            c = axpy4(zc, beta, po);
-        }
+        const float4 c = kFirst ? po : axpy4(zc, beta, po);
         float4 s = make_float4(0.0f, 0.0f, 0.0f, 0.0f);
 #pragma unroll
         for (int q = 0; q < 4; ++q) {
@@ -521,11 +538,14 @@ __device__ void spmv_fast(const PcgArgs& a, const FastGeom& f, int k, float beta
             st4(pnew + i, c);
             const float4 en = axpy4(ev, alpha_prev, po);
             st4(a.e + i, en);
-            if (kSmooth && smooth) {  // s += eta (z diag - s); y += eta (e - y)
+            if (active) {  // s += eta (z diag - s); y += eta (e - y)
                 st4(a.s + i, make_float4(sv.x + eta * (zc.x * d.x - sv.x), sv.y + eta * (zc.y * d.y - sv.y), sv.z + eta * (zc.z * d.z - sv.z),
                                          sv.w + eta * (zc.w * d.w - sv.w)));
                 st4(a.y + i, make_float4(yv.x + eta * (en.x - yv.x), yv.y + eta * (en.y - yv.y), yv.z + eta * (en.z - yv.z),
                                          yv.w + eta * (en.w - yv.w)));
+            } else if (kSmooth && smooth == kSmoothStart) {  // s = z diag; y = e
+                st4(a.s + i, make_float4(zc.x * d.x, zc.y * d.y, zc.z * d.z, zc.w * d.w));
+                st4(a.y + i, en);
             }
         }
         st4(a.q + i, qv);
@@ -537,11 +557,30 @@ __device__ void spmv_fast(const PcgArgs& a, const FastGeom& f, int k, float beta
 // update_phase for the fast path.  (Recomputing q = A p_k here instead of
 // storing it saves 4 B/cell, but measured slower on B200: 183 vs 167 ms per
 // 1329-iteration solve at 256^3, from the extra stencil loads and spills.)
+// The loads of the thread's next group are issued before this group's
+// stores (software prefetch): a thread then keeps two groups' vectors in
+// flight, which the phase needs to cover HBM latency at 4 blocks per SM.
 template <bool kSmooth>
 __device__ void update_fast(const PcgArgs& a, const FastGeom& f, float alpha, bool smooth, double (&v)[4]) {
     v[0] = v[1] = v[2] = v[3] = 0.0;
-    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < f.groups; t += gridDim.x * blockDim.x) {
+    const uint32_t stride = gridDim.x * blockDim.x;
+    uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    float4 zn = make_float4(0.0f, 0.0f, 0.0f, 0.0f), qn = zn, sn = zn;
+    if (t < f.groups) {
+        zn = ld4(a.z + 4u * t);
+        qn = ld4(a.q + 4u * t);
+        if (kSmooth && smooth) sn = ld4(a.s + 4u * t);
+    }
+    for (; t < f.groups; t += stride) {
         const uint32_t i = 4u * t;
+        float4 zz = zn;
+        const float4 q = qn, sv = sn;
+        if (t + stride < f.groups) {
+            const uint32_t j = i + 4u * stride;
+            zn = ld4(a.z + j);
+            qn = ld4(a.q + j);
+            if (kSmooth && smooth) sn = ld4(a.s + j);
+        }
         const uint32_t row = fastdiv(i, f.dnx);
         const uint32_t x0 = i - row * f.nx;
         const uint32_t z = fastdiv(row, f.dny);
@@ -550,10 +589,6 @@ __device__ void update_fast(const PcgArgs& a, const FastGeom& f, float alpha, bo
         int32_t left, right;
         float4 d;
         x_geom(f, x0, rg.dyz, left, right, d);
-        float4 zz = ld4(a.z + i);
-        const float4 q = ld4(a.q + i);
-        float4 sv;
-        if (kSmooth && smooth) sv = ld4(a.s + i);
         zz.x -= alpha * q.x / d.x;
         zz.y -= alpha * q.y / d.y;
         zz.z -= alpha * q.z / d.z;
@@ -573,8 +608,11 @@ __device__ void update_fast(const PcgArgs& a, const FastGeom& f, float alpha, bo
 
 constexpr uint32_t kMaxRefinements = 4;
 
+// Register caps measured at 256^3: the plain solve is fastest at 4 blocks
+// per SM (64 registers); the smoothing specialisation carries five more
+// vectors per group and spills at that cap, and runs 10 % faster at 3.
 template <bool kFast, bool kSmooth>
-__global__ void __launch_bounds__(kBlock, 4) pcg_kernel(PcgArgs a) {
+__global__ void __launch_bounds__(kBlock, kSmooth ? 3 : 4) pcg_kernel(PcgArgs a) {
     __shared__ double red[4 * 32];
     SolverState* st = a.st;
     double v3[3];
@@ -606,6 +644,11 @@ __global__ void __launch_bounds__(kBlock, 4) pcg_kernel(PcgArgs a) {
     // iteration.  A dropped guess, or one no better than zero (an empty
     // history), makes this the plain solve.
     const bool smooth_run = kSmooth && warm != 0u && rr < 0.01 * bb;
+    // The smoothed sequence begins once the CG residual is within 10x of the
+    // tolerance: the plateau it cures lies below that, and the first
+    // iterations of a pass then move 16 bytes per cell less (same iteration
+    // count within 2 in FP64 experiments at 128^3).
+    const double smooth_begin2 = 100.0 * target2;
     uint32_t iterations = 0, refinements = 0;
     uint32_t status = XS_OK;
     while (true) {
@@ -627,27 +670,29 @@ __global__ void __launch_bounds__(kBlock, 4) pcg_kernel(PcgArgs a) {
         float beta = 0.0f, alpha = 0.0f, eta = 0.0f;
         double eta_final = 0.0;
         bool broke = false, smoothed = false;
+        // the residual phase set s = r, y = 0 for a pass that starts close enough
+        int smode = smooth_run && rr < smooth_begin2 ? kSmoothActive : kSmoothOff;
         while (true) {
             double pq[1];
             if (kFast) {
-                if (k == 0) spmv_fast<true, kSmooth>(a, a.fast, k, beta, alpha, eta, smooth_run, pq[0]);
-                else spmv_fast<false, kSmooth>(a, a.fast, k, beta, alpha, eta, smooth_run, pq[0]);
+                if (k == 0) spmv_fast<true, kSmooth>(a, a.fast, k, beta, alpha, eta, smode, pq[0]);
+                else spmv_fast<false, kSmooth>(a, a.fast, k, beta, alpha, eta, smode, pq[0]);
             } else {
-                spmv_phase<kSmooth>(a, k, beta, alpha, eta, smooth_run, pq[0]);
+                spmv_phase<kSmooth>(a, k, beta, alpha, eta, smode, pq[0]);
             }
             if (!grid_reduce<1>(st, a.partials, pq, red)) return;
             if (!(pq[0] > 0.0) || !isfinite(pq[0])) { broke = true; break; }
             alpha = static_cast<float>(rz / pq[0]);
             double v4[4];
-            if (kFast) update_fast<kSmooth>(a, a.fast, alpha, smooth_run, v4);
-            else update_phase<kSmooth>(a, alpha, smooth_run, v4);
+            if (kFast) update_fast<kSmooth>(a, a.fast, alpha, smode != kSmoothOff, v4);
+            else update_phase<kSmooth>(a, alpha, smode != kSmoothOff, v4);
             if (!grid_reduce<4>(st, a.partials, v4, red)) return;
             ++iterations;
             beta = static_cast<float>(v4[0] / rz);
             rz = v4[0];
             if (!isfinite(v4[1])) { broke = true; break; }
             if (v4[1] <= target2 || iterations >= a.max_iterations) break;
-            if (smooth_run) {
+            if (smode != kSmoothOff) {
                 // s.s, s.r, r.r -> eta and the norm of the next smoothed residual
                 const double den = v4[1] - 2.0 * v4[2] + v4[3];
                 const double e = den > 0.0 ? (v4[3] - v4[2]) / den : 0.0;
@@ -658,6 +703,9 @@ __global__ void __launch_bounds__(kBlock, 4) pcg_kernel(PcgArgs a) {
                     eta_final = e;
                     break;
                 }
+                smode = kSmoothActive;
+            } else if (smooth_run && v4[1] < smooth_begin2) {
+                smode = kSmoothStart;
             }
             ++k;
         }
@@ -843,8 +891,8 @@ namespace {
 
 struct DeviceLimits {
     int sms = 0;
-    int pcg_blocks_per_sm = 0;
-    int pcg_fast_blocks_per_sm = 0;
+    int pcg_blocks_per_sm[2] = {0, 0};       // [smooth]
+    int pcg_fast_blocks_per_sm[2] = {0, 0};  // [smooth]
     int rbgs_blocks_per_sm = 0;
     int rev_blocks_per_sm = 0;
 };
@@ -859,16 +907,12 @@ XsStatus device_limits(DeviceLimits& out) {
     if (dev != cached_device) {
         DeviceLimits l;
         if (cudaDeviceGetAttribute(&l.sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess) return XS_CUDA_ERROR;
-        // the smoothing variants have the same register cap (launch bounds);
-        // the smaller occupancy of the two sizes both grids
-        int a0 = 0, a1 = 0, b0 = 0, b1 = 0;
-        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a0, pcg_kernel<false, false>, kBlock, 0) != cudaSuccess ||
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&a1, pcg_kernel<false, true>, kBlock, 0) != cudaSuccess ||
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b0, pcg_kernel<true, false>, kBlock, 0) != cudaSuccess ||
-            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&b1, pcg_kernel<true, true>, kBlock, 0) != cudaSuccess)
+        // each specialisation's cooperative grid is its own co-resident count
+        if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&l.pcg_blocks_per_sm[0], pcg_kernel<false, false>, kBlock, 0) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&l.pcg_blocks_per_sm[1], pcg_kernel<false, true>, kBlock, 0) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&l.pcg_fast_blocks_per_sm[0], pcg_kernel<true, false>, kBlock, 0) != cudaSuccess ||
+            cudaOccupancyMaxActiveBlocksPerMultiprocessor(&l.pcg_fast_blocks_per_sm[1], pcg_kernel<true, true>, kBlock, 0) != cudaSuccess)
             return XS_CUDA_ERROR;
-        l.pcg_blocks_per_sm = std::min(a0, a1);
-        l.pcg_fast_blocks_per_sm = std::min(b0, b1);
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&l.rbgs_blocks_per_sm, rbgs_kernel, kBlock, 0) != cudaSuccess) return XS_CUDA_ERROR;
         if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&l.rev_blocks_per_sm, rbgs_reverse_kernel, kBlock, 0) != cudaSuccess)
             return XS_CUDA_ERROR;
@@ -957,8 +1001,8 @@ XsStatus solve_pressure(cudaStream_t stream, const Grid& g, const XsPressureSolv
             f.kind[face] = per ? 2u : (pb.modes[face] == 0u ? 1u : 0u);
         }
     }
-    const unsigned fast_blocks = persistent_blocks(lim.pcg_fast_blocks_per_sm, lim.sms, n / 4);
-    const unsigned blocks = persistent_blocks(lim.pcg_blocks_per_sm, lim.sms, n);
+    const unsigned fast_blocks = persistent_blocks(lim.pcg_fast_blocks_per_sm[a.smooth], lim.sms, n / 4);
+    const unsigned blocks = persistent_blocks(lim.pcg_blocks_per_sm[a.smooth], lim.sms, n);
     if (a.use_fast)
         return a.smooth ? launch_cooperative(pcg_kernel<true, true>, fast_blocks, a, stream)
                         : launch_cooperative(pcg_kernel<true, false>, fast_blocks, a, stream);
