@@ -10,10 +10,14 @@ velocity on the sides and bottom, open top), pressure by Jacobi-PCG to a
 The plume first spins up from rest (seeded uniform velocity noise in
 +-0.01) for --spinup steps; every arm then starts from that state:
 
-  plain            zero start (the reference's zero-initialised solve)
-  history          Galerkin start from the last 5 forward solutions
-  learned          the warm-start network's guess alone, energy-scaled
-  learned+history  the ring and the network's correction together (headline)
+  plain                   zero start (the reference's zero-initialised solve)
+  history                 Galerkin start from the last 5 forward solutions
+  history+coarse          ... then a step along the coarse-grid correction
+  learned                 the warm-start network's guess alone, energy-scaled
+  learned+history         the ring start, then a step along the network's
+                          correction of its residual
+  learned+history+coarse  the ring start, the coarse-grid step, then the
+                          network's step (headline)
 
 Each arm runs W warm-up steps (which also refill its ring) and K timed steps.
 ``value`` is the headline arm's steps/s; every arm's steps/s and PCG
@@ -44,6 +48,7 @@ METRIC = "256^3 smoke steps/s: learned-warm-start vs plain PCG at rel. residual 
 UNIT = "steps/s"
 GRID = 256
 HISTORY = 5
+COARSENING = 4  # coarse-grid correction of the start on the grid coarsened x4 per axis
 WEIGHTS = os.path.join(ROOT, "diff_solver_b200", "weights", "warm_start_128.npz")
 
 
@@ -53,7 +58,7 @@ def grid_shape(spec):
     return tuple(v * 3) if len(v) == 1 else tuple(v)
 
 
-def workload_configuration(shape=(GRID,) * 3, history=0):
+def workload_configuration(shape=(GRID,) * 3, history=0, coarsening=0):
     """dx = 1 / nx; the inflow sits at x = 0.5, y = 0.1 and the middle of z."""
     from diff_solver_b200.data import plume_configuration
     nx, ny, nz = shape
@@ -61,6 +66,7 @@ def workload_configuration(shape=(GRID,) * 3, history=0):
     cfg.pressure_tolerance = 1e-6
     cfg.pressure_max_iterations = 20000
     cfg.warm_start_history = history
+    cfg.warm_start_coarsening = coarsening
     return cfg
 
 
@@ -199,9 +205,9 @@ def cpu_sample(shape=(GRID,) * 3, sample_iterations=8, gpu_iterations=None):
 class Rollout:
     """One execution context of the workload with its own state buffers."""
 
-    def __init__(self, grid, history, network):
+    def __init__(self, grid, history, network, coarsening=0):
         from diff_solver_b200.model import ExecutionMode, Model, fill_parameters
-        self.model = Model(workload_configuration(grid, history))
+        self.model = Model(workload_configuration(grid, history, coarsening))
         self.ctx = self.model.allocate_context(ExecutionMode.forward)
         if network is not None:
             self.ctx.set_learned_warm_start(network)
@@ -263,6 +269,7 @@ def timed_arm(args, world, ro, initial, e2e=False):
     per_step = [N.XsSolveStats.from_buffer_copy(bytes(stats_host[i].numpy())) for i in range(k_steps)]
     out = dict(elapsed_ms=max_over_ranks(start.elapsed_time(end), world), launches=launches,
                iterations=[s.iterations for s in per_step], refinements=[s.refinements for s in per_step],
+               coarse_iterations=[s.coarse_iterations for s in per_step],
                residuals=[s.final_residual for s in per_step], initial_residuals=[s.initial_residual for s in per_step],
                solve_ms=[a.elapsed_time(b) for a, b in events])
     if e2e:
@@ -317,7 +324,7 @@ def product_run(args, world, rank, local):
         network = WarmStartNetwork(tuple(s // 2 for s in args.shape), factor=2)
         network.load(args.weights)
     # spin-up from rest with the fastest start; its final state opens every arm
-    spin = Rollout(args.shape, HISTORY, network)
+    spin = Rollout(args.shape, HISTORY, network, args.coarsening)
     gen = torch.Generator(device="cuda").manual_seed(0)
     for t in spin.cur.velocity.components():
         t.uniform_(-0.01, 0.01, generator=gen)
@@ -330,15 +337,19 @@ def product_run(args, world, rank, local):
     for d, s in zip(tensors_of(initial), tensors_of(spin.cur)):
         d.copy_(s)
     del spin
-    arms = [("plain", 0, None), ("history", HISTORY, None)]
+    arms = [("plain", 0, None, 0), ("history", HISTORY, None, 0)]
+    if args.coarsening:
+        arms += [("history+coarse", HISTORY, None, args.coarsening)]
     if network is not None:
-        arms += [("learned", 0, network), ("learned+history", HISTORY, network)]
+        arms += [("learned", 0, network, 0), ("learned+history", HISTORY, network, 0)]
+        if args.coarsening:
+            arms += [("learned+history+coarse", HISTORY, network, args.coarsening)]
     headline = arms[-1][0]
     sampler = ClockSampler(local)
     sampler.start()
     results = {}
-    for name, history, net in arms:
-        ro = Rollout(args.shape, history, net)
+    for name, history, net, coarsening in arms:
+        ro = Rollout(args.shape, history, net, coarsening)
         results[name] = timed_arm(args, world, ro, initial, e2e=(name == headline))
         del ro
         torch.cuda.empty_cache()
@@ -361,6 +372,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="plain and history arms only")
     ap.add_argument("--weights", default=WEIGHTS, help="warm-start network parameters (.npz)")
+    ap.add_argument("--coarsening", type=int, default=COARSENING, help="coarse-grid correction factor (0: off)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -370,8 +382,10 @@ def main():
     name = "x".join(map(str, args.shape))
     config = {"workload": f"smoke plume {name} after a {args.spinup}-step spin-up from rest, Jacobi-PCG to rel. residual 1e-6",
               "grid": list(args.shape), "cells": n, "dt": "0.5 dx", "steps_per_replica": args.steps, "spinup_steps": args.spinup,
-              "warm_start": f"Galerkin start over the last {HISTORY} solutions + U-Net correction (network trained at 128^3, "
-                            f"applied on the grid restricted x2)",
+              "warm_start": f"Galerkin start over the last {HISTORY} solutions"
+                            + (f", step along the coarse-grid correction (grid coarsened x{args.coarsening}, Jacobi-PCG to 1e-2)"
+                               if args.coarsening else "")
+                            + ", step along the U-Net correction (network trained at 128^3, applied on the grid restricted x2)",
               "l2": f"inputs larger than L2 (state {n * 21 * 4 / 1e6:.0f} MB)", "parallelism": f"replicas{world}"}
     if args.impl == "reference":
         if rank == 0:
@@ -391,6 +405,7 @@ def main():
     for name, r in results.items():
         arms[name] = {"steps_per_s": steps_total / (r["elapsed_ms"] / 1e3), "ms_per_step": r["elapsed_ms"] / args.steps,
                       "pcg_iterations_per_step": r["iterations"], "mean_pcg_iterations": statistics.mean(r["iterations"]),
+                      "coarse_iterations_per_step": r["coarse_iterations"],
                       "refinement_passes_per_step": r["refinements"],
                       "solve_ms_per_step": statistics.mean(r["solve_ms"]), "initial_residuals": r["initial_residuals"],
                       "final_residuals": r["residuals"], "gpu_launches": r["launches"]}

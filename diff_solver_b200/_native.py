@@ -49,7 +49,7 @@ class XsPressureSolve(C.Structure):
 class XsSolveStats(C.Structure):
     _fields_ = [("iterations", C.c_uint32), ("status", C.c_uint32), ("refinements", C.c_uint32), ("warm_start_used", C.c_uint32),
                 ("rhs_norm", C.c_double), ("initial_residual", C.c_double), ("final_residual", C.c_double),
-                ("guess_scale", C.c_double)]
+                ("guess_scale", C.c_double), ("coarse_iterations", C.c_uint32), ("reserved", C.c_uint32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -66,7 +66,8 @@ class XsSmokeModel(C.Structure):
                 ("vorticity_confinement_enabled", C.c_uint32), ("pressure_anchor", C.c_uint32), ("pressure", XsPressureSolve),
                 ("inflows", C.c_void_p), ("inflow_count", C.c_uint32), ("cell_mask", C.c_void_p), ("collider_velocity", XsVector),
                 ("collider_density", C.c_void_p), ("collider_temperature", C.c_void_p), ("solve_begin", C.c_void_p),
-                ("solve_end", C.c_void_p), ("warm_start", C.c_void_p), ("warm_start_history", C.c_uint32)]
+                ("solve_end", C.c_void_p), ("warm_start", C.c_void_p), ("warm_start_history", C.c_uint32),
+                ("warm_start_coarsening", C.c_uint32)]
 
 
 class XsState(C.Structure):

@@ -1028,7 +1028,7 @@ XsStatus reverse_rbgs(cudaStream_t stream, const Grid& g, uint32_t sweeps, uint3
 // slot live on the device) and optionally one extra vector (the learned
 // guess).  Dependent vectors are dropped by an LDL^T of the Jacobi-scaled
 // Gram matrix that skips pivots below kBasisPivot.
-constexpr int kGramBlocks = 148 * 3;  // one wave at 3 blocks per SM
+constexpr int kGramBlocks = 148 * 3;  // one wave at 3 blocks per SM (bases of 6 vectors run at 2)
 constexpr double kBasisPivot = 1e-11;
 
 template <int M>
@@ -1076,7 +1076,7 @@ __device__ __forceinline__ double boundary_fixed_sum(const Operator& op, uint64_
 
 // Streams the vectors and their stored A products: no stencil work here.
 template <int M>
-__global__ void __launch_bounds__(256, 3) basis_gram_kernel(BasisArgs<M> a) {
+__global__ void __launch_bounds__(256, M > 5 ? 2 : 3) basis_gram_kernel(BasisArgs<M> a) {
     constexpr int K = M * (M + 1) / 2 + M;
     __shared__ double red[K * 32];
     const float* ptr[M];
@@ -1261,14 +1261,32 @@ __global__ void history_advance_kernel(uint32_t history, uint32_t* meta) {
     meta[0] = min(meta[0] + 1, history);
 }
 
-size_t warm_history_bytes(const Grid& g, uint32_t history) {
-    if (history == 0) return 0;
-    const size_t n = cell_count(g);
-    return align_up(256, 256) + (2 * history + 4) * align_up(n * 4, 256) +
-           align_up(sizeof(double) * kGramBlocks * (kMaxBasis * (kMaxBasis + 1) / 2 + kMaxBasis), 256) + 256;
+bool coarse_grid(const Grid& g, uint32_t coarsening, Grid& coarse) {
+    if (coarsening < 2 || g.nx % static_cast<int>(coarsening) != 0 || g.ny % static_cast<int>(coarsening) != 0 ||
+        g.nz % static_cast<int>(coarsening) != 0)
+        return false;
+    coarse = g;
+    coarse.nx = g.nx / static_cast<int>(coarsening);
+    coarse.ny = g.ny / static_cast<int>(coarsening);
+    coarse.nz = g.nz / static_cast<int>(coarsening);
+    coarse.h = g.h * static_cast<float>(coarsening);
+    return true;
 }
 
-WarmHistory carve_warm_history(void* base, const Grid& g, uint32_t history) {
+size_t warm_history_bytes(const Grid& g, uint32_t history, uint32_t coarsening) {
+    if (history == 0) return 0;
+    const size_t n = cell_count(g);
+    size_t bytes = align_up(256, 256) + (2 * history + 4) * align_up(n * 4, 256) +
+                   align_up(sizeof(double) * kGramBlocks * (kMaxBasis * (kMaxBasis + 1) / 2 + kMaxBasis), 256) + 256;
+    Grid c;
+    if (coarse_grid(g, coarsening, c)) {
+        const size_t nc = cell_count(c);
+        bytes += align_up(n * 4, 256) + align_up(nc * 8, 256) + align_up(nc * 4, 256) + align_up(pressure_workspace_bytes(c), 256);
+    }
+    return bytes;
+}
+
+WarmHistory carve_warm_history(void* base, const Grid& g, uint32_t history, uint32_t coarsening) {
     WarmHistory h{};
     h.history = history;
     if (history == 0 || !base) return h;
@@ -1276,23 +1294,29 @@ WarmHistory carve_warm_history(void* base, const Grid& g, uint32_t history) {
     char* p = static_cast<char*>(base);
     h.meta = reinterpret_cast<uint32_t*>(p);
     size_t off = 256;
+    auto take = [&](size_t bytes) {
+        char* r = p + off;
+        off += align_up(bytes, 256);
+        return r;
+    };
     for (uint32_t i = 0; i < history; ++i) {
-        h.slots[i] = reinterpret_cast<float*>(p + off);
-        off += align_up(n * 4, 256);
-        h.products[i] = reinterpret_cast<float*>(p + off);
-        off += align_up(n * 4, 256);
+        h.slots[i] = reinterpret_cast<float*>(take(n * 4));
+        h.products[i] = reinterpret_cast<float*>(take(n * 4));
     }
-    h.extra_product = reinterpret_cast<float*>(p + off);
-    off += align_up(n * 4, 256);
-    h.start = reinterpret_cast<float*>(p + off);
-    off += align_up(n * 4, 256);
-    h.ring_start = reinterpret_cast<float*>(p + off);
-    off += align_up(n * 4, 256);
-    h.residual = reinterpret_cast<float*>(p + off);
-    off += align_up(n * 4, 256);
-    h.partials = reinterpret_cast<double*>(p + off);
-    off += align_up(sizeof(double) * kGramBlocks * (kMaxBasis * (kMaxBasis + 1) / 2 + kMaxBasis), 256);
-    h.coef = reinterpret_cast<double*>(p + off);
+    h.extra_product = reinterpret_cast<float*>(take(n * 4));
+    h.start = reinterpret_cast<float*>(take(n * 4));
+    h.ring_start = reinterpret_cast<float*>(take(n * 4));
+    h.residual = reinterpret_cast<float*>(take(n * 4));
+    h.partials = reinterpret_cast<double*>(take(sizeof(double) * kGramBlocks * (kMaxBasis * (kMaxBasis + 1) / 2 + kMaxBasis)));
+    h.coef = reinterpret_cast<double*>(take(256));
+    if (coarse_grid(g, coarsening, h.coarse)) {
+        const size_t nc = cell_count(h.coarse);
+        h.coarsening = coarsening;
+        h.correction = reinterpret_cast<float*>(take(n * 4));
+        h.coarse_rhs = reinterpret_cast<double*>(take(nc * 8));
+        h.coarse_solution = reinterpret_cast<float*>(take(nc * 4));
+        h.coarse_solver = take(pressure_workspace_bytes(h.coarse));
+    }
     return h;
 }
 
@@ -1346,6 +1370,136 @@ XsStatus galerkin_combine(cudaStream_t st, const Grid& g, uint32_t anchor, const
         case 5: return galerkin_m<5>(st, op, h, ring, extra, n_extra, rhs, rhs_d, out);
         default: return galerkin_m<kMaxBasis>(st, op, h, ring, extra, n_extra, rhs, rhs_d, out);
     }
+}
+
+// ---------------------------------------------- coarse-grid correction
+// One thread per coarse cell sums its f^3 children in a fixed order (a warp
+// reads f consecutive floats per thread and fine row: coalesced).
+__global__ void coarse_restrict_kernel(Grid g, Grid c, uint32_t f, const float* __restrict__ r, double* __restrict__ rc, double scale) {
+    const uint64_t nc = cell_count(c);
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < nc; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        int x, y, z;
+        decode(i, c.nx, c.ny, x, y, z);
+        double acc = 0.0;
+        for (uint32_t dz = 0; dz < f; ++dz)
+            for (uint32_t dy = 0; dy < f; ++dy) {
+                const uint64_t row = (static_cast<uint64_t>(z) * f + dz) * static_cast<uint64_t>(g.ny) + static_cast<uint64_t>(y) * f + dy;
+                const float* src = r + row * static_cast<uint64_t>(g.nx) + static_cast<uint64_t>(x) * f;
+                for (uint32_t dx = 0; dx < f; ++dx) acc += static_cast<double>(src[dx]);
+            }
+        rc[i] = acc * scale;
+    }
+}
+
+// Trilinear interpolation of a cell-centred coarse field at the fine cell
+// centres: coarse coordinate u = (i + 1/2) / f - 1/2 clamped to [0, n_c - 1].
+__device__ __forceinline__ void coarse_axis(int i, int nc, float inv_f, int& i0, int& i1, float& w) {
+    const float u = fminf(fmaxf((static_cast<float>(i) + 0.5f) * inv_f - 0.5f, 0.0f), static_cast<float>(nc - 1));
+    i0 = min(static_cast<int>(u), nc - 1);
+    i1 = min(i0 + 1, nc - 1);
+    w = u - static_cast<float>(i0);
+}
+
+__global__ void coarse_prolong_kernel(Grid g, Grid c, float inv_f, const float* __restrict__ ec, float* __restrict__ out) {
+    const uint64_t n = cell_count(g);
+    const uint64_t sy = static_cast<uint64_t>(c.nx), sz = static_cast<uint64_t>(c.nx) * static_cast<uint64_t>(c.ny);
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        int x, y, z;
+        decode(i, g.nx, g.ny, x, y, z);
+        int x0, x1, y0, y1, z0, z1;
+        float wx, wy, wz;
+        coarse_axis(x, c.nx, inv_f, x0, x1, wx);
+        coarse_axis(y, c.ny, inv_f, y0, y1, wy);
+        coarse_axis(z, c.nz, inv_f, z0, z1, wz);
+        auto at = [&](int xx, int yy, int zz) { return __ldg(ec + static_cast<uint64_t>(zz) * sz + static_cast<uint64_t>(yy) * sy + static_cast<uint64_t>(xx)); };
+        const float c00 = at(x0, y0, z0) * (1.0f - wx) + at(x1, y0, z0) * wx;
+        const float c10 = at(x0, y1, z0) * (1.0f - wx) + at(x1, y1, z0) * wx;
+        const float c01 = at(x0, y0, z1) * (1.0f - wx) + at(x1, y0, z1) * wx;
+        const float c11 = at(x0, y1, z1) * (1.0f - wx) + at(x1, y1, z1) * wx;
+        const float c0 = c00 * (1.0f - wy) + c10 * wy;
+        const float c1 = c01 * (1.0f - wy) + c11 * wy;
+        out[i] = c0 * (1.0f - wz) + c1 * wz;
+    }
+}
+
+XsStatus coarse_correction(cudaStream_t st, const Grid& g, uint32_t anchor, const XsScalarBoundary& pb, const WarmHistory& h, const float* r) {
+    if (h.coarsening < 2 || !h.correction || !h.coarse_rhs || !h.coarse_solution || !h.coarse_solver || !r) return XS_INVALID_ARGUMENT;
+    const Grid& c = h.coarse;
+    const uint32_t f = h.coarsening;
+    const uint64_t n = cell_count(g), nc = cell_count(c);
+    coarse_restrict_kernel<<<static_cast<unsigned>(std::min<uint64_t>((nc + 255) / 256, 148 * 16)), 256, 0, st>>>(g, c, f, r, h.coarse_rhs,
+                                                                                                                   1.0 / static_cast<double>(f));
+    XsStatus s = check_launch();
+    if (s != XS_OK) return s;
+    // the anchor moves to the coarse cell that contains it (n: none, on both grids)
+    uint32_t anchor_c = anchor;
+    if (anchor < n) {
+        const uint64_t ax = anchor % static_cast<uint64_t>(g.nx), ay = (anchor / static_cast<uint64_t>(g.nx)) % static_cast<uint64_t>(g.ny),
+                       az = anchor / (static_cast<uint64_t>(g.nx) * static_cast<uint64_t>(g.ny));
+        anchor_c = static_cast<uint32_t>(ax / f + static_cast<uint64_t>(c.nx) * (ay / f + static_cast<uint64_t>(c.ny) * (az / f)));
+    }
+    XsPressureSolve cs{};
+    cs.kind = XS_SOLVER_JACOBI_PCG;
+    cs.max_iterations = kCoarseMaxIterations;
+    cs.tolerance = kCoarseTolerance;
+    cs.initial_guess = nullptr;
+    cs.scale_guess = 0u;
+    // FP64 right-hand side: the adjoint form of the solve, without fixed values
+    if ((s = solve_pressure(st, c, cs, anchor_c, nullptr, pb, nullptr, h.coarse_rhs, h.coarse_solution, nullptr, h.coarse_solver, nullptr)) !=
+        XS_OK)
+        return s;
+    coarse_prolong_kernel<<<static_cast<unsigned>(std::min<uint64_t>((n + 255) / 256, 148 * 16)), 256, 0, st>>>(
+        g, c, 1.0f / static_cast<float>(f), h.coarse_solution, h.correction);
+    return check_launch();
+}
+
+XsStatus record_coarse_iterations(cudaStream_t st, const WarmHistory& h, void* fine_workspace, const Grid& g) {
+    if (h.coarsening < 2 || !h.coarse_solver || !fine_workspace) return XS_OK;
+    const PressureWorkspace fw = carve_pressure_workspace(fine_workspace, g);
+    const PressureWorkspace cw = carve_pressure_workspace(h.coarse_solver, h.coarse);
+    return check_cuda(cudaMemcpyAsync(&fw.state->stats.coarse_iterations, &cw.state->stats.iterations, sizeof(uint32_t),
+                                      cudaMemcpyDeviceToDevice, st));
+}
+
+// ------------------------------------------------ energy-optimal line step
+__global__ void line_update_kernel(uint64_t n, const double* __restrict__ coef, const float* __restrict__ d, const float* __restrict__ ad,
+                                   const float* x, float* r, float* x_out) {
+    const float c = static_cast<float>(coef[0]);
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        x_out[i] = fmaf(c, d[i], x[i]);
+        r[i] = fmaf(-c, ad[i], r[i]);
+    }
+}
+
+XsStatus line_step(cudaStream_t st, const Grid& g, uint32_t anchor, const uint32_t* mask, const XsScalarBoundary& pb, const WarmHistory& h,
+                   const float* d, const float* x, float* r, float* x_out) {
+    if (!h.meta || !h.extra_product || !d || !x || !r || !x_out) return XS_INVALID_ARGUMENT;
+    const Operator op{g, mask, anchor, pb, true};
+    const uint64_t n = cell_count(g);
+    const unsigned grid = static_cast<unsigned>(std::min<uint64_t>((n + 255) / 256, 148 * 16));
+    apply_operator_kernel<<<grid, 256, 0, st>>>(op, d, h.extra_product);
+    XsStatus s = check_launch();
+    if (s != XS_OK) return s;
+    // the Galerkin machinery with the one vector d and b = r (r already holds
+    // the fixed boundary values; r and A d vanish on inactive cells):
+    // coef = (d . r) / (d . A d)
+    BasisArgs<1> a{};
+    a.op = op;
+    a.v[0] = d;
+    a.w[0] = h.extra_product;
+    a.history = 0;
+    a.meta = h.meta;
+    a.rhs = r;
+    a.rhs_d = nullptr;
+    a.partials = h.partials;
+    a.fixed_terms = 0u;
+    const unsigned blocks = static_cast<unsigned>(std::min<uint64_t>((n + 255) / 256, kGramBlocks));
+    basis_gram_kernel<1><<<blocks, 256, 0, st>>>(a);
+    if ((s = check_launch()) != XS_OK) return s;
+    basis_solve_kernel<1><<<1, 64, 0, st>>>(h.partials, blocks, h.coef);
+    if ((s = check_launch()) != XS_OK) return s;
+    line_update_kernel<<<grid, 256, 0, st>>>(n, h.coef, d, h.extra_product, x, r, x_out);
+    return check_launch();
 }
 
 XsStatus start_residual(cudaStream_t st, const Grid& g, uint32_t anchor, const uint32_t* mask, const XsScalarBoundary& pb, const float* rhs,

@@ -68,7 +68,8 @@ XsStatus read_solve_stats(cudaStream_t stream, const void* workspace, const Grid
 
 // Warm-start subspace: a ring of the last `history` forward solutions plus
 // at most one extra vector (kMaxBasis in all) spanning the Galerkin start.
-constexpr int kMaxBasis = 6;
+constexpr int kMaxHistory = 5;
+constexpr int kMaxBasis = kMaxHistory + 1;
 struct WarmHistory {
     float* slots[kMaxBasis];
     float* products[kMaxBasis];  // A slot, computed when the slot is written
@@ -77,18 +78,47 @@ struct WarmHistory {
     float* start;       // the start vector of the last forward solve (N)
     float* ring_start;  // the Galerkin start from the ring alone (N)
     float* residual;    // b - A ring_start (N)
-    float* extra_product;  // A of the extra vector of a combination (N)
+    float* extra_product;  // A of the extra vector of a combination or of a line step's direction (N)
     double* partials;
     double* coef;
+    // coarse-grid correction of the start (coarsening > 0): the residual
+    // restricted by `coarsening` per axis, solved on the coarse grid to
+    // kCoarseTolerance by Jacobi-PCG, interpolated back (trilinear)
+    uint32_t coarsening;
+    Grid coarse;            // the coarse grid
+    float* correction;      // the interpolated coarse solution (N)
+    double* coarse_rhs;     // the restricted residual (coarse cells)
+    float* coarse_solution; // (coarse cells)
+    void* coarse_solver;    // pressure workspace of the coarse grid
 };
-size_t warm_history_bytes(const Grid& g, uint32_t history);
-WarmHistory carve_warm_history(void* base, const Grid& g, uint32_t history);
+constexpr double kCoarseTolerance = 1e-2;
+constexpr uint32_t kCoarseMaxIterations = 1000;
+// The coarse grid of g for a coarsening factor (false: none, or g not divisible).
+bool coarse_grid(const Grid& g, uint32_t coarsening, Grid& coarse);
+size_t warm_history_bytes(const Grid& g, uint32_t history, uint32_t coarsening = 0);
+WarmHistory carve_warm_history(void* base, const Grid& g, uint32_t history, uint32_t coarsening = 0);
 // out = the A-norm-optimal combination of the valid ring vectors (use_ring)
 // and the n_extra vectors in `extra`, for the right-hand side rhs (+ fixed
 // boundary values), or for the FP64 adjoint right-hand side rhs_d (no fixed
 // values) when given.  out must not be one of the combined vectors.
 XsStatus galerkin_combine(cudaStream_t st, const Grid& g, uint32_t anchor, const uint32_t* mask, const XsScalarBoundary& pb, const WarmHistory& h,
                           bool use_ring, const float* const* extra, int n_extra, const float* rhs, float* out, const double* rhs_d = nullptr);
+// The coarse-grid correction of a start residual r: h.correction =
+// P A_c^-1 R r.  R r = (sum of the f^3 children) / f: the operator is the
+// spacing-squared-scaled Laplacian, so the coarse system at spacing f h
+// takes f^2 times the children's mean.  A_c is the same stencil on the
+// coarse grid (boundary modes kept, no fixed values), solved by Jacobi-PCG
+// to kCoarseTolerance; P is trilinear interpolation at the fine cell
+// centres, clamped at the domain edges.  Grids without colliders only.
+XsStatus coarse_correction(cudaStream_t st, const Grid& g, uint32_t anchor, const XsScalarBoundary& pb, const WarmHistory& h, const float* r);
+// Copies the coarse solve's iteration count into the fine solve's statistics.
+XsStatus record_coarse_iterations(cudaStream_t st, const WarmHistory& h, void* fine_workspace, const Grid& g);
+// One energy-optimal step along a direction d from x (in place allowed):
+// x_out = x + c d, r -= c A d with c = (d . r) / (d . A d) minimising the
+// A-norm of the error along d (0 when d . A d vanishes); r is the residual
+// of x on entry and of x_out on return.  A d goes to h.extra_product.
+XsStatus line_step(cudaStream_t st, const Grid& g, uint32_t anchor, const uint32_t* mask, const XsScalarBoundary& pb, const WarmHistory& h,
+                   const float* d, const float* x, float* r, float* x_out);
 // r = b + fixed boundary values - A x
 XsStatus start_residual(cudaStream_t st, const Grid& g, uint32_t anchor, const uint32_t* mask, const XsScalarBoundary& pb, const float* rhs,
                         const float* x, float* r);

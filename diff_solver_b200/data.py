@@ -153,6 +153,9 @@ class Configuration:
     # previous forward solutions kept for the Galerkin start of the next
     # forward PCG solve (0..5; 0: off)
     warm_start_history: int = 0
+    # coarse-grid correction of that start (0: off; else the coarsening
+    # factor per axis, dividing the grid; needs a ring and no colliders)
+    warm_start_coarsening: int = 0
 
 
 def plume_configuration(n=(64, 64, 64), cell_size=None, inflow_center=(0.5, 0.1, 0.5), inflow_radius=0.08,

@@ -290,6 +290,7 @@ class Model:
         m.collider_density = cd.data_ptr() if has_colliders else None
         m.collider_temperature = ct.data_ptr() if has_colliders else None
         m.warm_start_history = int(cfg.warm_start_history)
+        m.warm_start_coarsening = int(cfg.warm_start_coarsening)
         ctx.native = m
         nbytes = L.xs_smoke_workspace_bytes(C.byref(m), int(mode))
         if nbytes == 0:

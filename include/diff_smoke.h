@@ -116,6 +116,8 @@ typedef struct XsSolveStats {
     double initial_residual;      /* ||b - A p0||_2 / ||b||_2 of the accepted start */
     double final_residual;        /* ||b - A p||_2 / ||b||_2, p in FP64 */
     double guess_scale;           /* alpha applied to the guess (1 if unscaled, 0 if none) */
+    uint32_t coarse_iterations;   /* CG iterations of the coarse-grid correction of the start (0: none) */
+    uint32_t reserved;
 } XsSolveStats;
 
 /* ------------------------------------------------------------------------ */
@@ -303,11 +305,20 @@ typedef struct XsSmokeModel {
     XsWarmStartNet* warm_start;
     /* number of previous forward solutions kept in the workspace (0..5; 0:
      * off).  The forward PCG then starts from the A-norm-optimal (Galerkin)
-     * combination of those solutions and the learned guess, if any.  The ring
+     * combination of those solutions, followed by one energy-optimal step
+     * along the learned correction of its residual, if any.  The ring
      * is part of the workspace (xs_smoke_workspace_bytes counts it) and is
      * emptied by xs_smoke_reset_warm_start, which must run once after the
      * workspace is allocated. */
     uint32_t warm_start_history;
+    /* coarse-grid correction of the forward start (0: off; otherwise the
+     * coarsening factor per axis, which must divide the grid; needs
+     * warm_start_history > 0 and no colliders).  The residual of the ring's
+     * start is restricted to the coarse grid, solved there by Jacobi-PCG to
+     * 1e-2 relative residual and interpolated back; the start then takes one
+     * energy-optimal step along it (before the learned correction's step).
+     * It removes the smooth error that fine-grid CG reduces slowest. */
+    uint32_t warm_start_coarsening;
 } XsSmokeModel;
 
 /* State / Control / Parameters (data.ixx:117-134) */

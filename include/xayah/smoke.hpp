@@ -93,6 +93,9 @@ struct Configuration {
     std::uint32_t pressure_max_iterations{4000u};
     // previous forward solutions kept for the Galerkin warm start (0..5; 0: off)
     std::uint32_t warm_start_history{0u};
+    // coarse-grid correction of that start (0: off; else the coarsening factor
+    // per axis, dividing the grid; needs a ring and no colliders)
+    std::uint32_t warm_start_coarsening{0u};
 };
 
 // ------------------------------------------------------------- data.ixx:85-204
@@ -260,6 +263,7 @@ public:
         m.collider_density = colliders ? ctx.domain.collider_density.values.data : nullptr;
         m.collider_temperature = colliders ? ctx.domain.collider_temperature.values.data : nullptr;
         m.warm_start_history = configuration.warm_start_history;
+        m.warm_start_coarsening = configuration.warm_start_coarsening;
         const std::size_t bytes = xs_smoke_workspace_bytes(&m, static_cast<std::uint32_t>(mode));
         if (bytes == 0) throw std::invalid_argument("invalid smoke configuration");
         ctx.workspace_ = cuda::Buffer<unsigned char>(ctx.resource, bytes);

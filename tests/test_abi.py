@@ -81,6 +81,32 @@ def test_workspace_queries_without_gpu():
     assert diff > fwd > ws
 
 
+def test_warm_start_options_are_validated_without_gpu():
+    """The ring (0..5 solutions) and the coarse-grid correction (a factor that
+    divides the grid, with a ring and no colliders) size the workspace; other
+    settings make the model invalid (0 bytes)."""
+    lib = _native.lib()
+    m = _native.XsSmokeModel()
+    m.grid = _native.XsGrid(32, 32, 16, 1 / 32, 1 / 64)
+    base = lib.xs_smoke_workspace_bytes(ctypes.byref(m), 0)
+    m.warm_start_history = 5
+    ring = lib.xs_smoke_workspace_bytes(ctypes.byref(m), 0)
+    assert ring > base
+    m.warm_start_coarsening = 4
+    coarse = lib.xs_smoke_workspace_bytes(ctypes.byref(m), 0)
+    assert coarse > ring
+    m.warm_start_coarsening = 3  # does not divide 32
+    assert lib.xs_smoke_workspace_bytes(ctypes.byref(m), 0) == 0
+    m.warm_start_coarsening = 32  # 16 / 32 is not whole
+    assert lib.xs_smoke_workspace_bytes(ctypes.byref(m), 0) == 0
+    m.warm_start_coarsening = 2
+    m.warm_start_history = 0  # no ring
+    assert lib.xs_smoke_workspace_bytes(ctypes.byref(m), 0) == 0
+    m.warm_start_history = 6
+    m.warm_start_coarsening = 0
+    assert lib.xs_smoke_workspace_bytes(ctypes.byref(m), 0) == 0
+
+
 def test_invalid_arguments_are_rejected_before_any_launch():
     lib = _native.lib()
     g = _native.XsGrid(0, 4, 4, 0.25, 0.1)
