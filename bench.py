@@ -344,6 +344,12 @@ def product_run(args, world, rank, local):
         arms += [("learned", 0, network, 0), ("learned+history", HISTORY, network, 0)]
         if args.coarsening:
             arms += [("learned+history+coarse", HISTORY, network, args.coarsening)]
+    if args.arms:  # a subset (profiling runs); the last one named is the headline
+        keep = args.arms.split(",")
+        unknown = [k for k in keep if k not in {a[0] for a in arms}]
+        if unknown:
+            raise ValueError(f"unknown arms {unknown}: choose from {[a[0] for a in arms]}")
+        arms = [a for k in keep for a in arms if a[0] == k]
     headline = arms[-1][0]
     sampler = ClockSampler(local)
     sampler.start()
@@ -373,6 +379,8 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="plain and history arms only")
     ap.add_argument("--weights", default=WEIGHTS, help="warm-start network parameters (.npz)")
     ap.add_argument("--coarsening", type=int, default=COARSENING, help="coarse-grid correction factor (0: off)")
+    ap.add_argument("--arms", default="", help="comma-separated subset of the arms, headline last (profiling; no roofline "
+                                               "or CPU baseline without the plain arm)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -422,23 +430,25 @@ def main():
     value = arms[headline]["steps_per_s"]
     # roofline of the dominant kernel (the persistent PCG), from the plain arm
     # where the solve window holds that kernel alone
-    p = results["plain"]
-    peak, peak_kind = measured_peaks()
-    kbytes_each = [pcg_algorithmic_bytes(n, it, rf) for it, rf in zip(p["iterations"], p["refinements"])]
-    achieved = sum(kbytes_each) / (sum(p["solve_ms"]) / 1e3) / 1e9
+    roofline = None
+    if "plain" in results:
+        p = results["plain"]
+        peak, peak_kind = measured_peaks()
+        kbytes_each = [pcg_algorithmic_bytes(n, it, rf) for it, rf in zip(p["iterations"], p["refinements"])]
+        achieved = sum(kbytes_each) / (sum(p["solve_ms"]) / 1e3) / 1e9
+        roofline = {"bound": "hbm", "kernel": "pcg_kernel", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                    "traffic": None, "peak_kind": peak_kind, "algorithmic_bytes_per_launch": statistics.mean(kbytes_each),
+                    "launch_ms": statistics.mean(p["solve_ms"]), "iterations_per_launch": statistics.mean(p["iterations"]), "arm": "plain"}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": h["elapsed_ms"] / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 (FP64 CG reductions and iterate)", "data": "synthetic", "config": config,
-            "method": headline, "speedup_vs_plain": value / arms["plain"]["steps_per_s"], "arms": arms,
-            "roofline": {"bound": "hbm", "kernel": "pcg_kernel", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                         "frac": achieved / peak, "traffic": None, "peak_kind": peak_kind,
-                         "algorithmic_bytes_per_launch": statistics.mean(kbytes_each), "launch_ms": statistics.mean(p["solve_ms"]),
-                         "iterations_per_launch": statistics.mean(p["iterations"]), "arm": "plain"},
+            "method": headline, "speedup_vs_plain": value / arms["plain"]["steps_per_s"] if "plain" in arms else None, "arms": arms,
+            "roofline": roofline,
             "gpu_launches": h["launches"], "clocks": clocks,
             "e2e": {"value": steps_total / (h["e2e_ms"] / 1e3), "unit": UNIT, "h2d_bytes_per_step": h["h2d"],
                     "d2h_bytes_per_step": h["d2h"]},
             "example_metrics_last_step": [float(v) for v in h["metrics"]]}
-    if world == 1 and not args.no_cpu_baseline:
+    if world == 1 and not args.no_cpu_baseline and "plain" in arms:
         cpu = cpu_sample(args.shape, gpu_iterations=int(arms["plain"]["mean_pcg_iterations"]))
         line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
     print(json.dumps(line), flush=True)

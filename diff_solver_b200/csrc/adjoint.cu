@@ -376,14 +376,24 @@ XsStatus projection_vjp(cudaStream_t st, const Grid& g, const XsPressureSolve& s
         adj.initial_guess = nullptr;
         adj.scale_guess = 0u;
         const bool ring = history && history->history > 0;
+        const bool coarse = ring && history->coarsening != 0 && mask == nullptr;
         if (ring) {
             // successive adjoint solves of a reverse pass are close: Galerkin
-            // start from the ring of previous adjoint solutions
-            if ((s = galerkin_combine(st, g, anchor, mask, pb, *history, true, nullptr, 0, nullptr, history->ring_start, pa)) != XS_OK)
-                return s;
-            adj.initial_guess = history->ring_start;
+            // start from the ring of previous adjoint solutions, then (with
+            // coarsening) one energy-optimal step along the coarse-grid
+            // correction of its residual, as in the forward solve
+            const WarmHistory& h = *history;
+            if ((s = galerkin_combine(st, g, anchor, mask, pb, h, true, nullptr, 0, nullptr, h.ring_start, pa)) != XS_OK) return s;
+            adj.initial_guess = h.ring_start;
+            if (coarse) {
+                if ((s = start_residual(st, g, anchor, mask, pb, nullptr, h.ring_start, h.residual, pa)) != XS_OK) return s;
+                if ((s = coarse_correction(st, g, anchor, pb, h, h.residual)) != XS_OK) return s;
+                if ((s = line_step(st, g, anchor, mask, pb, h, h.correction, h.ring_start, h.residual, h.start)) != XS_OK) return s;
+                adj.initial_guess = h.start;
+            }
         }
         s = solve_pressure(st, g, adj, anchor, mask, pb, nullptr, pa, nullptr, ra, workspace, nullptr);
+        if (s == XS_OK && coarse) s = record_coarse_iterations(st, *history, workspace, g);
         if (s == XS_OK && ring) s = history_push(st, g, anchor, mask, pb, *history, nullptr, ra);
     }
     if (s != XS_OK) return s;

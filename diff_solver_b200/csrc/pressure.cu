@@ -1199,7 +1199,8 @@ __global__ void basis_combine_kernel(BasisArgs<M> a, const double* __restrict__ 
 }
 
 // r = b + fixed boundary values - A x on the active cells, 0 elsewhere
-__global__ void start_residual_kernel(Operator op, const float* __restrict__ rhs, const float* __restrict__ x, float* __restrict__ r) {
+template <class T>
+__global__ void start_residual_kernel(Operator op, const T* __restrict__ rhs, const float* __restrict__ x, float* __restrict__ r) {
     const Grid& g = op.g;
     const uint64_t n = cell_count(g);
     for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
@@ -1503,10 +1504,14 @@ XsStatus line_step(cudaStream_t st, const Grid& g, uint32_t anchor, const uint32
 }
 
 XsStatus start_residual(cudaStream_t st, const Grid& g, uint32_t anchor, const uint32_t* mask, const XsScalarBoundary& pb, const float* rhs,
-                        const float* x, float* r) {
-    const Operator op{g, mask, anchor, pb, true};
+                        const float* x, float* r, const double* rhs_d) {
+    const Operator op{g, mask, anchor, pb, rhs_d == nullptr};
     const uint64_t n = cell_count(g);
-    start_residual_kernel<<<static_cast<unsigned>(std::min<uint64_t>((n + 255) / 256, 148 * 16)), 256, 0, st>>>(op, rhs, x, r);
+    const unsigned blocks = static_cast<unsigned>(std::min<uint64_t>((n + 255) / 256, 148 * 16));
+    if (rhs_d)
+        start_residual_kernel<double><<<blocks, 256, 0, st>>>(op, rhs_d, x, r);
+    else
+        start_residual_kernel<float><<<blocks, 256, 0, st>>>(op, rhs, x, r);
     return check_launch();
 }
 

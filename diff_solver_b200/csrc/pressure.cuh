@@ -119,9 +119,10 @@ XsStatus record_coarse_iterations(cudaStream_t st, const WarmHistory& h, void* f
 // of x on entry and of x_out on return.  A d goes to h.extra_product.
 XsStatus line_step(cudaStream_t st, const Grid& g, uint32_t anchor, const uint32_t* mask, const XsScalarBoundary& pb, const WarmHistory& h,
                    const float* d, const float* x, float* r, float* x_out);
-// r = b + fixed boundary values - A x
+// r = b + fixed boundary values - A x, or r = rhs_d - A x for the FP64
+// adjoint right-hand side (no fixed values) when rhs_d is given
 XsStatus start_residual(cudaStream_t st, const Grid& g, uint32_t anchor, const uint32_t* mask, const XsScalarBoundary& pb, const float* rhs,
-                        const float* x, float* r);
+                        const float* x, float* r, const double* rhs_d = nullptr);
 // Stores a solution (FP32, or FP64 rounded to FP32) in the next ring slot,
 // with its product by the operator.
 XsStatus history_push(cudaStream_t st, const Grid& g, uint32_t anchor, const uint32_t* mask, const XsScalarBoundary& pb, const WarmHistory& h,

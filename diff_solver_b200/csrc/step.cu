@@ -142,7 +142,7 @@ StepWorkspace carve_step(void* base, const Grid& g, uint32_t mode, uint32_t hist
         w.forced_a = fadj();
         w.pressure_a = static_cast<double*>(take(8 * n));
         w.rhs_a = static_cast<double*>(take(8 * n));
-        w.adjoint_history = carve_warm_history(take(warm_history_bytes(g, history)), g, history);
+        w.adjoint_history = carve_warm_history(take(warm_history_bytes(g, history, coarsening)), g, history, coarsening);
     }
     w.bytes = off;
     return w;

@@ -41,7 +41,7 @@ import numpy as np
 PARAMS = dict(ambient_temperature=0.0, density_buoyancy=-0.1, temperature_buoyancy=0.5, vorticity_confinement=0.0)
 
 
-def _setup(grid, tolerance, history=0, mode=None):
+def _setup(grid, tolerance, history=0, mode=None, coarsening=0):
     import torch
 
     from .data import plume_configuration
@@ -50,6 +50,7 @@ def _setup(grid, tolerance, history=0, mode=None):
     cfg.pressure_tolerance = tolerance
     cfg.pressure_max_iterations = 50000
     cfg.warm_start_history = history
+    cfg.warm_start_coarsening = coarsening
     model = Model(cfg)
     ctx = model.allocate_context(ExecutionMode.differentiable if mode is None else mode)
     params = fill_parameters(model.allocate_parameters(ctx), **PARAMS)
@@ -166,10 +167,10 @@ def finite_difference_check(grid=128, steps=50, checkpoint=10, directions=16, ep
             "checkpoints": len(traj.states)}
 
 
-def adjoint_timing(grid=256, forward=200, window=40, checkpoint=8, tolerance=1e-6, learned=False, history=5, seed=0):
+def adjoint_timing(grid=256, forward=200, window=40, checkpoint=8, tolerance=1e-6, learned=False, history=5, seed=0, coarsening=4):
     from .model import ExecutionMode, tensors_of
     from .solver import TapeMode, simulate, vjp
-    torch, model, ctx, params = _setup(grid, tolerance, history=history)
+    torch, model, ctx, params = _setup(grid, tolerance, history=history, coarsening=coarsening if history else 0)
     network = None
     if learned:
         from .warm_start import WarmStartNetwork
@@ -203,7 +204,7 @@ def adjoint_timing(grid=256, forward=200, window=40, checkpoint=8, tolerance=1e-
     if network is not None:
         network.check()
     return {"check": "adjoint", "grid": grid, "forward_steps": forward, "window": window, "checkpoint": checkpoint,
-            "learned": learned, "history": history, "lead_in_ms": ev[0].elapsed_time(ev[1]),
+            "learned": learned, "history": history, "coarsening": coarsening if history else 0, "lead_in_ms": ev[0].elapsed_time(ev[1]),
             "window_forward_ms": ev[1].elapsed_time(ev[2]), "vjp_ms": ev[2].elapsed_time(ev[3]),
             "vjp_ms_per_step": ev[2].elapsed_time(ev[3]) / window, "gradient_norm": gnorm, "checkpoints": len(traj.states)}
 
@@ -228,11 +229,13 @@ def main(argv=None) -> int:
     a.add_argument("--tolerance", type=float, default=1e-6)
     a.add_argument("--history", type=int, default=5)
     a.add_argument("--learned", action="store_true")
+    a.add_argument("--coarsening", type=int, default=4, help="coarse-grid correction of the forward and adjoint starts (0: off)")
     args = ap.parse_args(argv)
     if args.cmd == "fd":
         out = finite_difference_check(args.grid, args.steps, args.checkpoint, args.directions, args.eps, args.tolerance, args.seed)
     else:
-        out = adjoint_timing(args.grid, args.forward, args.window, args.checkpoint, args.tolerance, args.learned, args.history)
+        out = adjoint_timing(args.grid, args.forward, args.window, args.checkpoint, args.tolerance, args.learned, args.history,
+                             coarsening=args.coarsening)
     print(json.dumps(out), flush=True)
     return 0
 

@@ -221,17 +221,19 @@ def test_galerkin_history_start(cuda):
 
 def test_adjoint_solves_start_from_their_own_history(cuda):
     """A differentiable context with a ring also starts the adjoint pressure
-    solves of a reverse pass from previous adjoint solutions: the gradient
-    agrees with the zero-start one within the solver tolerance and the last
-    adjoint solve needs fewer iterations."""
+    solves of a reverse pass from previous adjoint solutions (and, with
+    coarsening, from their coarse-grid correction): the gradient agrees with
+    the zero-start one within the solver tolerance and the last adjoint solve
+    needs fewer iterations."""
     import torch
     from diff_solver_b200.data import plume_configuration
     from diff_solver_b200.model import ExecutionMode, Model, fill_parameters
     from diff_solver_b200.solver import TapeMode, simulate, vjp
     out = {}
-    for history in (0, 4):
+    for history, coarsening in ((0, 0), (4, 0), (4, 4)):
         cfg = plume_configuration((64, 64, 64))
         cfg.warm_start_history = history
+        cfg.warm_start_coarsening = coarsening
         m = Model(cfg)
         ctx = m.allocate_context(ExecutionMode.differentiable)
         q = fill_parameters(m.allocate_parameters(ctx), 0.0, -0.1, 0.5)
@@ -246,9 +248,14 @@ def test_adjoint_solves_start_from_their_own_history(cuda):
         grad = vjp(m, ctx, traj, controls, q, {12: seed})
         last = ctx.read_solve_stats()
         assert last["status"] == 0 and last["final_residual"] <= 1e-6
-        out[history] = (torch.cat([t.reshape(-1) for t in grad.initial_state.velocity.components()]).cpu().numpy(), last["iterations"])
-    assert rel(out[4][0], out[0][0]) < 1e-3
-    assert out[4][1] < out[0][1], (out[4][1], out[0][1])
+        out[(history, coarsening)] = (torch.cat([t.reshape(-1) for t in grad.initial_state.velocity.components()]).cpu().numpy(),
+                                      last["iterations"], last["coarse_iterations"])
+    assert rel(out[(4, 0)][0], out[(0, 0)][0]) < 1e-3
+    assert out[(4, 0)][1] < out[(0, 0)][1], (out[(4, 0)][1], out[(0, 0)][1])
+    # with the coarse-grid step the adjoint solves start from the ring's start
+    # corrected on the 16^3 grid: the same gradient
+    assert rel(out[(4, 4)][0], out[(0, 0)][0]) < 1e-3
+    assert out[(4, 4)][2] > 0 and out[(4, 4)][1] < out[(0, 0)][1]
 
 
 def test_coarse_grid_correction(cuda):
