@@ -393,7 +393,8 @@ def main():
               "warm_start": f"Galerkin start over the last {HISTORY} solutions"
                             + (f", step along the coarse-grid correction (grid coarsened x{args.coarsening}, Jacobi-PCG to 1e-2)"
                                if args.coarsening else "")
-                            + ", step along the U-Net correction (network trained at 128^3, applied on the grid restricted x2)",
+                            + ("" if args.no_learned else
+                               ", step along the U-Net correction (network trained at 128^3, applied on the grid restricted x2)"),
               "l2": f"inputs larger than L2 (state {n * 21 * 4 / 1e6:.0f} MB)", "parallelism": f"replicas{world}"}
     if args.impl == "reference":
         if rank == 0:
