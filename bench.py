@@ -130,6 +130,13 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+# DRAM traffic of the plain solve's persistent PCG launch per algorithmic byte,
+# from one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of this
+# workload's plain solve at 256^3: 800.5 GB for 1323 CG iterations and 2
+# refinement passes, whose algorithmic count below is 801.7 GB.
+PCG_TRAFFIC_PER_ALGORITHMIC_BYTE_256 = 800.5 / 801.7
+
+
 def pcg_algorithmic_bytes(n_cells, iterations, refinements):
     """Unique bytes the persistent PCG kernel must move: per CG iteration
     36 B/cell (spmv phase: read z, p_old, e; write p_new, q, e -- 24 B;
@@ -437,8 +444,12 @@ def main():
         peak, peak_kind = measured_peaks()
         kbytes_each = [pcg_algorithmic_bytes(n, it, rf) for it, rf in zip(p["iterations"], p["refinements"])]
         achieved = sum(kbytes_each) / (sum(p["solve_ms"]) / 1e3) / 1e9
+        traffic = None
+        if tuple(args.shape) == (GRID,) * 3:  # the captured workload: its measured traffic per algorithmic byte
+            traffic = PCG_TRAFFIC_PER_ALGORITHMIC_BYTE_256 * statistics.mean(kbytes_each)
         roofline = {"bound": "hbm", "kernel": "pcg_kernel", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                    "traffic": None, "peak_kind": peak_kind, "algorithmic_bytes_per_launch": statistics.mean(kbytes_each),
+                    "traffic": traffic, "traffic_unit": "bytes per launch", "peak_kind": peak_kind,
+                    "algorithmic_bytes_per_launch": statistics.mean(kbytes_each),
                     "launch_ms": statistics.mean(p["solve_ms"]), "iterations_per_launch": statistics.mean(p["iterations"]), "arm": "plain"}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": h["elapsed_ms"] / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
