@@ -176,7 +176,7 @@ def max_over_ranks(value, world):
 
 
 # --------------------------------------------------------------------- CPU
-def cpu_sample(shape=(GRID,) * 3, sample_iterations=8, gpu_iterations=None):
+def cpu_sample(shape=(GRID,) * 3, sample_iterations=40, gpu_iterations=None):
     """The FP64 oracle step on the host cores: one step with the PCG capped at
     0 and at `sample_iterations` iterations; the step time at the GPU's
     iteration count is t0 + k * (t_k - t0) / sample_iterations."""
