@@ -48,7 +48,7 @@ METRIC = "256^3 smoke steps/s: learned-warm-start vs plain PCG at rel. residual 
 UNIT = "steps/s"
 GRID = 256
 HISTORY = 5
-COARSENING = 4  # coarse-grid correction of the start on the grid coarsened x4 per axis
+COARSENING = 2  # coarse-grid correction of the start on the grid coarsened x2 per axis
 WEIGHTS = os.path.join(ROOT, "diff_solver_b200", "weights", "warm_start_128.npz")
 
 
@@ -427,7 +427,8 @@ def main():
     config = {"workload": f"smoke plume {name} after a {args.spinup}-step spin-up from rest, Jacobi-PCG to rel. residual 1e-6",
               "grid": list(args.shape), "cells": n, "dt": "0.5 dx", "steps_per_replica": args.steps, "spinup_steps": args.spinup,
               "warm_start": f"Galerkin start over the last {HISTORY} solutions"
-                            + (f", step along the coarse-grid correction (grid coarsened x{args.coarsening}, Jacobi-PCG to 1e-2)"
+                            + (f", 4 Jacobi sweeps and a step along the coarse-grid correction (grid coarsened x{args.coarsening}, "
+                               f"Jacobi-PCG to 1e-2 from its own two-level start)"
                                if args.coarsening else "")
                             + ("" if args.no_learned else
                                ", step along the U-Net correction (network trained at 128^3, applied on the grid restricted x2)"),

@@ -386,9 +386,10 @@ XsStatus projection_vjp(cudaStream_t st, const Grid& g, const XsPressureSolve& s
             if ((s = galerkin_combine(st, g, anchor, mask, pb, h, true, nullptr, 0, nullptr, h.ring_start, pa)) != XS_OK) return s;
             adj.initial_guess = h.ring_start;
             if (coarse) {
-                if ((s = start_residual(st, g, anchor, mask, pb, nullptr, h.ring_start, h.residual, pa)) != XS_OK) return s;
+                if ((s = jacobi_sweeps(st, g, anchor, mask, pb, nullptr, pa, h.ring_start, h.extra_product, h.start)) != XS_OK) return s;
+                if ((s = start_residual(st, g, anchor, mask, pb, nullptr, h.start, h.residual, pa)) != XS_OK) return s;
                 if ((s = coarse_correction(st, g, anchor, pb, h, h.residual)) != XS_OK) return s;
-                if ((s = line_step(st, g, anchor, mask, pb, h, h.correction, h.ring_start, h.residual, h.start)) != XS_OK) return s;
+                if ((s = line_step(st, g, anchor, mask, pb, h, h.correction, h.start, h.residual, h.start)) != XS_OK) return s;
                 adj.initial_guess = h.start;
             }
         }

@@ -1274,15 +1274,27 @@ bool coarse_grid(const Grid& g, uint32_t coarsening, Grid& coarse) {
     return true;
 }
 
+uint32_t second_coarsening(const Grid& coarse) {
+    Grid c2;
+    for (uint32_t f : {4u, 2u})
+        if (coarse_grid(coarse, f, c2) && c2.nx >= 8 && c2.ny >= 8 && c2.nz >= 8) return f;
+    return 0;
+}
+
 size_t warm_history_bytes(const Grid& g, uint32_t history, uint32_t coarsening) {
     if (history == 0) return 0;
     const size_t n = cell_count(g);
     size_t bytes = align_up(256, 256) + (2 * history + 4) * align_up(n * 4, 256) +
                    align_up(sizeof(double) * kGramBlocks * (kMaxBasis * (kMaxBasis + 1) / 2 + kMaxBasis), 256) + 256;
-    Grid c;
+    Grid c, c2;
     if (coarse_grid(g, coarsening, c)) {
         const size_t nc = cell_count(c);
         bytes += align_up(n * 4, 256) + align_up(nc * 8, 256) + align_up(nc * 4, 256) + align_up(pressure_workspace_bytes(c), 256);
+        const uint32_t f2 = second_coarsening(c);
+        if (f2 && coarse_grid(c, f2, c2)) {
+            const size_t nc2 = cell_count(c2);
+            bytes += 5 * align_up(nc * 4, 256) + align_up(nc2 * 8, 256) + align_up(nc2 * 4, 256) + align_up(pressure_workspace_bytes(c2), 256);
+        }
     }
     return bytes;
 }
@@ -1317,6 +1329,19 @@ WarmHistory carve_warm_history(void* base, const Grid& g, uint32_t history, uint
         h.coarse_rhs = reinterpret_cast<double*>(take(nc * 8));
         h.coarse_solution = reinterpret_cast<float*>(take(nc * 4));
         h.coarse_solver = take(pressure_workspace_bytes(h.coarse));
+        const uint32_t f2 = second_coarsening(h.coarse);
+        if (f2 && coarse_grid(h.coarse, f2, h.coarsest)) {
+            const size_t nc2 = cell_count(h.coarsest);
+            h.coarsening2 = f2;
+            h.coarse_start = reinterpret_cast<float*>(take(nc * 4));
+            h.coarse_tmp = reinterpret_cast<float*>(take(nc * 4));
+            h.coarse_residual = reinterpret_cast<float*>(take(nc * 4));
+            h.coarse_product = reinterpret_cast<float*>(take(nc * 4));
+            h.coarse_correction = reinterpret_cast<float*>(take(nc * 4));
+            h.coarsest_rhs = reinterpret_cast<double*>(take(nc2 * 8));
+            h.coarsest_solution = reinterpret_cast<float*>(take(nc2 * 4));
+            h.coarsest_solver = take(pressure_workspace_bytes(h.coarsest));
+        }
     }
     return h;
 }
@@ -1423,35 +1448,78 @@ __global__ void coarse_prolong_kernel(Grid g, Grid c, float inv_f, const float* 
     }
 }
 
-XsStatus coarse_correction(cudaStream_t st, const Grid& g, uint32_t anchor, const XsScalarBoundary& pb, const WarmHistory& h, const float* r) {
-    if (h.coarsening < 2 || !h.correction || !h.coarse_rhs || !h.coarse_solution || !h.coarse_solver || !r) return XS_INVALID_ARGUMENT;
-    const Grid& c = h.coarse;
-    const uint32_t f = h.coarsening;
-    const uint64_t n = cell_count(g), nc = cell_count(c);
-    coarse_restrict_kernel<<<static_cast<unsigned>(std::min<uint64_t>((nc + 255) / 256, 148 * 16)), 256, 0, st>>>(g, c, f, r, h.coarse_rhs,
+namespace {
+
+XsStatus restrict_to(cudaStream_t st, const Grid& fine, const Grid& coarse, uint32_t f, const float* r, double* rc) {
+    const uint64_t nc = cell_count(coarse);
+    coarse_restrict_kernel<<<static_cast<unsigned>(std::min<uint64_t>((nc + 255) / 256, 148 * 16)), 256, 0, st>>>(fine, coarse, f, r, rc,
                                                                                                                    1.0 / static_cast<double>(f));
-    XsStatus s = check_launch();
-    if (s != XS_OK) return s;
-    // the anchor moves to the coarse cell that contains it (n: none, on both grids)
-    uint32_t anchor_c = anchor;
-    if (anchor < n) {
-        const uint64_t ax = anchor % static_cast<uint64_t>(g.nx), ay = (anchor / static_cast<uint64_t>(g.nx)) % static_cast<uint64_t>(g.ny),
-                       az = anchor / (static_cast<uint64_t>(g.nx) * static_cast<uint64_t>(g.ny));
-        anchor_c = static_cast<uint32_t>(ax / f + static_cast<uint64_t>(c.nx) * (ay / f + static_cast<uint64_t>(c.ny) * (az / f)));
-    }
+    return check_launch();
+}
+
+XsStatus prolong_from(cudaStream_t st, const Grid& fine, const Grid& coarse, uint32_t f, const float* ec, float* out) {
+    const uint64_t n = cell_count(fine);
+    coarse_prolong_kernel<<<static_cast<unsigned>(std::min<uint64_t>((n + 255) / 256, 148 * 16)), 256, 0, st>>>(
+        fine, coarse, 1.0f / static_cast<float>(f), ec, out);
+    return check_launch();
+}
+
+// the anchor moves to the coarse cell that contains it (n: none, on both grids)
+uint32_t coarse_anchor(const Grid& g, uint32_t f, const Grid& c, uint32_t anchor) {
+    const uint64_t n = cell_count(g);
+    if (anchor >= n) return anchor;
+    const uint64_t ax = anchor % static_cast<uint64_t>(g.nx), ay = (anchor / static_cast<uint64_t>(g.nx)) % static_cast<uint64_t>(g.ny),
+                   az = anchor / (static_cast<uint64_t>(g.nx) * static_cast<uint64_t>(g.ny));
+    return static_cast<uint32_t>(ax / f + static_cast<uint64_t>(c.nx) * (ay / f + static_cast<uint64_t>(c.ny) * (az / f)));
+}
+
+XsPressureSolve coarse_solve_settings(const float* guess) {
     XsPressureSolve cs{};
     cs.kind = XS_SOLVER_JACOBI_PCG;
     cs.max_iterations = kCoarseMaxIterations;
     cs.tolerance = kCoarseTolerance;
-    cs.initial_guess = nullptr;
+    cs.initial_guess = guess;
     cs.scale_guess = 0u;
-    // FP64 right-hand side: the adjoint form of the solve, without fixed values
-    if ((s = solve_pressure(st, c, cs, anchor_c, nullptr, pb, nullptr, h.coarse_rhs, h.coarse_solution, nullptr, h.coarse_solver, nullptr)) !=
-        XS_OK)
+    return cs;
+}
+
+}  // namespace
+
+XsStatus coarse_correction(cudaStream_t st, const Grid& g, uint32_t anchor, const XsScalarBoundary& pb, const WarmHistory& h, const float* r) {
+    if (h.coarsening < 2 || !h.correction || !h.coarse_rhs || !h.coarse_solution || !h.coarse_solver || !r) return XS_INVALID_ARGUMENT;
+    const Grid& c = h.coarse;
+    const uint32_t f = h.coarsening;
+    XsStatus s = restrict_to(st, g, c, f, r, h.coarse_rhs);
+    if (s != XS_OK) return s;
+    const uint32_t anchor_c = coarse_anchor(g, f, c, anchor);
+    const float* guess = nullptr;
+    if (h.coarsening2) {
+        // the coarse solve's own start, the same way one level down (from
+        // zero: pre-sweeps, the coarsest grid's correction, one line step);
+        // FP64 right-hand sides without fixed values on both levels
+        const Grid& c2 = h.coarsest;
+        const uint32_t f2 = h.coarsening2;
+        const uint64_t nc = cell_count(c);
+        if ((s = check_cuda(cudaMemsetAsync(h.coarse_product, 0, sizeof(float) * nc, st))) != XS_OK) return s;
+        if ((s = jacobi_sweeps(st, c, anchor_c, nullptr, pb, nullptr, h.coarse_rhs, h.coarse_product, h.coarse_tmp, h.coarse_start)) != XS_OK)
+            return s;
+        if ((s = start_residual(st, c, anchor_c, nullptr, pb, nullptr, h.coarse_start, h.coarse_residual, h.coarse_rhs)) != XS_OK) return s;
+        if ((s = restrict_to(st, c, c2, f2, h.coarse_residual, h.coarsest_rhs)) != XS_OK) return s;
+        if ((s = solve_pressure(st, c2, coarse_solve_settings(nullptr), coarse_anchor(c, f2, c2, anchor_c), nullptr, pb, nullptr,
+                                h.coarsest_rhs, h.coarsest_solution, nullptr, h.coarsest_solver, nullptr)) != XS_OK)
+            return s;
+        if ((s = prolong_from(st, c, c2, f2, h.coarsest_solution, h.coarse_correction)) != XS_OK) return s;
+        WarmHistory level = h;
+        level.extra_product = h.coarse_product;
+        if ((s = line_step(st, c, anchor_c, nullptr, pb, level, h.coarse_correction, h.coarse_start, h.coarse_residual, h.coarse_start)) !=
+            XS_OK)
+            return s;
+        guess = h.coarse_start;
+    }
+    if ((s = solve_pressure(st, c, coarse_solve_settings(guess), anchor_c, nullptr, pb, nullptr, h.coarse_rhs, h.coarse_solution, nullptr,
+                            h.coarse_solver, nullptr)) != XS_OK)
         return s;
-    coarse_prolong_kernel<<<static_cast<unsigned>(std::min<uint64_t>((n + 255) / 256, 148 * 16)), 256, 0, st>>>(
-        g, c, 1.0f / static_cast<float>(f), h.coarse_solution, h.correction);
-    return check_launch();
+    return prolong_from(st, g, c, f, h.coarse_solution, h.correction);
 }
 
 XsStatus record_coarse_iterations(cudaStream_t st, const WarmHistory& h, void* fine_workspace, const Grid& g) {
@@ -1460,6 +1528,51 @@ XsStatus record_coarse_iterations(cudaStream_t st, const WarmHistory& h, void* f
     const PressureWorkspace cw = carve_pressure_workspace(h.coarse_solver, h.coarse);
     return check_cuda(cudaMemcpyAsync(&fw.state->stats.coarse_iterations, &cw.state->stats.iterations, sizeof(uint32_t),
                                       cudaMemcpyDeviceToDevice, st));
+}
+
+template <class T>
+__global__ void jacobi_sweep_kernel(Operator op, const T* __restrict__ rhs, const float* __restrict__ x, float* __restrict__ x_out, float omega) {
+    const Grid& g = op.g;
+    const uint64_t n = cell_count(g);
+    for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
+        int cx, cy, cz;
+        decode(i, g.nx, g.ny, cx, cy, cz);
+        CellStencil s;
+        if (!stencil(op, cx, cy, cz, i, s)) {
+            x_out[i] = 0.0f;
+            continue;
+        }
+        const float xi = x[i];
+        double ax = s.diag * static_cast<double>(xi);
+#pragma unroll
+        for (int f = 0; f < 6; ++f)
+            if ((s.conn >> f) & 1u) { const uint64_t nb = s.nb[f]; if (nb != op.anchor) ax -= static_cast<double>(x[nb]); }
+        const double r = static_cast<double>(rhs[i]) + static_cast<double>(s.fixed_sum) - ax;
+        x_out[i] = static_cast<float>(static_cast<double>(xi) + omega * r / s.diag);
+    }
+}
+
+XsStatus jacobi_sweeps(cudaStream_t st, const Grid& g, uint32_t anchor, const uint32_t* mask, const XsScalarBoundary& pb, const float* rhs,
+                       const double* rhs_d, const float* x, float* tmp, float* x_out) {
+    if (!x || !tmp || !x_out || x_out == x || x_out == tmp || (!rhs && !rhs_d)) return XS_INVALID_ARGUMENT;
+    const Operator op{g, mask, anchor, pb, rhs_d == nullptr};
+    const uint64_t n = cell_count(g);
+    const unsigned blocks = static_cast<unsigned>(std::min<uint64_t>((n + 255) / 256, 148 * 16));
+    const float omega = 2.0f / 3.0f;
+    // ping-pong so that the last sweep writes x_out
+    const float* src = x;
+    for (int k = 0; k < kCoarsePreSweeps; ++k) {
+        float* dst = ((kCoarsePreSweeps - 1 - k) % 2 == 0) ? x_out : tmp;
+        if (rhs_d)
+            jacobi_sweep_kernel<double><<<blocks, 256, 0, st>>>(op, rhs_d, src, dst, omega);
+        else
+            jacobi_sweep_kernel<float><<<blocks, 256, 0, st>>>(op, rhs, src, dst, omega);
+        const XsStatus s = check_launch();
+        if (s != XS_OK) return s;
+        src = dst;
+    }
+    if (kCoarsePreSweeps == 0) return check_cuda(cudaMemcpyAsync(x_out, x, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
+    return XS_OK;
 }
 
 // ------------------------------------------------ energy-optimal line step

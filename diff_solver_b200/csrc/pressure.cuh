@@ -90,9 +90,28 @@ struct WarmHistory {
     double* coarse_rhs;     // the restricted residual (coarse cells)
     float* coarse_solution; // (coarse cells)
     void* coarse_solver;    // pressure workspace of the coarse grid
+    // the coarse solve's own start (coarsening2 > 0): pre-sweeps from zero,
+    // the coarsest grid's solution for their residual, one line step
+    uint32_t coarsening2;     // factor from the coarse grid to the coarsest
+    Grid coarsest;
+    float* coarse_start;      // (coarse cells)
+    float* coarse_tmp;        // (coarse cells)
+    float* coarse_residual;   // (coarse cells)
+    float* coarse_product;    // A of a coarse line step's direction (coarse cells)
+    float* coarse_correction; // the interpolated coarsest solution (coarse cells)
+    double* coarsest_rhs;     // (coarsest cells)
+    float* coarsest_solution; // (coarsest cells)
+    void* coarsest_solver;    // pressure workspace of the coarsest grid
 };
 constexpr double kCoarseTolerance = 1e-2;
 constexpr uint32_t kCoarseMaxIterations = 1000;
+// Damped Jacobi sweeps (weight 2/3) on the start before its residual is
+// restricted: they remove the high-frequency part of the error, which the
+// coarse grid cannot represent and CG would otherwise meet first.
+constexpr int kCoarsePreSweeps = 4;
+// The coarse grid's own coarsening for the start of its solve: 4 when its
+// extents allow (divisible, at least 8 cells after), else 2, else none.
+uint32_t second_coarsening(const Grid& coarse);
 // The coarse grid of g for a coarsening factor (false: none, or g not divisible).
 bool coarse_grid(const Grid& g, uint32_t coarsening, Grid& coarse);
 size_t warm_history_bytes(const Grid& g, uint32_t history, uint32_t coarsening = 0);
@@ -111,6 +130,11 @@ XsStatus galerkin_combine(cudaStream_t st, const Grid& g, uint32_t anchor, const
 // to kCoarseTolerance; P is trilinear interpolation at the fine cell
 // centres, clamped at the domain edges.  Grids without colliders only.
 XsStatus coarse_correction(cudaStream_t st, const Grid& g, uint32_t anchor, const XsScalarBoundary& pb, const WarmHistory& h, const float* r);
+// kCoarsePreSweeps damped Jacobi sweeps from x (FP32 rhs with fixed values,
+// or the FP64 adjoint rhs_d without), result in x_out; tmp is scratch (N).
+// x_out may not alias x or tmp.
+XsStatus jacobi_sweeps(cudaStream_t st, const Grid& g, uint32_t anchor, const uint32_t* mask, const XsScalarBoundary& pb, const float* rhs,
+                       const double* rhs_d, const float* x, float* tmp, float* x_out);
 // Copies the coarse solve's iteration count into the fine solve's statistics.
 XsStatus record_coarse_iterations(cudaStream_t st, const WarmHistory& h, void* fine_workspace, const Grid& g);
 // One energy-optimal step along a direction d from x (in place allowed):
