@@ -167,7 +167,7 @@ def finite_difference_check(grid=128, steps=50, checkpoint=10, directions=16, ep
             "checkpoints": len(traj.states)}
 
 
-def adjoint_timing(grid=256, forward=200, window=40, checkpoint=8, tolerance=1e-6, learned=False, history=5, seed=0, coarsening=4):
+def adjoint_timing(grid=256, forward=200, window=40, checkpoint=8, tolerance=1e-6, learned=False, history=5, seed=0, coarsening=2):
     from .model import ExecutionMode, tensors_of
     from .solver import TapeMode, simulate, vjp
     torch, model, ctx, params = _setup(grid, tolerance, history=history, coarsening=coarsening if history else 0)
@@ -229,7 +229,7 @@ def main(argv=None) -> int:
     a.add_argument("--tolerance", type=float, default=1e-6)
     a.add_argument("--history", type=int, default=5)
     a.add_argument("--learned", action="store_true")
-    a.add_argument("--coarsening", type=int, default=4, help="coarse-grid correction of the forward and adjoint starts (0: off)")
+    a.add_argument("--coarsening", type=int, default=2, help="coarse-grid correction of the forward and adjoint starts (0: off)")
     args = ap.parse_args(argv)
     if args.cmd == "fd":
         out = finite_difference_check(args.grid, args.steps, args.checkpoint, args.directions, args.eps, args.tolerance, args.seed)
