@@ -160,9 +160,25 @@ __device__ __forceinline__ float load_face(const float* __restrict__ v, int axis
     return __ldg(v + mapped_face(x, y, z, g, axis, b));
 }
 
+// Division by the spacing h; for a power-of-two h the product with its exact
+// reciprocal, which is the same IEEE result (see grid_coordinates below).
+struct SpacingDivider {
+    float h, r;
+    bool pow2;
+    __device__ __forceinline__ float operator()(float v) const { return pow2 ? v * r : v / h; }
+};
+__device__ __forceinline__ SpacingDivider spacing_divider(float h) {
+    SpacingDivider d;
+    d.h = h;
+    d.r = 1.0f / h;
+    d.pow2 = (__float_as_uint(h) & 0x007FFFFFu) == 0u;
+    return d;
+}
+
 // Trilinear value and gradient of an 8-value cell (operators.cu:150-163).
 __device__ __forceinline__ Sample trilinear(const float v[2][2][2], float tx, float ty, float tz, float h) {
     const float wx[2] = {1.0f - tx, tx}, wy[2] = {1.0f - ty, ty}, wz[2] = {1.0f - tz, tz};
+    const SpacingDivider over_h = spacing_divider(h);
     Sample s{0.0f, {0.0f, 0.0f, 0.0f}};
 #pragma unroll
     for (int dz = 0; dz < 2; ++dz) {
@@ -170,15 +186,15 @@ __device__ __forceinline__ Sample trilinear(const float v[2][2][2], float tx, fl
         for (int dy = 0; dy < 2; ++dy) {
 #pragma unroll
             for (int dx = 0; dx < 2; ++dx) s.value += wx[dx] * wy[dy] * wz[dz] * v[dz][dy][dx];
-            s.gradient.x += wy[dy] * wz[dz] * (v[dz][dy][1] - v[dz][dy][0]) / h;
+            s.gradient.x += over_h(wy[dy] * wz[dz] * (v[dz][dy][1] - v[dz][dy][0]));
         }
 #pragma unroll
-        for (int dx = 0; dx < 2; ++dx) s.gradient.y += wx[dx] * wz[dz] * (v[dz][1][dx] - v[dz][0][dx]) / h;
+        for (int dx = 0; dx < 2; ++dx) s.gradient.y += over_h(wx[dx] * wz[dz] * (v[dz][1][dx] - v[dz][0][dx]));
     }
 #pragma unroll
     for (int dy = 0; dy < 2; ++dy)
 #pragma unroll
-        for (int dx = 0; dx < 2; ++dx) s.gradient.z += wx[dx] * wy[dy] * (v[1][dy][dx] - v[0][dy][dx]) / h;
+        for (int dx = 0; dx < 2; ++dx) s.gradient.z += over_h(wx[dx] * wy[dy] * (v[1][dy][dx] - v[0][dy][dx]));
     return s;
 }
 
@@ -194,10 +210,26 @@ __device__ __forceinline__ float trilinear_value(const float v[2][2][2], float t
 
 // Grid coordinates of a sample point for a cell-centred field (offset 0.5
 // on every axis) or face component `axis` (offset 0 along axis).
+// A power-of-two spacing has an exact reciprocal, and both IEEE operations
+// round the same exact quotient: p * (1/h) is then bit-identical to p / h at
+// one multiply instead of a division sequence (the advection kernels issue
+// 21 of these per face and are instruction-issue bound).  Other spacings
+// divide.
 __device__ __forceinline__ void grid_coordinates(const Vec3& p, float h, int axis, float& gx, float& gy, float& gz) {
-    gx = p.x / h - (axis == 0 ? 0.0f : 0.5f);
-    gy = p.y / h - (axis == 1 ? 0.0f : 0.5f);
-    gz = p.z / h - (axis == 2 ? 0.0f : 0.5f);
+    float x, y, z;
+    if ((__float_as_uint(h) & 0x007FFFFFu) == 0u) {
+        const float r = 1.0f / h;
+        x = p.x * r;
+        y = p.y * r;
+        z = p.z * r;
+    } else {
+        x = p.x / h;
+        y = p.y / h;
+        z = p.z / h;
+    }
+    gx = x - (axis == 0 ? 0.0f : 0.5f);
+    gy = y - (axis == 1 ? 0.0f : 0.5f);
+    gz = z - (axis == 2 ? 0.0f : 0.5f);
 }
 
 // True when the 2x2x2 stencil with lower corner (x0, y0, z0) lies inside an
