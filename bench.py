@@ -356,8 +356,10 @@ def product_run(args, world, rank, local):
         from diff_solver_b200.warm_start import WarmStartNetwork
         if not os.path.exists(args.weights):
             raise FileNotFoundError(f"{args.weights} is missing: train it with python -m diff_solver_b200.train_warm_start")
-        # trained at 128^3, applied fully convolutionally on the grid restricted x2
-        network = WarmStartNetwork(tuple(s // 2 for s in args.shape), factor=2)
+        # trained at 128^3, applied fully convolutionally on the grid restricted
+        # x network_factor (2 by default)
+        f = args.network_factor
+        network = WarmStartNetwork(tuple(s // f for s in args.shape), factor=f)
         network.load(args.weights)
     # spin-up from rest with the fastest start; its final state opens every arm
     spin = Rollout(args.shape, HISTORY, network, args.coarsening)
@@ -415,6 +417,7 @@ def main():
     ap.add_argument("--no-learned", action="store_true", help="plain and history arms only")
     ap.add_argument("--weights", default=WEIGHTS, help="warm-start network parameters (.npz)")
     ap.add_argument("--coarsening", type=int, default=COARSENING, help="coarse-grid correction factor (0: off)")
+    ap.add_argument("--network-factor", type=int, default=2, help="restriction from the grid to the network's grid (1, 2 or 4)")
     ap.add_argument("--arms", default="", help="comma-separated subset of the arms, headline last (profiling; no roofline "
                                                "or CPU baseline without the plain arm)")
     args = ap.parse_args()
@@ -431,7 +434,8 @@ def main():
                                f"Jacobi-PCG to 1e-2 from its own two-level start)"
                                if args.coarsening else "")
                             + ("" if args.no_learned else
-                               ", step along the U-Net correction (network trained at 128^3, applied on the grid restricted x2)"),
+                               f", step along the U-Net correction (network trained at 128^3, applied on the grid restricted "
+                               f"x{args.network_factor})"),
               "l2": f"inputs larger than L2 (state {n * 21 * 4 / 1e6:.0f} MB)", "parallelism": f"replicas{world}"}
     if args.impl == "reference":
         if rank == 0:

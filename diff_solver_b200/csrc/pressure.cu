@@ -606,6 +606,81 @@ __device__ void update_fast(const PcgArgs& a, const FastGeom& f, float alpha, bo
     }
 }
 
+// ------------------------------------------- stencil passes, fast path
+// The warm start's passes outside the CG iteration (sweeps, residuals,
+// operator products) on grids the fast path serves that also have no anchor
+// cell and no non-zero fixed boundary values: A x for the 4 cells of a row
+// a thread owns, accumulated in FP64 like the general path.  (For a smooth
+// field A x is a small difference of large terms: accumulated in FP32, the
+// stored products of the ring lost most of their digits and the Galerkin
+// start measured 1.5-2x more CG iterations.)
+struct Double4 {
+    double x, y, z, w;
+};
+
+__device__ __forceinline__ Double4 apply4(const FastGeom& f, const float* __restrict__ x, uint32_t i, float4& c, float4& d) {
+    const uint32_t row = fastdiv(i, f.dnx);
+    const uint32_t x0 = i - row * f.nx;
+    const uint32_t z = fastdiv(row, f.dny);
+    const uint32_t y = row - z * f.ny;
+    const RowGeom rg = row_geom(f, y, z);
+    int32_t left, right;
+    x_geom(f, x0, rg.dyz, left, right, d);
+    c = ld4(x + i);
+    Double4 q{static_cast<double>(d.x) * c.x, static_cast<double>(d.y) * c.y, static_cast<double>(d.z) * c.z,
+              static_cast<double>(d.w) * c.w};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (rg.off[k] != 0) {
+            const float4 v = ld4(x + static_cast<uint32_t>(static_cast<int32_t>(i) + rg.off[k]));
+            q.x -= v.x; q.y -= v.y; q.z -= v.z; q.w -= v.w;
+        }
+    }
+    if (left != 0) q.x -= x[static_cast<uint32_t>(static_cast<int32_t>(i) + left)];
+    if (right != 0) q.w -= x[static_cast<uint32_t>(static_cast<int32_t>(i) + right)];
+    q.x -= c.y;
+    q.y -= static_cast<double>(c.x) + c.z;
+    q.z -= static_cast<double>(c.y) + c.w;
+    q.w -= c.z;
+    return q;
+}
+
+__device__ __forceinline__ float4 round4(const Double4& v) {
+    return make_float4(static_cast<float>(v.x), static_cast<float>(v.y), static_cast<float>(v.z), static_cast<float>(v.w));
+}
+
+__device__ __forceinline__ Double4 ld4_rhs(const float* p) {
+    const float4 v = ld4(p);
+    return Double4{v.x, v.y, v.z, v.w};
+}
+__device__ __forceinline__ Double4 ld4_rhs(const double* p) {
+    const double2 a = *reinterpret_cast<const double2*>(p), b = *reinterpret_cast<const double2*>(p + 2);
+    return Double4{a.x, a.y, b.x, b.y};
+}
+
+enum FastPass { kPassJacobi = 0, kPassResidual = 1, kPassApply = 2 };
+
+// kPassJacobi: out = x + omega (b - A x) / diag; kPassResidual: out = b - A x;
+// kPassApply: out = A x.
+template <int kPass, class T>
+__global__ void fast_pass_kernel(FastGeom f, const float* __restrict__ x, const T* __restrict__ rhs, float* __restrict__ out, float omega) {
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < f.groups; t += gridDim.x * blockDim.x) {
+        const uint32_t i = 4u * t;
+        float4 c, d;
+        const Double4 q = apply4(f, x, i, c, d);
+        if (kPass == kPassApply) {
+            st4(out + i, round4(q));
+        } else {
+            const Double4 b = ld4_rhs(rhs + i);
+            const Double4 r{b.x - q.x, b.y - q.y, b.z - q.z, b.w - q.w};
+            if (kPass == kPassResidual)
+                st4(out + i, round4(r));
+            else
+                st4(out + i, round4(Double4{c.x + omega * r.x / d.x, c.y + omega * r.y / d.y, c.z + omega * r.z / d.z, c.w + omega * r.w / d.w}));
+        }
+    }
+}
+
 constexpr uint32_t kMaxRefinements = 4;
 
 // Register caps measured at 256^3: the plain solve is fastest at 4 blocks
@@ -942,6 +1017,45 @@ XsStatus launch_cooperative(void (*kernel)(Args), unsigned blocks, Args& args, c
 
 }  // namespace
 
+namespace {
+
+FastGeom fast_geom(const Grid& g, uint32_t anchor, const XsScalarBoundary& pb) {
+    const uint64_t n = cell_count(g);
+    FastGeom f{};
+    f.nx = static_cast<uint32_t>(g.nx);
+    f.ny = static_cast<uint32_t>(g.ny);
+    f.nz = static_cast<uint32_t>(g.nz);
+    f.n = static_cast<uint32_t>(n);
+    f.groups = static_cast<uint32_t>(n / 4);
+    f.dnx = make_fastdiv(f.nx);
+    f.dny = make_fastdiv(f.ny);
+    f.anchor = anchor < n ? anchor : static_cast<uint32_t>(n);
+    for (int face = 0; face < 6; ++face) {
+        const int d = face / 2;
+        const bool per = pb.modes[2 * d] == 2u && pb.modes[2 * d + 1] == 2u;
+        f.kind[face] = per ? 2u : (pb.modes[face] == 0u ? 1u : 0u);
+    }
+    return f;
+}
+
+// The stencil passes' fast path: the PCG's fast-path grids without an anchor
+// cell and, where b carries them (fixed_values), without non-zero fixed
+// boundary values.
+bool fast_pass_ok(const Grid& g, const uint32_t* mask, uint32_t anchor, const XsScalarBoundary& pb, bool fixed_values) {
+    const uint64_t n = cell_count(g);
+    if (mask != nullptr || g.nx % 4 != 0 || n >= (1ull << 31) || anchor < n) return false;
+    if (fixed_values)
+        for (int face = 0; face < 6; ++face)
+            if (pb.modes[face] == 0u && pb.values[face] != 0.0f) return false;
+    return true;
+}
+
+unsigned fast_pass_blocks(const Grid& g) {
+    return static_cast<unsigned>(std::min<uint64_t>((cell_count(g) / 4 + 255) / 256, 148 * 16));
+}
+
+}  // namespace
+
 XsStatus solve_pressure(cudaStream_t stream, const Grid& g, const XsPressureSolve& solve, uint32_t anchor, const uint32_t* mask,
                         const XsScalarBoundary& pb, const float* rhs_f, const double* rhs_d, float* pressure_out,
                         double* solution_out, void* workspace, PressureWorkspace* carved) {
@@ -985,22 +1099,7 @@ XsStatus solve_pressure(cudaStream_t stream, const Grid& g, const XsPressureSolv
     a.max_iterations = solve.max_iterations;
     const uint64_t n = cell_count(g);
     a.use_fast = (mask == nullptr && g.nx % 4 == 0 && n < (1ull << 31)) ? 1u : 0u;
-    if (a.use_fast) {
-        FastGeom& f = a.fast;
-        f.nx = static_cast<uint32_t>(g.nx);
-        f.ny = static_cast<uint32_t>(g.ny);
-        f.nz = static_cast<uint32_t>(g.nz);
-        f.n = static_cast<uint32_t>(n);
-        f.groups = static_cast<uint32_t>(n / 4);
-        f.dnx = make_fastdiv(f.nx);
-        f.dny = make_fastdiv(f.ny);
-        f.anchor = anchor < n ? anchor : static_cast<uint32_t>(n);
-        for (int face = 0; face < 6; ++face) {
-            const int d = face / 2;
-            const bool per = pb.modes[2 * d] == 2u && pb.modes[2 * d + 1] == 2u;
-            f.kind[face] = per ? 2u : (pb.modes[face] == 0u ? 1u : 0u);
-        }
-    }
+    if (a.use_fast) a.fast = fast_geom(g, anchor, pb);
     const unsigned fast_blocks = persistent_blocks(lim.pcg_fast_blocks_per_sm[a.smooth], lim.sms, n / 4);
     const unsigned blocks = persistent_blocks(lim.pcg_blocks_per_sm[a.smooth], lim.sms, n);
     if (a.use_fast)
@@ -1248,6 +1347,21 @@ __global__ void history_push_kernel(Operator op, const T* __restrict__ pressure,
     for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         dst[i] = static_cast<float>(pressure[i]);
         prod[i] = apply_at(op, pressure, i);
+    }
+}
+
+// history_push_kernel<float> on the stencil passes' fast path
+__global__ void fast_push_kernel(FastGeom f, const float* __restrict__ pressure, HistorySlots slots, HistorySlots products, uint32_t history,
+                                 const uint32_t* meta) {
+    const uint32_t k = min(meta[1], history - 1);
+    float* dst = slots.s[k];
+    float* prod = products.s[k];
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < f.groups; t += gridDim.x * blockDim.x) {
+        const uint32_t i = 4u * t;
+        float4 c, d;
+        const Double4 q = apply4(f, pressure, i, c, d);
+        st4(dst + i, c);
+        st4(prod + i, round4(q));
     }
 }
 
@@ -1560,10 +1674,16 @@ XsStatus jacobi_sweeps(cudaStream_t st, const Grid& g, uint32_t anchor, const ui
     const unsigned blocks = static_cast<unsigned>(std::min<uint64_t>((n + 255) / 256, 148 * 16));
     const float omega = 2.0f / 3.0f;
     // ping-pong so that the last sweep writes x_out
+    const bool fast = fast_pass_ok(g, mask, anchor, pb, rhs_d == nullptr);
+    const FastGeom f = fast ? fast_geom(g, anchor, pb) : FastGeom{};
     const float* src = x;
     for (int k = 0; k < kCoarsePreSweeps; ++k) {
         float* dst = ((kCoarsePreSweeps - 1 - k) % 2 == 0) ? x_out : tmp;
-        if (rhs_d)
+        if (fast && rhs_d)
+            fast_pass_kernel<kPassJacobi, double><<<fast_pass_blocks(g), 256, 0, st>>>(f, src, rhs_d, dst, omega);
+        else if (fast)
+            fast_pass_kernel<kPassJacobi, float><<<fast_pass_blocks(g), 256, 0, st>>>(f, src, rhs, dst, omega);
+        else if (rhs_d)
             jacobi_sweep_kernel<double><<<blocks, 256, 0, st>>>(op, rhs_d, src, dst, omega);
         else
             jacobi_sweep_kernel<float><<<blocks, 256, 0, st>>>(op, rhs, src, dst, omega);
@@ -1591,7 +1711,10 @@ XsStatus line_step(cudaStream_t st, const Grid& g, uint32_t anchor, const uint32
     const Operator op{g, mask, anchor, pb, true};
     const uint64_t n = cell_count(g);
     const unsigned grid = static_cast<unsigned>(std::min<uint64_t>((n + 255) / 256, 148 * 16));
-    apply_operator_kernel<<<grid, 256, 0, st>>>(op, d, h.extra_product);
+    if (fast_pass_ok(g, mask, anchor, pb, false))
+        fast_pass_kernel<kPassApply, float><<<fast_pass_blocks(g), 256, 0, st>>>(fast_geom(g, anchor, pb), d, nullptr, h.extra_product, 0.0f);
+    else
+        apply_operator_kernel<<<grid, 256, 0, st>>>(op, d, h.extra_product);
     XsStatus s = check_launch();
     if (s != XS_OK) return s;
     // the Galerkin machinery with the one vector d and b = r (r already holds
@@ -1621,10 +1744,17 @@ XsStatus start_residual(cudaStream_t st, const Grid& g, uint32_t anchor, const u
     const Operator op{g, mask, anchor, pb, rhs_d == nullptr};
     const uint64_t n = cell_count(g);
     const unsigned blocks = static_cast<unsigned>(std::min<uint64_t>((n + 255) / 256, 148 * 16));
-    if (rhs_d)
+    if (fast_pass_ok(g, mask, anchor, pb, rhs_d == nullptr)) {
+        const FastGeom f = fast_geom(g, anchor, pb);
+        if (rhs_d)
+            fast_pass_kernel<kPassResidual, double><<<fast_pass_blocks(g), 256, 0, st>>>(f, x, rhs_d, r, 0.0f);
+        else
+            fast_pass_kernel<kPassResidual, float><<<fast_pass_blocks(g), 256, 0, st>>>(f, x, rhs, r, 0.0f);
+    } else if (rhs_d) {
         start_residual_kernel<double><<<blocks, 256, 0, st>>>(op, rhs_d, x, r);
-    else
+    } else {
         start_residual_kernel<float><<<blocks, 256, 0, st>>>(op, rhs, x, r);
+    }
     return check_launch();
 }
 
@@ -1641,6 +1771,8 @@ XsStatus history_push(cudaStream_t st, const Grid& g, uint32_t anchor, const uin
     const unsigned blocks = static_cast<unsigned>(std::min<uint64_t>((n + 255) / 256, 148 * 16));
     if (pressure64)
         history_push_kernel<double><<<blocks, 256, 0, st>>>(op, pressure64, slots, products, h.history, h.meta);
+    else if (fast_pass_ok(g, mask, anchor, pb, false))
+        fast_push_kernel<<<fast_pass_blocks(g), 256, 0, st>>>(fast_geom(g, anchor, pb), pressure, slots, products, h.history, h.meta);
     else
         history_push_kernel<float><<<blocks, 256, 0, st>>>(op, pressure, slots, products, h.history, h.meta);
     XsStatus s = check_launch();
