@@ -430,7 +430,7 @@ def main():
     config = {"workload": f"smoke plume {name} after a {args.spinup}-step spin-up from rest, Jacobi-PCG to rel. residual 1e-6",
               "grid": list(args.shape), "cells": n, "dt": "0.5 dx", "steps_per_replica": args.steps, "spinup_steps": args.spinup,
               "warm_start": f"Galerkin start over the last {HISTORY} solutions"
-                            + (f", 4 Jacobi sweeps and a step along the coarse-grid correction (grid coarsened x{args.coarsening}, "
+                            + (f", 6 Jacobi sweeps and a step along the coarse-grid correction (grid coarsened x{args.coarsening}, "
                                f"Jacobi-PCG to 1e-2 from its own two-level start)"
                                if args.coarsening else "")
                             + ("" if args.no_learned else

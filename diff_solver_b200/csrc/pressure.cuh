@@ -108,7 +108,7 @@ constexpr uint32_t kCoarseMaxIterations = 1000;
 // Damped Jacobi sweeps (weight 2/3) on the start before its residual is
 // restricted: they remove the high-frequency part of the error, which the
 // coarse grid cannot represent and CG would otherwise meet first.
-constexpr int kCoarsePreSweeps = 4;
+constexpr int kCoarsePreSweeps = 6;
 // The coarse grid's own coarsening for the start of its solve: 4 when its
 // extents allow (divisible, at least 8 cells after), else 2, else none.
 uint32_t second_coarsening(const Grid& coarse);

@@ -313,7 +313,7 @@ typedef struct XsSmokeModel {
     uint32_t warm_start_history;
     /* coarse-grid correction of the forward start (0: off; otherwise the
      * coarsening factor per axis, which must divide the grid; needs
-     * warm_start_history > 0 and no colliders).  The ring's start takes 4
+     * warm_start_history > 0 and no colliders).  The ring's start takes 6
      * damped Jacobi sweeps; their residual is restricted to the coarse grid,
      * solved there by Jacobi-PCG to 1e-2 relative residual (from the same
      * kind of start one level further down, when the coarse grid divides
