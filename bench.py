@@ -166,11 +166,14 @@ def barrier(world):
 
 
 def max_over_ranks(value, world):
+    """The slowest rank's figure (NCCL groups reduce on the device, gloo on
+    the host)."""
     if world == 1:
         return value
     import torch
     import torch.distributed as dist
-    t = torch.tensor([value], dtype=torch.float64, device="cuda")
+    device = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([value], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
