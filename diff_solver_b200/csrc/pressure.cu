@@ -217,6 +217,7 @@ struct PcgArgs {
     FastGeom fast;
     uint32_t use_fast;
     uint32_t smooth;      // minimal-residual smoothing of the iterates (warm starts)
+    uint32_t fast_residual;  // residual_fast serves the residual phases (fast path, no anchor, no fixed values)
 };
 
 enum ResidualMode { kFromZero = 0, kFromGuess = 1, kFromX64 = 2 };
@@ -681,6 +682,101 @@ __global__ void fast_pass_kernel(FastGeom f, const float* __restrict__ x, const 
     }
 }
 
+// residual_phase on the fast path for grids without an anchor cell and with
+// no non-zero fixed boundary values (then every cell is an unknown and b is
+// the right-hand side alone): 4 cells of a row per thread, the same FP64
+// arithmetic per cell.
+__device__ __forceinline__ double rhs_at4(const PcgArgs& a, uint32_t i, int k) {
+    return a.rhs_d ? a.rhs_d[i + k] : static_cast<double>(a.rhs_f[i + k]);
+}
+
+template <class T>
+__device__ __forceinline__ void load_x4(const T* __restrict__ v, uint32_t i, double (&c)[4]) {
+#pragma unroll
+    for (int k = 0; k < 4; ++k) c[k] = static_cast<double>(v[i + k]);
+}
+
+// A x for the 4 cells at i: x is the guess (FP32) or the FP64 iterate.
+template <class T>
+__device__ __forceinline__ void apply4_fp64(const FastGeom& f, const T* __restrict__ x, uint32_t i, double (&c)[4], double (&ax)[4],
+                                            float4& d) {
+    const uint32_t row = fastdiv(i, f.dnx);
+    const uint32_t x0 = i - row * f.nx;
+    const uint32_t z = fastdiv(row, f.dny);
+    const uint32_t y = row - z * f.ny;
+    const RowGeom rg = row_geom(f, y, z);
+    int32_t left, right;
+    x_geom(f, x0, rg.dyz, left, right, d);
+    load_x4(x, i, c);
+    const float dd[4] = {d.x, d.y, d.z, d.w};
+#pragma unroll
+    for (int k = 0; k < 4; ++k) ax[k] = static_cast<double>(dd[k]) * c[k];
+#pragma unroll
+    for (int q = 0; q < 4; ++q) {
+        if (rg.off[q] != 0) {
+            double v[4];
+            load_x4(x, static_cast<uint32_t>(static_cast<int32_t>(i) + rg.off[q]), v);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) ax[k] -= v[k];
+        }
+    }
+    if (left != 0) ax[0] -= static_cast<double>(x[static_cast<uint32_t>(static_cast<int32_t>(i) + left)]);
+    if (right != 0) ax[3] -= static_cast<double>(x[static_cast<uint32_t>(static_cast<int32_t>(i) + right)]);
+    ax[0] -= c[1];
+    ax[1] -= c[0] + c[2];
+    ax[2] -= c[1] + c[3];
+    ax[3] -= c[2];
+}
+
+__device__ void residual_fast(const PcgArgs& a, const FastGeom& f, int mode, double (&v)[3], double scale = 1.0) {
+    v[0] = v[1] = v[2] = 0.0;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < f.groups; t += gridDim.x * blockDim.x) {
+        const uint32_t i = 4u * t;
+        double xi[4] = {0.0, 0.0, 0.0, 0.0}, ax[4] = {0.0, 0.0, 0.0, 0.0};
+        float4 d4;
+        if (mode == kFromGuess) {
+            apply4_fp64(f, a.guess, i, xi, ax, d4);
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+                xi[k] *= scale;
+                ax[k] *= scale;
+            }
+        } else if (mode == kFromX64) {
+            apply4_fp64(f, a.x64, i, xi, ax, d4);
+        } else {
+            const uint32_t row = fastdiv(i, f.dnx);
+            const uint32_t z = fastdiv(row, f.dny);
+            const RowGeom rg = row_geom(f, row - z * f.ny, z);
+            int32_t left, right;
+            x_geom(f, i - row * f.nx, rg.dyz, left, right, d4);
+        }
+        const float dd[4] = {d4.x, d4.y, d4.z, d4.w};
+        float zf[4];
+#pragma unroll
+        for (int k = 0; k < 4; ++k) {
+            const double b = rhs_at4(a, i, k);
+            const double r = b - ax[k];
+            zf[k] = static_cast<float>(r / dd[k]);
+            v[0] += b * b;
+            v[1] += r * r;
+            v[2] += r * static_cast<double>(zf[k]);
+            if (mode != kFromX64) a.x64[i + k] = xi[k];
+            if (a.solution_out) a.solution_out[i + k] = xi[k];
+        }
+        const float4 z4 = make_float4(zf[0], zf[1], zf[2], zf[3]);
+        st4(a.z + i, z4);
+        st4(a.p[0] + i, z4);
+        st4(a.e + i, make_float4(0.0f, 0.0f, 0.0f, 0.0f));
+        if (a.smooth) {  // the smoothed sequence starts at the pass' start
+            st4(a.s + i, make_float4(zf[0] * dd[0], zf[1] * dd[1], zf[2] * dd[2], zf[3] * dd[3]));
+            st4(a.y + i, make_float4(0.0f, 0.0f, 0.0f, 0.0f));
+        }
+        if (a.pressure_out)
+            st4(a.pressure_out + i, make_float4(static_cast<float>(xi[0]), static_cast<float>(xi[1]), static_cast<float>(xi[2]),
+                                                static_cast<float>(xi[3])));
+    }
+}
+
 constexpr uint32_t kMaxRefinements = 4;
 
 // Register caps measured at 256^3: the plain solve is fastest at 4 blocks
@@ -698,7 +794,8 @@ __global__ void __launch_bounds__(kBlock, kSmooth ? 3 : 4) pcg_kernel(PcgArgs a)
         if (!grid_reduce<2>(st, a.partials, e2, red)) return;
         scale = (e2[1] > 0.0 && isfinite(e2[0] / e2[1])) ? e2[0] / e2[1] : 0.0;
     }
-    residual_phase(a, a.guess ? kFromGuess : kFromZero, v3, scale);
+    if (kFast && a.fast_residual) residual_fast(a, a.fast, a.guess ? kFromGuess : kFromZero, v3, scale);
+    else residual_phase(a, a.guess ? kFromGuess : kFromZero, v3, scale);
     if (!grid_reduce<3>(st, a.partials, v3, red)) return;
     const double bb = v3[0];
     double rr = v3[1], rz = v3[2];
@@ -706,7 +803,8 @@ __global__ void __launch_bounds__(kBlock, kSmooth ? 3 : 4) pcg_kernel(PcgArgs a)
     if (a.guess && !(rr <= bb)) {  // the guess is worse than zero: fall back
         warm = 0u;
         scale = 0.0;
-        residual_phase(a, kFromZero, v3);
+        if (kFast && a.fast_residual) residual_fast(a, a.fast, kFromZero, v3);
+        else residual_phase(a, kFromZero, v3);
         if (!grid_reduce<3>(st, a.partials, v3, red)) return;
         rr = v3[1];
         rz = v3[2];
@@ -791,7 +889,8 @@ __global__ void __launch_bounds__(kBlock, kSmooth ? 3 : 4) pcg_kernel(PcgArgs a)
         if (smoothed) fold_smoothed_phase(a, k, alpha, eta_final);
         else fold_phase(a, k, alpha);
         if (!grid_barrier(st, a.partials, red)) return;
-        residual_phase(a, kFromX64, v3);
+        if (kFast && a.fast_residual) residual_fast(a, a.fast, kFromX64, v3);
+        else residual_phase(a, kFromX64, v3);
         if (!grid_reduce<3>(st, a.partials, v3, red)) return;
         rr = v3[1];
         rz = v3[2];
@@ -1100,6 +1199,7 @@ XsStatus solve_pressure(cudaStream_t stream, const Grid& g, const XsPressureSolv
     const uint64_t n = cell_count(g);
     a.use_fast = (mask == nullptr && g.nx % 4 == 0 && n < (1ull << 31)) ? 1u : 0u;
     if (a.use_fast) a.fast = fast_geom(g, anchor, pb);
+    a.fast_residual = (a.use_fast && fast_pass_ok(g, mask, anchor, pb, rhs_d == nullptr)) ? 1u : 0u;
     const unsigned fast_blocks = persistent_blocks(lim.pcg_fast_blocks_per_sm[a.smooth], lim.sms, n / 4);
     const unsigned blocks = persistent_blocks(lim.pcg_blocks_per_sm[a.smooth], lim.sms, n);
     if (a.use_fast)
