@@ -198,16 +198,6 @@ __device__ __forceinline__ Sample trilinear(const float v[2][2][2], float tx, fl
     return s;
 }
 
-__device__ __forceinline__ float trilinear_value(const float v[2][2][2], float tx, float ty, float tz) {
-    const float x00 = v[0][0][0] + tx * (v[0][0][1] - v[0][0][0]);
-    const float x01 = v[0][1][0] + tx * (v[0][1][1] - v[0][1][0]);
-    const float x10 = v[1][0][0] + tx * (v[1][0][1] - v[1][0][0]);
-    const float x11 = v[1][1][0] + tx * (v[1][1][1] - v[1][1][0]);
-    const float y0 = x00 + ty * (x01 - x00);
-    const float y1 = x10 + ty * (x11 - x10);
-    return y0 + tz * (y1 - y0);
-}
-
 // Grid coordinates of a sample point for a cell-centred field (offset 0.5
 // on every axis) or face component `axis` (offset 0 along axis).
 // A power-of-two spacing has an exact reciprocal, and both IEEE operations
