@@ -32,6 +32,27 @@ namespace xs {
 // ------------------------------------------------------------------ TMA maps
 namespace {
 
+// A set-up call that must run once per device (a kernel attribute applies to
+// the device and context it was set on), thread-safe.
+class DeviceOnce {
+public:
+    template <class F>
+    bool run(F&& f) {
+        int device = 0;
+        if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= kMaxDevices) return false;
+        std::lock_guard<std::mutex> lock(mu_);
+        if (done_[device]) return true;
+        if (f() != cudaSuccess) return false;
+        done_[device] = true;
+        return true;
+    }
+
+private:
+    static constexpr int kMaxDevices = 64;
+    std::mutex mu_;
+    bool done_[kMaxDevices] = {};
+};
+
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
     static std::once_flag once;
@@ -211,12 +232,9 @@ XsStatus launch_conv_forward(cudaStream_t st, const VolumeShape& s, const __nv_b
     CUtensorMap am, wm;
     if (!make_activation_map(&am, in, s, CIN, bx, by) || !make_weight_map(&wm, w, COUT, CIN)) return XS_CUDA_ERROR;
     using L = ConvSmem<CIN, COUT>;
-    static bool configured = false;
-    if (!configured) {
-        if (cudaFuncSetAttribute(conv3_forward_kernel<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::total) != cudaSuccess)
-            return XS_CUDA_ERROR;
-        configured = true;
-    }
+    static DeviceOnce configured;
+    if (!configured.run([] { return cudaFuncSetAttribute(conv3_forward_kernel<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::total); }))
+        return XS_CUDA_ERROR;
     ConvArgs args{s, bx, by, bias, out, relu ? 1 : 0, error};
     const uint64_t tiles = static_cast<uint64_t>(s.batch) * s.z * (s.y / by) * (s.x / bx);
     conv3_forward_kernel<CIN, COUT><<<static_cast<unsigned>(tiles), kConvThreads, L::total, st>>>(am, wm, args);
@@ -408,12 +426,9 @@ XsStatus launch_wgrad(cudaStream_t st, const VolumeShape& s, const __nv_bfloat16
     if (!conv_tile(s, bx, by)) return XS_INVALID_ARGUMENT;
     CUtensorMap xm, ym;
     if (!make_activation_map(&xm, x, s, CIN, bx, by) || !make_activation_map(&ym, dy, s, COUT, bx, by)) return XS_CUDA_ERROR;
-    static bool configured = false;
-    if (!configured) {
-        if (cudaFuncSetAttribute(conv3_wgrad_kernel<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::total) != cudaSuccess)
-            return XS_CUDA_ERROR;
-        configured = true;
-    }
+    static DeviceOnce configured;
+    if (!configured.run([] { return cudaFuncSetAttribute(conv3_wgrad_kernel<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::total); }))
+        return XS_CUDA_ERROR;
     const uint32_t tiles = static_cast<uint32_t>(static_cast<uint64_t>(s.batch) * s.z * (s.y / by) * (s.x / bx));
     const uint32_t ctas = wgrad_ctas(s);
     WgradArgs args{s, bx, by, tiles, partial, error};

@@ -7,14 +7,15 @@
 // allocation could fail or stall at an inconvenient time.  The regular
 // xs_pressure_solve needs a caller-provided workspace; this variant instead
 // keeps its scratch (solver control block, reduction slots, the FP64
-// iterate and the five FP32 CG vectors) in one statically sized array in
-// device memory that belongs to the library.
+// iterate and the seven FP32 vectors of the CG and smoothing recurrences) in
+// one statically sized array in device memory that belongs to the library.
 //
 // Limits and sharing:
 //  * At most XS_STATIC_SOLVE_MAX_CELLS cells; larger grids are rejected with
 //    XS_CAPACITY_EXCEEDED before anything is launched.
 //  * The array is part of this file's device module: each GPU on which the
-//    entry point is used holds it (about 7.5 MB) until the process exits.
+//    entry point is used holds it (about 9.1 MiB at the 64^3 limit) until the
+//    process exits.
 //  * All calls on a device share the one array and it keeps whatever the
 //    last call left in it; the solver zeroes its control block at the start
 //    of every call and writes every other scratch value before reading it.
@@ -24,6 +25,10 @@
 //  * The first call on a device looks up the array's device address with
 //    cudaGetSymbolAddress, with that device current, and remembers it; make
 //    that first call before any stream capture begins.
+//  * Failures inside the solve (a barrier timeout, no convergence within the
+//    iteration cap) are only reported through host_stats: with host_stats
+//    NULL the call does not synchronise, and its status covers the argument
+//    checks and the launches alone.
 #include <mutex>
 
 #include "common.cuh"

@@ -9,8 +9,11 @@
 // kind::f16: D format [4,6), A/B formats [7,10)/[10,13), A/B major bits 15/16,
 // N >> 3 in [17,23), M >> 4 in [24,29)).
 //
-// Every wait on an mbarrier is bounded: after kWaitLimit polls the caller
-// gets `false`, records an error and leaves.
+// Every wait on an mbarrier is bounded in time: once kWaitCycles SM clock
+// cycles (about 2 s) have passed without the phase completing, the caller
+// gets `false`, records an error and leaves.  The bound is on elapsed cycles,
+// not on polls: one try_wait may itself suspend the thread for a
+// hardware-defined interval.
 #pragma once
 
 #include <cstdint>
@@ -20,7 +23,7 @@
 namespace xs {
 namespace tc {
 
-constexpr uint32_t kWaitLimit = 1u << 26;
+constexpr long long kWaitCycles = 4000000000ll;  // ~2 s at 2 GHz
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return static_cast<uint32_t>(__cvta_generic_to_shared(p)); }
 
@@ -48,9 +51,11 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
 
 // Bounded wait for the phase with the given parity to complete.
 __device__ __forceinline__ bool mbar_wait(uint64_t* bar, uint32_t parity) {
-    for (uint32_t i = 0; i < kWaitLimit; ++i)
-        if (mbar_try_wait(bar, parity)) return true;
-    return false;
+    if (mbar_try_wait(bar, parity)) return true;
+    const long long start = clock64();
+    while (!mbar_try_wait(bar, parity))
+        if (clock64() - start > kWaitCycles) return false;
+    return true;
 }
 
 // 5-D tiled TMA load into shared memory, completing on `bar`.

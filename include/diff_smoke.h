@@ -231,13 +231,17 @@ XsStatus xs_pressure_solve(cudaStream_t stream, XsGrid grid, const XsPressureSol
  * that only hand over their input and output buffers, or that forbid
  * allocations outside their own pool): it takes no workspace and calls no
  * allocator; its scratch is one library-owned device array sized for at
- * most XS_STATIC_SOLVE_MAX_CELLS cells (about 7.5 MB, held by each GPU the
- * entry point runs on until the process exits).  Larger grids return
- * XS_CAPACITY_EXCEEDED without launching.  All calls share that array:
- * calls that overlap on the GPU race, so order them on one stream.  The
- * first call on a device resolves the array's address (make it before any
- * stream capture).  host_stats may be NULL; when given, the call
- * synchronises the stream and copies the solve statistics into it. */
+ * most XS_STATIC_SOLVE_MAX_CELLS cells (about 9.1 MiB: seven FP32 vectors
+ * plus the FP64 iterate at 64^3, held by each GPU the entry point runs on
+ * until the process exits).  Larger grids return XS_CAPACITY_EXCEEDED
+ * without launching.  All calls share that array: calls that overlap on the
+ * GPU race, so order them on one stream.  The first call on a device
+ * resolves the array's address (make it before any stream capture).
+ * host_stats may be NULL; when given, the call synchronises the stream and
+ * copies the solve statistics into it, and returns their status (a barrier
+ * timeout, no convergence).  With NULL it does not synchronise, and a
+ * failure inside the solve goes unreported: the status then covers only the
+ * argument checks and the launches. */
 #define XS_STATIC_SOLVE_MAX_CELLS (64u * 64u * 64u)
 XsStatus xs_pressure_solve_static(cudaStream_t stream, XsGrid grid, const XsPressureSolve* solve, uint32_t pressure_anchor,
                                   const uint32_t* cell_mask, XsScalarBoundary pressure_boundary, const float* rhs, float* pressure,

@@ -62,7 +62,7 @@ class og_config(C.Structure):
         ("temperature_boundary", og_sbnd), ("pressure_anchor", C.c_uint32), ("vorticity_enabled", C.c_uint32),
         ("solver", C.c_uint32), ("iterations", C.c_uint32), ("tolerance", C.c_double), ("inflow_count", C.c_uint32),
         ("inflows", C.c_void_p), ("cell_mask", C.c_void_p), ("collider_velocity", C.c_void_p * 3),
-        ("collider_density", C.c_void_p), ("collider_temperature", C.c_void_p),
+        ("collider_density", C.c_void_p), ("collider_temperature", C.c_void_p), ("pressure_guess", C.c_void_p),
     ]
 
 
@@ -318,8 +318,19 @@ class Problem:
                 "acceleration": [np.ascontiguousarray(v, self.dt) for v in c["acceleration"]]}
 
     # ---- step composition ---------------------------------------------------
-    def forward_step(self, state, control, params):
-        """model.cpp:341-349.  Returns (next_state, cache, stats, pressure)."""
+    def forward_step(self, state, control, params, guess=None):
+        """model.cpp:341-349.  Returns (next_state, cache, stats, scratch);
+        scratch["p"] is the pressure.  `guess` (optional, PCG kind only)
+        starts the pressure solve from the given field instead of zero: the
+        converged result is the same, a good start only saves iterations."""
+        g = None if guess is None else np.ascontiguousarray(guess, self.dt)
+        self.c.pressure_guess = None if g is None else g.ctypes.data
+        try:
+            return self._forward_step(state, control, params)
+        finally:
+            self.c.pressure_guess = None
+
+    def _forward_step(self, state, control, params):
         s = self.cast_state(state)
         u = self.cast_control(control)
         nxt = zeros_state(self.res, self.dt)

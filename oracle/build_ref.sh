@@ -3,10 +3,14 @@
 # the reference's own solvers/smoke/operators.cu, included unmodified from
 # the read-only reference checkout, compiled for sm_100a behind the small C
 # ABI of oracle/ref_harness.cu.  Nothing is copied out of the reference.
-#   REFERENCE=/path/to/diff-solver oracle/build_ref.sh
+#   oracle/build_ref.sh /path/to/diff-solver      (or REFERENCE=/path/to/diff-solver)
 set -euo pipefail
 HERE="$(cd "$(dirname "$0")" && pwd)"
-REFERENCE="${REFERENCE:-/root/reference}"
+REFERENCE="${1:-${REFERENCE:-}}"
+if [ -z "$REFERENCE" ]; then
+    echo "no reference checkout given (argument or REFERENCE); skipping the harness build" >&2
+    exit 0
+fi
 SMOKE="$REFERENCE/solvers/smoke"
 if [ ! -f "$SMOKE/operators.cu" ]; then
     echo "reference checkout not found at $REFERENCE; skipping the harness build" >&2

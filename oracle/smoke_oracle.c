@@ -80,6 +80,7 @@ typedef struct {
     const real* collider_velocity[3];     /* faces per axis, NULL = zero */
     const real* collider_density;         /* N, NULL = zero */
     const real* collider_temperature;     /* N, NULL = zero */
+    const real* pressure_guess;           /* extension: start of the forward PCG solve, NULL = zero */
 } og_config;
 
 typedef struct { real* density; real* temperature; real* velocity[3]; } og_state;
@@ -1035,7 +1036,7 @@ static void projection_forward(const og_config* c, G g, const SB* pb, real* cons
         for (uint32_t it = 0; it < c->iterations; ++it) { rbgs_sweep(c, g, pb, 0, rhs, p); rbgs_sweep(c, g, pb, 1, rhs, p); }
         if (st) { st->iterations = c->iterations; st->initial_residual = 0; st->final_residual = relative_residual(c, g, pb, rhs, p); st->converged = 1; }
     } else {
-        pcg_solve(c, g, pb, rhs, NULL, c->iterations, c->tolerance, p, st);
+        pcg_solve(c, g, pb, rhs, c->pressure_guess, c->iterations, c->tolerance, p, st);
     }
     project_velocity(c, g, u, p, out);
 }

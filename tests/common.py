@@ -186,3 +186,43 @@ def cache_arrays(k):
             "normal": [v[7], v[8], v[9]], "normalizer": v[10],
             "forced_velocity": [t.cpu().numpy() for t in k.forced_velocity.components()],
             "advected_velocity": [t.cpu().numpy() for t in k.advected_velocity.components()]}
+
+
+# ---------------------------------------------------------------- differentiable plume
+PLUME_PARAMS = dict(ambient_temperature=0.0, density_buoyancy=-0.1, temperature_buoyancy=0.5, vorticity_confinement=0.0)
+
+
+def differentiable_plume(n=128):
+    """The differentiable plume at n^3: the benchmark physics (inflow sphere
+    r = 0.08 at (0.5, 0.1, 0.5) setting density = temperature = 1, buoyancy
+    0.5 T - 0.1 rho, walls with a fixed normal velocity, open top), initial
+    velocity = seeded uniform noise in +-0.01 (FP32-representable, so the FP32
+    product and the FP64 oracle start from the same state), density and
+    temperature 0, zero controls.  The target is a Gaussian blob (sigma 0.1,
+    amplitude 1) at a seeded uniform centre in [0.3, 0.7]^3.
+    Returns (configuration, [u0 per face component], target)."""
+    cfg = plume_configuration((n, n, n), inflow_center=(0.5, 0.1, 0.5), inflow_radius=0.08)
+    rng = np.random.default_rng(0)
+    _, f = sizes((n, n, n))
+    u0 = [rng.uniform(-0.01, 0.01, f[a]).astype(np.float32).astype(np.float64) for a in range(3)]
+    centre = np.random.default_rng(1).uniform(0.3, 0.7, 3)
+    c = (np.arange(n) + 0.5) / n
+    Z, Y, X = np.meshgrid(c, c, c, indexing="ij")
+    target = np.exp(-((X - centre[0]) ** 2 + (Y - centre[1]) ** 2 + (Z - centre[2]) ** 2) / (2 * 0.1 ** 2)).reshape(-1)
+    return cfg, u0, target
+
+
+def plume_directions(n, count):
+    """The first `count` of the seeded unit directions of the finite-difference
+    check: smooth random velocity fields (Gaussian bumps per face component)
+    scaled to unit L2 norm over all faces, flattened per component."""
+    from diff_solver_b200.gradcheck import smooth_direction
+    rng = np.random.default_rng(2)
+    shapes = [(n, n, n + 1), (n, n + 1, n), (n + 1, n, n)]  # (z, y, x) extents of the face components
+    return [[x.reshape(-1) for x in smooth_direction(rng, shapes, n)] for _ in range(count)]
+
+
+def density_distance(density, target):
+    """The loss of the differentiable plume: ||rho_T - target||_2."""
+    d = np.asarray(density, np.float64) - target
+    return float(np.sqrt(d @ d))
