@@ -10,6 +10,7 @@
 // scatter with FP64 atomics to the 8 corners, as their targets depend on the
 // velocity field.  Parameter adjoints are reduced per block first.
 #include "ops.cuh"
+#include "advect_tile.cuh"
 #include "common.cuh"
 #include "launch.cuh"
 
@@ -93,57 +94,6 @@ __global__ void integrate_vjp_cells_kernel(Grid g, const uint32_t* __restrict__ 
     }
 }
 
-// ---------------------------------------------------------------- scatter
-__device__ __forceinline__ void scatter_scalar(double* v, const Vec3& p, double adj, const Grid& g, const XsScalarBoundary& b) {
-    if (adj == 0.0) return;
-    float gx, gy, gz;
-    grid_coordinates(p, g.h, -1, gx, gy, gz);
-    const int x0 = static_cast<int>(floorf(gx)), y0 = static_cast<int>(floorf(gy)), z0 = static_cast<int>(floorf(gz));
-    const double wx[2] = {1.0 - (gx - x0), static_cast<double>(gx - x0)};
-    const double wy[2] = {1.0 - (gy - y0), static_cast<double>(gy - y0)};
-    const double wz[2] = {1.0 - (gz - z0), static_cast<double>(gz - z0)};
-#pragma unroll
-    for (int dz = 0; dz < 2; ++dz)
-#pragma unroll
-        for (int dy = 0; dy < 2; ++dy)
-#pragma unroll
-            for (int dx = 0; dx < 2; ++dx) {
-                const int x = x0 + dx, y = y0 + dy, z = z0 + dz;
-                if ((x < 0 && b.modes[0] == 0u) || (beyond(x, g.nx) && b.modes[1] == 0u) || (y < 0 && b.modes[2] == 0u) ||
-                    (beyond(y, g.ny) && b.modes[3] == 0u) || (z < 0 && b.modes[4] == 0u) || (beyond(z, g.nz) && b.modes[5] == 0u))
-                    continue;
-                atomicAdd(v + mapped_cell(x, y, z, g, periodic(b, 0), periodic(b, 1), periodic(b, 2)), adj * wx[dx] * wy[dy] * wz[dz]);
-            }
-}
-
-// operators.cu:217-240
-__device__ __forceinline__ void scatter_face(double* v, int axis, const Vec3& p, double adj, const Grid& g, const XsVelocityBoundary& b) {
-    if (adj == 0.0) return;
-    float gx, gy, gz;
-    grid_coordinates(p, g.h, axis, gx, gy, gz);
-    const int x0 = static_cast<int>(floorf(gx)), y0 = static_cast<int>(floorf(gy)), z0 = static_cast<int>(floorf(gz));
-    const double wx[2] = {1.0 - (gx - x0), static_cast<double>(gx - x0)};
-    const double wy[2] = {1.0 - (gy - y0), static_cast<double>(gy - y0)};
-    const double wz[2] = {1.0 - (gz - z0), static_cast<double>(gz - z0)};
-#pragma unroll
-    for (int dz = 0; dz < 2; ++dz)
-#pragma unroll
-        for (int dy = 0; dy < 2; ++dy)
-#pragma unroll
-            for (int dx = 0; dx < 2; ++dx) {
-                const int c[3] = {x0 + dx, y0 + dy, z0 + dz};
-                bool constant = false;
-#pragma unroll
-                for (int d = 0; d < 3; ++d) {
-                    const int size = extent(g, axis, d);
-                    if (c[d] >= 0 && c[d] < size) continue;
-                    const int face = 2 * d + (c[d] >= size);
-                    if (b.modes[face] == 0u || (b.modes[face] == 2u && axis == d)) constant = true;
-                }
-                if (!constant) atomicAdd(v + mapped_face(c[0], c[1], c[2], g, axis, b), adj * wx[dx] * wy[dy] * wz[dz]);
-            }
-}
-
 // Shared tail of both advection adjoints (operators.cu:426-438, 548-560):
 // adjoint of value1 through the final position, midpoint sample gradients,
 // then of value0 at the start.
@@ -166,6 +116,18 @@ __device__ __forceinline__ void trace_adjoint(const Vec3& start, const Vec3& mid
     scatter_face(ua.z, 2, start, -0.5 * static_cast<double>(g.dt) * mz, g, vb);
 }
 
+// operators.cu:415-439, one face (general form: colliders, any spacing).
+__device__ __forceinline__ void advect_velocity_vjp_face(int a, int x, int y, int z, double o, const Grid& g, const uint32_t* __restrict__ mask,
+                                                         const XsVector& u, const XsVelocityBoundary& vb, const XsAdjointVector& ua) {
+    const Vec3 s = face_position(a, x, y, z, g);
+    const Vec3 v0 = sample_velocity(u.x, u.y, u.z, s, g, vb);
+    const Vec3 mid{s.x - 0.5f * g.dt * v0.x, s.y - 0.5f * g.dt * v0.y, s.z - 0.5f * g.dt * v0.z};
+    const Trace t = trace_rk2(s, u.x, u.y, u.z, mask, g, vb);
+    const Sample src = sample_face<true>(component<const float>(u.x, u.y, u.z, a), a, t.position, g, vb);
+    scatter_face(component<double>(ua.x, ua.y, ua.z, a), a, t.position, o, g, vb);
+    trace_adjoint(s, mid, t, src.gradient, o, u, g, vb, ua);
+}
+
 // operators.cu:415-439 for all three components in one launch.
 __global__ void advect_velocity_vjp_kernel(Grid g, uint64_t f0, uint64_t f1, uint64_t f2, const uint32_t* __restrict__ mask, XsVector u,
                                            XsVelocityBoundary vb, XsAdjointVector oa, XsAdjointVector ua) {
@@ -178,13 +140,197 @@ __global__ void advect_velocity_vjp_kernel(Grid g, uint64_t f0, uint64_t f1, uin
     if (o == 0.0) return;
     int x, y, z;
     decode(local, extent(g, a, 0), extent(g, a, 1), x, y, z);
-    const Vec3 s = face_position(a, x, y, z, g);
-    const Vec3 v0 = sample_velocity(u.x, u.y, u.z, s, g, vb);
-    const Vec3 mid{s.x - 0.5f * g.dt * v0.x, s.y - 0.5f * g.dt * v0.y, s.z - 0.5f * g.dt * v0.z};
-    const Trace t = trace_rk2(s, u.x, u.y, u.z, mask, g, vb);
-    const Sample src = sample_face<true>(component<const float>(u.x, u.y, u.z, a), a, t.position, g, vb);
-    scatter_face(component<double>(ua.x, ua.y, ua.z, a), a, t.position, o, g, vb);
-    trace_adjoint(s, mid, t, src.gradient, o, u, g, vb, ua);
+    advect_velocity_vjp_face(a, x, y, z, o, g, mask, u, vb, ua);
+}
+
+// ------------------------------------------------ tile-staged adjoints
+// Grids without colliders and with a power-of-two spacing (advect_tile.cuh).
+// u is staged over the tile's box; every scatter of the transposed trilinear
+// gathers goes to FP64 box accumulators in shared memory, and each touched
+// box node is added to global memory once at the end (instead of 56 global
+// atomics per face).  The same products as the general kernels; only the
+// order of the FP64 additions differs.
+using AdjointTile = tile::Shape<32, 4, 4>;
+constexpr size_t kVelocityVjpSmem = 3 * AdjointTile::kNodes * (sizeof(double) + sizeof(float));
+constexpr size_t kScalarVjpSmem = 5 * AdjointTile::kNodes * (sizeof(double) + sizeof(float));
+
+// The trace adjoint of one sample at the trace end (operators.cu:426-438):
+// through the end position to the midpoint samples (their gradients m), and
+// through the midpoint to the start (exact start weights).
+template <int A>
+__device__ __forceinline__ void staged_trace_adjoint(const Vec3& mid, const Sample (&m)[3], const Vec3& der, const Vec3& src_gradient,
+                                                     double o, int li, double* const (&acc)[3], const tile::Origin& org, const Grid& g,
+                                                     const XsVelocityBoundary& vb, const XsAdjointVector& ua, bool cell) {
+    using S = AdjointTile;
+    const double v1x = -static_cast<double>(der.x * g.dt * src_gradient.x) * o;
+    const double v1y = -static_cast<double>(der.y * g.dt * src_gradient.y) * o;
+    const double v1z = -static_cast<double>(der.z * g.dt * src_gradient.z) * o;
+    tile::staged_face_scatter<S, 0>(acc[0], ua.x, mid, v1x, org, g, vb);
+    tile::staged_face_scatter<S, 1>(acc[1], ua.y, mid, v1y, org, g, vb);
+    tile::staged_face_scatter<S, 2>(acc[2], ua.z, mid, v1z, org, g, vb);
+    const double mx = m[0].gradient.x * v1x + m[1].gradient.x * v1y + m[2].gradient.x * v1z;
+    const double my = m[0].gradient.y * v1x + m[1].gradient.y * v1y + m[2].gradient.y * v1z;
+    const double mz = m[0].gradient.z * v1x + m[1].gradient.z * v1y + m[2].gradient.z * v1z;
+    const double h = -0.5 * static_cast<double>(g.dt);
+    if (cell) {
+        tile::cell_start_scatter<S, 0>(acc[0], li, h * mx);
+        tile::cell_start_scatter<S, 1>(acc[1], li, h * my);
+        tile::cell_start_scatter<S, 2>(acc[2], li, h * mz);
+    } else {
+        tile::face_start_scatter<S, A, 0>(acc[0], li, h * mx);
+        tile::face_start_scatter<S, A, 1>(acc[1], li, h * my);
+        tile::face_start_scatter<S, A, 2>(acc[2], li, h * mz);
+    }
+}
+
+// Midpoint samples (values and gradients) and the clamped end of the trace
+// from a start with known velocity.
+__device__ __forceinline__ Vec3 staged_trace_with_samples(const tile::StagedVelocity& sv, const Vec3& s, const Vec3& v0, const tile::Origin& org,
+                                                          const Grid& g, const XsVelocityBoundary& vb, Vec3& mid, Sample (&m)[3], Vec3& der) {
+    using S = AdjointTile;
+    mid = Vec3{s.x - 0.5f * g.dt * v0.x, s.y - 0.5f * g.dt * v0.y, s.z - 0.5f * g.dt * v0.z};
+    m[0] = tile::staged_face<S, 0, true>(sv.s[0], sv.u.x, mid, org, g, vb);
+    m[1] = tile::staged_face<S, 1, true>(sv.s[1], sv.u.y, mid, org, g, vb);
+    m[2] = tile::staged_face<S, 2, true>(sv.s[2], sv.u.z, mid, org, g, vb);
+    Vec3 raw{s.x - g.dt * m[0].value, s.y - g.dt * m[1].value, s.z - g.dt * m[2].value};
+    der = Vec3{1.0f, 1.0f, 1.0f};
+    tile::clamp_trace(raw, der, g, vb);
+    return raw;
+}
+
+template <int A>
+__device__ __forceinline__ void advect_velocity_vjp_tile_face(int x, int y, int z, int li, const tile::StagedVelocity& sv,
+                                                              double* const (&acc)[3], const tile::Origin& org, const Grid& g,
+                                                              const XsVelocityBoundary& vb, const XsAdjointVector& oa,
+                                                              const XsAdjointVector& ua) {
+    using S = AdjointTile;
+    const double o = component<const double>(oa.x, oa.y, oa.z, A)[tile::index32(x, y, z, extent(g, A, 0), extent(g, A, 1))];
+    if (o == 0.0) return;
+    const Vec3 s = face_position(A, x, y, z, g);
+    Vec3 mid, der;
+    Sample m[3];
+    const Vec3 end = staged_trace_with_samples(sv, s, tile::face_start_velocity<S, A>(sv, li), org, g, vb, mid, m, der);
+    const Sample src = tile::staged_face<S, A, true>(sv.s[A], component<const float>(sv.u.x, sv.u.y, sv.u.z, A), end, org, g, vb);
+    tile::staged_face_scatter<S, A>(acc[A], component<double>(ua.x, ua.y, ua.z, A), end, o, org, g, vb);
+    staged_trace_adjoint<A>(mid, m, der, src.gradient, o, li, acc, org, g, vb, ua, false);
+}
+
+__global__ void __launch_bounds__(AdjointTile::kThreads, 2) advect_velocity_vjp_tile_kernel(Grid g, XsVector u, XsVelocityBoundary vb,
+                                                                                          XsAdjointVector oa, XsAdjointVector ua) {
+    using S = AdjointTile;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* const acc[3] = {reinterpret_cast<double*>(smem_raw), reinterpret_cast<double*>(smem_raw) + S::kNodes,
+                            reinterpret_cast<double*>(smem_raw) + 2 * S::kNodes};
+    float* box = reinterpret_cast<float*>(acc[0] + 3 * S::kNodes);
+    const tile::Origin org = tile::tile_origin<S>();
+    tile::stage_face<S, 0>(box, u.x, org, g, vb);
+    tile::stage_face<S, 1>(box + S::kNodes, u.y, org, g, vb);
+    tile::stage_face<S, 2>(box + 2 * S::kNodes, u.z, org, g, vb);
+    tile::zero_box<S>(acc[0]);
+    tile::zero_box<S>(acc[1]);
+    tile::zero_box<S>(acc[2]);
+    tile::stage_wait();
+    __syncthreads();
+    const tile::StagedVelocity sv{{box, box + S::kNodes, box + 2 * S::kNodes}, u};
+    const int x = static_cast<int>(blockIdx.x) * S::TX + static_cast<int>(threadIdx.x);
+    const int y = static_cast<int>(blockIdx.y) * S::TY + static_cast<int>(threadIdx.y);
+    if (x < g.nx && y < g.ny) {
+#pragma unroll 1
+        for (int kz = 0; kz < S::TZ; ++kz) {
+            const int z = static_cast<int>(blockIdx.z) * S::TZ + kz;
+            if (z >= g.nz) break;
+            const int li = tile::local_index<S>(kz);
+            advect_velocity_vjp_tile_face<0>(x, y, z, li, sv, acc, org, g, vb, oa, ua);
+            advect_velocity_vjp_tile_face<1>(x, y, z, li, sv, acc, org, g, vb, oa, ua);
+            advect_velocity_vjp_tile_face<2>(x, y, z, li, sv, acc, org, g, vb, oa, ua);
+        }
+    }
+    __syncthreads();
+    tile::flush_face<S, 0>(acc[0], ua.x, org, g, vb);
+    tile::flush_face<S, 1>(acc[1], ua.y, org, g, vb);
+    tile::flush_face<S, 2>(acc[2], ua.z, org, g, vb);
+}
+
+// The faces at the upper end of their own axis, general form.
+__global__ void advect_velocity_vjp_upper_kernel(Grid g, const uint32_t* __restrict__ mask, XsVector u, XsVelocityBoundary vb,
+                                                 XsAdjointVector oa, XsAdjointVector ua) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t sx = static_cast<uint32_t>(g.ny) * g.nz, sy = static_cast<uint32_t>(g.nx) * g.nz, sz = static_cast<uint32_t>(g.nx) * g.ny;
+    int a, x, y, z;
+    if (i < sx) {
+        a = 0; x = g.nx; y = static_cast<int>(i % g.ny); z = static_cast<int>(i / g.ny);
+    } else if (i < sx + sy) {
+        const uint32_t j = i - sx;
+        a = 1; x = static_cast<int>(j % g.nx); y = g.ny; z = static_cast<int>(j / g.nx);
+    } else if (i < sx + sy + sz) {
+        const uint32_t j = i - sx - sy;
+        a = 2; x = static_cast<int>(j % g.nx); y = static_cast<int>(j / g.nx); z = g.nz;
+    } else {
+        return;
+    }
+    const double o = component<double>(oa.x, oa.y, oa.z, a)[idx3(x, y, z, extent(g, a, 0), extent(g, a, 1))];
+    if (o == 0.0) return;
+    advect_velocity_vjp_face(a, x, y, z, o, g, mask, u, vb, ua);
+}
+
+// Density and temperature together (operators.cu:537-561 twice on one
+// trace): u and both sources staged, the velocity and both source adjoints
+// accumulated in the box.
+__global__ void __launch_bounds__(AdjointTile::kThreads, 1) advect_scalar_vjp_tile_kernel(Grid g, const float* __restrict__ src,
+                                                                                        XsScalarBoundary sb, const double* __restrict__ oa,
+                                                                                        double* __restrict__ sa, const float* __restrict__ src2,
+                                                                                        XsScalarBoundary sb2, const double* __restrict__ oa2,
+                                                                                        double* __restrict__ sa2, XsVector u,
+                                                                                        XsVelocityBoundary vb, XsAdjointVector ua) {
+    using S = AdjointTile;
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    double* const acc[3] = {reinterpret_cast<double*>(smem_raw), reinterpret_cast<double*>(smem_raw) + S::kNodes,
+                            reinterpret_cast<double*>(smem_raw) + 2 * S::kNodes};
+    double* const sacc[2] = {acc[0] + 3 * S::kNodes, acc[0] + 4 * S::kNodes};
+    float* box = reinterpret_cast<float*>(acc[0] + 5 * S::kNodes);
+    const bool two = oa2 != nullptr;
+    const tile::Origin org = tile::tile_origin<S>();
+    tile::stage_face<S, 0>(box, u.x, org, g, vb);
+    tile::stage_face<S, 1>(box + S::kNodes, u.y, org, g, vb);
+    tile::stage_face<S, 2>(box + 2 * S::kNodes, u.z, org, g, vb);
+    tile::stage_cells<S>(box + 3 * S::kNodes, src, org, g, sb);
+    if (two) tile::stage_cells<S>(box + 4 * S::kNodes, src2, org, g, sb2);
+    for (int k = 0; k < 5; ++k) tile::zero_box<S>(acc[0] + k * S::kNodes);
+    tile::stage_wait();
+    __syncthreads();
+    const tile::StagedVelocity sv{{box, box + S::kNodes, box + 2 * S::kNodes}, u};
+    const int x = static_cast<int>(blockIdx.x) * S::TX + static_cast<int>(threadIdx.x);
+    const int y = static_cast<int>(blockIdx.y) * S::TY + static_cast<int>(threadIdx.y);
+    if (x < g.nx && y < g.ny) {
+#pragma unroll 1
+        for (int kz = 0; kz < S::TZ; ++kz) {
+            const int z = static_cast<int>(blockIdx.z) * S::TZ + kz;
+            if (z >= g.nz) break;
+            const uint32_t i = tile::index32(x, y, z, g.nx, g.ny);
+            const double o1 = oa[i];
+            const double o2 = two ? oa2[i] : 0.0;
+            if (o1 == 0.0 && o2 == 0.0) continue;
+            const int li = tile::local_index<S>(kz);
+            const Vec3 s = cell_position(x, y, z, g);
+            Vec3 mid, der;
+            Sample m[3];
+            const Vec3 end = staged_trace_with_samples(sv, s, tile::cell_start_velocity<S>(sv, li), org, g, vb, mid, m, der);
+            const Sample smp = tile::staged_scalar<S, true>(box + 3 * S::kNodes, src, end, org, g, sb);
+            tile::staged_scalar_scatter<S>(sacc[0], sa, end, o1, org, g, sb);
+            if (o1 != 0.0) staged_trace_adjoint<0>(mid, m, der, smp.gradient, o1, li, acc, org, g, vb, ua, true);
+            if (two && o2 != 0.0) {
+                const Sample smp2 = tile::staged_scalar<S, true>(box + 4 * S::kNodes, src2, end, org, g, sb2);
+                tile::staged_scalar_scatter<S>(sacc[1], sa2, end, o2, org, g, sb2);
+                staged_trace_adjoint<0>(mid, m, der, smp2.gradient, o2, li, acc, org, g, vb, ua, true);
+            }
+        }
+    }
+    __syncthreads();
+    tile::flush_face<S, 0>(acc[0], ua.x, org, g, vb);
+    tile::flush_face<S, 1>(acc[1], ua.y, org, g, vb);
+    tile::flush_face<S, 2>(acc[2], ua.z, org, g, vb);
+    tile::flush_cells<S>(sacc[0], sa, org, g, sb);
+    if (two) tile::flush_cells<S>(sacc[1], sa2, org, g, sb2);
 }
 
 // operators.cu:537-561; density and temperature share one trace when both
@@ -340,6 +486,21 @@ XsStatus launch_integrate_vjp(cudaStream_t st, const Grid& g, const uint32_t* ma
 
 XsStatus launch_advect_velocity_vjp(cudaStream_t st, const Grid& g, const uint32_t* mask, const XsVector& u, const XsVelocityBoundary& vb,
                                     const XsAdjointVector& oa, const XsAdjointVector& ua) {
+    if (tile::tiled_advection(g, mask)) {
+        static DeviceOnce configured;
+        if (!configured.run([] {
+                return cudaFuncSetAttribute(advect_velocity_vjp_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            static_cast<int>(kVelocityVjpSmem));
+            }))
+            return XS_CUDA_ERROR;
+        advect_velocity_vjp_tile_kernel<<<tile::tile_grid<AdjointTile>(g), tile::tile_block<AdjointTile>(), kVelocityVjpSmem, st>>>(g, u, vb,
+                                                                                                                                  oa, ua);
+        XsStatus s = check_launch();
+        if (s != XS_OK) return s;
+        const uint64_t upper = static_cast<uint64_t>(g.ny) * g.nz + static_cast<uint64_t>(g.nx) * g.nz + static_cast<uint64_t>(g.nx) * g.ny;
+        advect_velocity_vjp_upper_kernel<<<blocks_for(upper), kBlock, 0, st>>>(g, mask, u, vb, oa, ua);
+        return check_launch();
+    }
     const uint64_t f0 = face_count(g, 0), f1 = face_count(g, 1), f2 = face_count(g, 2);
     advect_velocity_vjp_kernel<<<blocks_for(f0 + f1 + f2), kBlock, 0, st>>>(g, f0, f1, f2, mask, u, vb, oa, ua);
     return check_launch();
@@ -348,6 +509,17 @@ XsStatus launch_advect_velocity_vjp(cudaStream_t st, const Grid& g, const uint32
 XsStatus launch_advect_scalar_vjp(cudaStream_t st, const Grid& g, const uint32_t* mask, const float* src, const XsScalarBoundary& sb,
                                   const double* oa, double* sa, const float* src2, const XsScalarBoundary& sb2, const double* oa2,
                                   double* sa2, const XsVector& u, const XsVelocityBoundary& vb, const XsAdjointVector& ua) {
+    if (tile::tiled_advection(g, mask)) {
+        static DeviceOnce configured;
+        if (!configured.run([] {
+                return cudaFuncSetAttribute(advect_scalar_vjp_tile_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                            static_cast<int>(kScalarVjpSmem));
+            }))
+            return XS_CUDA_ERROR;
+        advect_scalar_vjp_tile_kernel<<<tile::tile_grid<AdjointTile>(g), tile::tile_block<AdjointTile>(), kScalarVjpSmem, st>>>(
+            g, src, sb, oa, sa, src2, sb2, oa2, sa2, u, vb, ua);
+        return check_launch();
+    }
     advect_scalar_vjp_kernel<<<blocks_for(cell_count(g)), kBlock, 0, st>>>(g, mask, src, sb, oa, sa, src2, sb2, oa2, sa2, u, vb, ua);
     return check_launch();
 }

@@ -246,22 +246,28 @@ __device__ __forceinline__ void load_stencil(const float* __restrict__ v, int x0
     v8[1][1][1] = __ldg(c + sz + sy + 1);
 }
 
-// Boundary-aware loads of a whole stencil.  Only samples near the domain
-// edge take them; they stay out of line so that the gather loops of the
-// advection kernels fit the instruction cache (inlined eight times per
-// sample they made the kernels instruction-fetch bound).
-static __device__ __noinline__ void load_scalar_stencil(const float* __restrict__ v, int x0, int y0, int z0, const Grid& g,
-                                                        const XsScalarBoundary& b, float (&v8)[2][2][2]) {
+// Boundary-aware samples (stencils that reach past the domain edge or wrap).
+// Only samples near the edge take them; they stay out of line so that the
+// gather loops of the advection kernels fit the instruction cache (inlined
+// eight times per sample they made the kernels instruction-fetch bound).
+// They return the whole sample by value: a stencil array passed out of line
+// by reference would live in local memory on the interior path as well.
+static __device__ __noinline__ Sample edge_scalar_sample(const float* __restrict__ v, int x0, int y0, int z0, float tx, float ty, float tz,
+                                                         const Grid& g, const XsScalarBoundary& b) {
+    float v8[2][2][2];
     for (int dz = 0; dz < 2; ++dz)
         for (int dy = 0; dy < 2; ++dy)
             for (int dx = 0; dx < 2; ++dx) v8[dz][dy][dx] = load_scalar(v, x0 + dx, y0 + dy, z0 + dz, g, b);
+    return trilinear(v8, tx, ty, tz, g.h);
 }
 
-static __device__ __noinline__ void load_face_stencil(const float* __restrict__ v, int axis, int x0, int y0, int z0, const Grid& g,
-                                                      const XsVelocityBoundary& b, float (&v8)[2][2][2]) {
+static __device__ __noinline__ Sample edge_face_sample(const float* __restrict__ v, int axis, int x0, int y0, int z0, float tx, float ty,
+                                                       float tz, const Grid& g, const XsVelocityBoundary& b) {
+    float v8[2][2][2];
     for (int dz = 0; dz < 2; ++dz)
         for (int dy = 0; dy < 2; ++dy)
             for (int dx = 0; dx < 2; ++dx) v8[dz][dy][dx] = load_face(v, axis, x0 + dx, y0 + dy, z0 + dz, g, b);
+    return trilinear(v8, tx, ty, tz, g.h);
 }
 
 // operators.cu:136-164
@@ -270,13 +276,16 @@ __device__ __forceinline__ Sample sample_scalar(const float* __restrict__ v, con
     float gx, gy, gz;
     grid_coordinates(p, g.h, -1, gx, gy, gz);
     const int x0 = static_cast<int>(floorf(gx)), y0 = static_cast<int>(floorf(gy)), z0 = static_cast<int>(floorf(gz));
-    float v8[2][2][2];
-    if (interior_stencil(x0, y0, z0, g.nx, g.ny, g.nz))
+    Sample r;
+    if (interior_stencil(x0, y0, z0, g.nx, g.ny, g.nz)) {
+        float v8[2][2][2];
         load_stencil(v, x0, y0, z0, g.nx, g.ny, v8);
-    else
-        load_scalar_stencil(v, x0, y0, z0, g, b, v8);
-    if (kGradient) return trilinear(v8, gx - x0, gy - y0, gz - z0, g.h);
-    return Sample{trilinear(v8, gx - x0, gy - y0, gz - z0, g.h).value, {0.0f, 0.0f, 0.0f}};
+        r = trilinear(v8, gx - x0, gy - y0, gz - z0, g.h);
+    } else {
+        r = edge_scalar_sample(v, x0, y0, z0, gx - x0, gy - y0, gz - z0, g, b);
+    }
+    if (kGradient) return r;
+    return Sample{r.value, {0.0f, 0.0f, 0.0f}};
 }
 
 // operators.cu:166-194
@@ -286,14 +295,17 @@ __device__ __forceinline__ Sample sample_face(const float* __restrict__ v, int a
     float gx, gy, gz;
     grid_coordinates(p, g.h, axis, gx, gy, gz);
     const int x0 = static_cast<int>(floorf(gx)), y0 = static_cast<int>(floorf(gy)), z0 = static_cast<int>(floorf(gz));
-    float v8[2][2][2];
     const int ex = extent(g, axis, 0), ey = extent(g, axis, 1), ez = extent(g, axis, 2);
-    if (interior_stencil(x0, y0, z0, periodic(b, 0) ? g.nx : ex, periodic(b, 1) ? g.ny : ey, periodic(b, 2) ? g.nz : ez))
+    Sample r;
+    if (interior_stencil(x0, y0, z0, periodic(b, 0) ? g.nx : ex, periodic(b, 1) ? g.ny : ey, periodic(b, 2) ? g.nz : ez)) {
+        float v8[2][2][2];
         load_stencil(v, x0, y0, z0, ex, ey, v8);
-    else
-        load_face_stencil(v, axis, x0, y0, z0, g, b, v8);
-    if (kGradient) return trilinear(v8, gx - x0, gy - y0, gz - z0, g.h);
-    return Sample{trilinear(v8, gx - x0, gy - y0, gz - z0, g.h).value, {0.0f, 0.0f, 0.0f}};
+        r = trilinear(v8, gx - x0, gy - y0, gz - z0, g.h);
+    } else {
+        r = edge_face_sample(v, axis, x0, y0, z0, gx - x0, gy - y0, gz - z0, g, b);
+    }
+    if (kGradient) return r;
+    return Sample{r.value, {0.0f, 0.0f, 0.0f}};
 }
 
 // operators.cu:242-244
@@ -347,6 +359,60 @@ __device__ __forceinline__ Vec3 face_position(int axis, int x, int y, int z, con
 }
 __device__ __forceinline__ Vec3 cell_position(int x, int y, int z, const Grid& g) {
     return Vec3{(x + 0.5f) * g.h, (y + 0.5f) * g.h, (z + 0.5f) * g.h};
+}
+
+// Transposes of the trilinear gathers (FP64 atomics), the reference's
+// scatter_scalar / scatter_face (operators.cu:196-240): nodes on a constant
+// boundary receive nothing, nodes beyond the domain go to their clamped or
+// wrapped partner.
+__device__ __forceinline__ void scatter_scalar(double* v, const Vec3& p, double adj, const Grid& g, const XsScalarBoundary& b) {
+    if (adj == 0.0) return;
+    float gx, gy, gz;
+    grid_coordinates(p, g.h, -1, gx, gy, gz);
+    const int x0 = static_cast<int>(floorf(gx)), y0 = static_cast<int>(floorf(gy)), z0 = static_cast<int>(floorf(gz));
+    const double wx[2] = {1.0 - (gx - x0), static_cast<double>(gx - x0)};
+    const double wy[2] = {1.0 - (gy - y0), static_cast<double>(gy - y0)};
+    const double wz[2] = {1.0 - (gz - z0), static_cast<double>(gz - z0)};
+#pragma unroll
+    for (int dz = 0; dz < 2; ++dz)
+#pragma unroll
+        for (int dy = 0; dy < 2; ++dy)
+#pragma unroll
+            for (int dx = 0; dx < 2; ++dx) {
+                const int x = x0 + dx, y = y0 + dy, z = z0 + dz;
+                if ((x < 0 && b.modes[0] == 0u) || (beyond(x, g.nx) && b.modes[1] == 0u) || (y < 0 && b.modes[2] == 0u) ||
+                    (beyond(y, g.ny) && b.modes[3] == 0u) || (z < 0 && b.modes[4] == 0u) || (beyond(z, g.nz) && b.modes[5] == 0u))
+                    continue;
+                atomicAdd(v + mapped_cell(x, y, z, g, periodic(b, 0), periodic(b, 1), periodic(b, 2)), adj * wx[dx] * wy[dy] * wz[dz]);
+            }
+}
+
+// operators.cu:217-240
+__device__ __forceinline__ void scatter_face(double* v, int axis, const Vec3& p, double adj, const Grid& g, const XsVelocityBoundary& b) {
+    if (adj == 0.0) return;
+    float gx, gy, gz;
+    grid_coordinates(p, g.h, axis, gx, gy, gz);
+    const int x0 = static_cast<int>(floorf(gx)), y0 = static_cast<int>(floorf(gy)), z0 = static_cast<int>(floorf(gz));
+    const double wx[2] = {1.0 - (gx - x0), static_cast<double>(gx - x0)};
+    const double wy[2] = {1.0 - (gy - y0), static_cast<double>(gy - y0)};
+    const double wz[2] = {1.0 - (gz - z0), static_cast<double>(gz - z0)};
+#pragma unroll
+    for (int dz = 0; dz < 2; ++dz)
+#pragma unroll
+        for (int dy = 0; dy < 2; ++dy)
+#pragma unroll
+            for (int dx = 0; dx < 2; ++dx) {
+                const int c[3] = {x0 + dx, y0 + dy, z0 + dz};
+                bool constant = false;
+#pragma unroll
+                for (int d = 0; d < 3; ++d) {
+                    const int size = extent(g, axis, d);
+                    if (c[d] >= 0 && c[d] < size) continue;
+                    const int face = 2 * d + (c[d] >= size);
+                    if (b.modes[face] == 0u || (b.modes[face] == 2u && axis == d)) constant = true;
+                }
+                if (!constant) atomicAdd(v + mapped_face(c[0], c[1], c[2], g, axis, b), adj * wx[dx] * wy[dy] * wz[dz]);
+            }
 }
 
 // Inflow spheres travel as a kernel parameter.

@@ -32,27 +32,6 @@ namespace xs {
 // ------------------------------------------------------------------ TMA maps
 namespace {
 
-// A set-up call that must run once per device (a kernel attribute applies to
-// the device and context it was set on), thread-safe.
-class DeviceOnce {
-public:
-    template <class F>
-    bool run(F&& f) {
-        int device = 0;
-        if (cudaGetDevice(&device) != cudaSuccess || device < 0 || device >= kMaxDevices) return false;
-        std::lock_guard<std::mutex> lock(mu_);
-        if (done_[device]) return true;
-        if (f() != cudaSuccess) return false;
-        done_[device] = true;
-        return true;
-    }
-
-private:
-    static constexpr int kMaxDevices = 64;
-    std::mutex mu_;
-    bool done_[kMaxDevices] = {};
-};
-
 PFN_cuTensorMapEncodeTiled_v12000 encode_fn() {
     static PFN_cuTensorMapEncodeTiled_v12000 fn = nullptr;
     static std::once_flag once;

@@ -3,6 +3,7 @@
 // divergence and projection.  Operator-level C ABI (operators.h:40-72).
 #include <atomic>
 
+#include "advect_tile.cuh"
 #include "common.cuh"
 #include "launch.cuh"
 #include "ops.cuh"
@@ -192,11 +193,30 @@ __global__ void constrain_kernel(Grid g, FaceSpace fs, const uint32_t* __restric
     oa[local] = ua[local];
 }
 
-// Advection and constraint fused (operators.cu:381-388 then :466-481): the
-// constrained output is written directly; a periodic face at the upper end
-// takes the advected value of its wrapped partner at coordinate 0.
-// Latency-bound on its ~56 L1 gathers per face: the launch bounds trade a few
-// registers for a fourth resident block per SM.
+// Advection and constraint fused for one face (operators.cu:381-388 then
+// :466-481): the constrained value is produced directly; a periodic face at
+// the upper end takes the advected value of its wrapped partner at
+// coordinate 0.
+__device__ __forceinline__ float advect_constrain_face(int a, int x, int y, int z, uint64_t local, const Grid& g,
+                                                       const uint32_t* __restrict__ mask, const XsVector& col, const XsVector& u,
+                                                       const XsVelocityBoundary& b) {
+    float v;
+    if (constrained_boundary(a, x, y, z, g, b, v)) return v;
+    if (adjacent_solid(a, x, y, z, g, mask)) {
+        const float* ca = component(col.x, col.y, col.z, a);
+        return ca == nullptr ? 0.0f : ca[local];
+    }
+    if (periodic(b, a) && (a == 0 ? x == g.nx : (a == 1 ? y == g.ny : z == g.nz))) {
+        if (a == 0) x = 0;
+        if (a == 1) y = 0;
+        if (a == 2) z = 0;
+    }
+    return advect_face(a, x, y, z, g, mask, u, b);
+}
+
+// General form (colliders, any spacing), one thread per face.  Latency-bound
+// on its ~56 L1 gathers per face: the launch bounds trade a few registers for
+// a fourth resident block per SM.
 __global__ void __launch_bounds__(kBlock, 4) advect_constrain_kernel(Grid g, FaceSpace fs, const uint32_t* __restrict__ mask, XsVector col, XsVector u,
                                         XsVelocityBoundary b, XsVector out) {
     const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -205,20 +225,92 @@ __global__ void __launch_bounds__(kBlock, 4) advect_constrain_kernel(Grid g, Fac
     const int a = fs.locate(i, local);
     int x, y, z;
     decode(local, extent(g, a, 0), extent(g, a, 1), x, y, z);
-    float* oa = component(out.x, out.y, out.z, a);
+    component(out.x, out.y, out.z, a)[local] = advect_constrain_face(a, x, y, z, local, g, mask, col, u, b);
+}
+
+// ------------------------------------------------ tile-staged advection
+// Grids without colliders and with a power-of-two spacing (advect_tile.cuh).
+// A CTA stages u over its box once and advects the three faces at each of
+// its kTX x kTY x kTZ positions (x, y, z < nx, ny, nz): every face whose
+// coordinate along its own axis is below the grid size.  The faces at the
+// upper end of their axis (x = nx for u, ...) are left to the remainder
+// kernel below.  Bit-identical to advect_constrain_kernel.
+using ForwardTile = tile::Shape<32, 8, 4>;
+
+template <int A, bool kConstrain>
+__device__ __forceinline__ void advect_constrain_tile_face(int x, int y, int z, int li, const tile::StagedVelocity& sv, const tile::Origin& o,
+                                                           const Grid& g, const XsVelocityBoundary& b, float* __restrict__ out) {
+    using S = ForwardTile;
     float v;
-    if (constrained_boundary(a, x, y, z, g, b, v)) { oa[local] = v; return; }
-    if (adjacent_solid(a, x, y, z, g, mask)) {
-        const float* ca = component(col.x, col.y, col.z, a);
-        oa[local] = ca == nullptr ? 0.0f : ca[local];
+    if (!kConstrain || !constrained_boundary(A, x, y, z, g, b, v)) {
+        const Vec3 s = face_position(A, x, y, z, g);
+        const Vec3 p = tile::staged_trace<S>(sv, s, tile::face_start_velocity<S, A>(sv, li), o, g, b);
+        v = tile::staged_face<S, A, false>(sv.s[A], component<const float>(sv.u.x, sv.u.y, sv.u.z, A), p, o, g, b).value;
+    }
+    const uint32_t ex = static_cast<uint32_t>(extent(g, A, 0)), ey = static_cast<uint32_t>(extent(g, A, 1));
+    out[static_cast<uint32_t>(x) + ex * (static_cast<uint32_t>(y) + ey * static_cast<uint32_t>(z))] = v;
+}
+
+// kConstrain = false: the raw advected field of advect_velocity_kernel.
+template <bool kConstrain>
+__global__ void __launch_bounds__(ForwardTile::kThreads, 4) advect_constrain_tile_kernel(Grid g, XsVector u, XsVelocityBoundary b, XsVector out) {
+    using S = ForwardTile;
+    __shared__ float box[3][S::kNodes];
+    const tile::Origin o = tile::tile_origin<S>();
+    tile::stage_face<S, 0>(box[0], u.x, o, g, b);
+    tile::stage_face<S, 1>(box[1], u.y, o, g, b);
+    tile::stage_face<S, 2>(box[2], u.z, o, g, b);
+    tile::stage_wait();
+    __syncthreads();
+    const tile::StagedVelocity sv{{box[0], box[1], box[2]}, u};
+    const int x = static_cast<int>(blockIdx.x) * S::TX + static_cast<int>(threadIdx.x);
+    const int y = static_cast<int>(blockIdx.y) * S::TY + static_cast<int>(threadIdx.y);
+    if (x >= g.nx || y >= g.ny) return;
+#pragma unroll 1
+    for (int kz = 0; kz < S::TZ; ++kz) {
+        const int z = static_cast<int>(blockIdx.z) * S::TZ + kz;
+        if (z >= g.nz) break;
+        const int li = tile::local_index<S>(kz);
+        advect_constrain_tile_face<0, kConstrain>(x, y, z, li, sv, o, g, b, out.x);
+        advect_constrain_tile_face<1, kConstrain>(x, y, z, li, sv, o, g, b, out.y);
+        advect_constrain_tile_face<2, kConstrain>(x, y, z, li, sv, o, g, b, out.z);
+    }
+}
+
+// The faces at the upper end of their own axis (ny nz + nx nz + nx ny of
+// them), general form.
+template <bool kConstrain>
+__global__ void advect_constrain_upper_kernel(Grid g, const uint32_t* __restrict__ mask, XsVector col, XsVector u, XsVelocityBoundary b,
+                                              XsVector out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t sx = static_cast<uint32_t>(g.ny) * g.nz, sy = static_cast<uint32_t>(g.nx) * g.nz, sz = static_cast<uint32_t>(g.nx) * g.ny;
+    int a, x, y, z;
+    if (i < sx) {
+        a = 0; x = g.nx; y = static_cast<int>(i % g.ny); z = static_cast<int>(i / g.ny);
+    } else if (i < sx + sy) {
+        const uint32_t j = i - sx;
+        a = 1; x = static_cast<int>(j % g.nx); y = g.ny; z = static_cast<int>(j / g.nx);
+    } else if (i < sx + sy + sz) {
+        const uint32_t j = i - sx - sy;
+        a = 2; x = static_cast<int>(j % g.nx); y = static_cast<int>(j / g.nx); z = g.nz;
+    } else {
         return;
     }
-    if (periodic(b, a) && (a == 0 ? x == g.nx : (a == 1 ? y == g.ny : z == g.nz))) {
-        if (a == 0) x = 0;
-        if (a == 1) y = 0;
-        if (a == 2) z = 0;
-    }
-    oa[local] = advect_face(a, x, y, z, g, mask, u, b);
+    const uint64_t local = idx3(x, y, z, extent(g, a, 0), extent(g, a, 1));
+    component(out.x, out.y, out.z, a)[local] =
+        kConstrain ? advect_constrain_face(a, x, y, z, local, g, mask, col, u, b) : advect_face(a, x, y, z, g, mask, u, b);
+}
+
+// Both tile launches of the MAC advection (with or without the constraint).
+template <bool kConstrain>
+XsStatus launch_advect_tiled(cudaStream_t st, const Grid& g, const XsVector& col, const XsVector& u, const XsVelocityBoundary& b,
+                             const XsVector& out) {
+    advect_constrain_tile_kernel<kConstrain><<<tile::tile_grid<ForwardTile>(g), tile::tile_block<ForwardTile>(), 0, st>>>(g, u, b, out);
+    XsStatus s = check_launch();
+    if (s != XS_OK) return s;
+    const uint64_t upper = static_cast<uint64_t>(g.ny) * g.nz + static_cast<uint64_t>(g.nx) * g.nz + static_cast<uint64_t>(g.nx) * g.ny;
+    advect_constrain_upper_kernel<kConstrain><<<blocks_for(upper), kBlock, 0, st>>>(g, nullptr, col, u, b, out);
+    return check_launch();
 }
 
 // operators.cu:499-507
@@ -253,6 +345,48 @@ __global__ void __launch_bounds__(kBlock, 5) advect_scalar_pair_kernel(Grid g, c
     const Trace t = trace_rk2(cell_position(x, y, z, g), u.x, u.y, u.z, mask, g, vb);
     out_rho[i] = sample_scalar<false>(src_rho, t.position, g, rb).value;
     out_temp[i] = sample_scalar<false>(src_temp, t.position, g, tb).value;
+}
+
+// Tile-staged form of advect_scalar_pair_kernel for grids without colliders
+// and with a power-of-two spacing: u, the sourced density and the sourced
+// temperature are staged over the box (5 boxes, dynamic shared memory).
+// Bit-identical to advect_scalar_pair_kernel; kFields = 1 advects one field
+// (advect_scalar_kernel).
+constexpr size_t scalar_tile_smem(int fields) { return (3 + fields) * sizeof(float) * ForwardTile::kNodes; }
+
+template <int kFields>
+__global__ void __launch_bounds__(ForwardTile::kThreads, 3) advect_scalar_pair_tile_kernel(Grid g, const float* __restrict__ src_rho,
+                                                                                      const float* __restrict__ src_temp, XsVector u,
+                                                                                      XsScalarBoundary rb, XsScalarBoundary tb,
+                                                                                      XsVelocityBoundary vb, float* __restrict__ out_rho,
+                                                                                      float* __restrict__ out_temp) {
+    using S = ForwardTile;
+    extern __shared__ float smem[];
+    float* box[5] = {smem, smem + S::kNodes, smem + 2 * S::kNodes, smem + 3 * S::kNodes, smem + 4 * S::kNodes};
+    const tile::Origin o = tile::tile_origin<S>();
+    tile::stage_face<S, 0>(box[0], u.x, o, g, vb);
+    tile::stage_face<S, 1>(box[1], u.y, o, g, vb);
+    tile::stage_face<S, 2>(box[2], u.z, o, g, vb);
+    tile::stage_cells<S>(box[3], src_rho, o, g, rb);
+    if (kFields == 2) tile::stage_cells<S>(box[4], src_temp, o, g, tb);
+    tile::stage_wait();
+    __syncthreads();
+    const tile::StagedVelocity sv{{box[0], box[1], box[2]}, u};
+    const int x = static_cast<int>(blockIdx.x) * S::TX + static_cast<int>(threadIdx.x);
+    const int y = static_cast<int>(blockIdx.y) * S::TY + static_cast<int>(threadIdx.y);
+    if (x >= g.nx || y >= g.ny) return;
+#pragma unroll 1
+    for (int kz = 0; kz < S::TZ; ++kz) {
+        const int z = static_cast<int>(blockIdx.z) * S::TZ + kz;
+        if (z >= g.nz) break;
+        const int li = tile::local_index<S>(kz);
+        const Vec3 s = cell_position(x, y, z, g);
+        const Vec3 p = tile::staged_trace<S>(sv, s, tile::cell_start_velocity<S>(sv, li), o, g, vb);
+        const uint32_t i = static_cast<uint32_t>(x) + static_cast<uint32_t>(g.nx) * (static_cast<uint32_t>(y) + static_cast<uint32_t>(g.ny) *
+                                                                                                                static_cast<uint32_t>(z));
+        out_rho[i] = tile::staged_scalar<S, false>(box[3], src_rho, p, o, g, rb).value;
+        if (kFields == 2) out_temp[i] = tile::staged_scalar<S, false>(box[4], src_temp, p, o, g, tb).value;
+    }
 }
 
 // ------------------------------------------------------------ projection
@@ -319,6 +453,21 @@ __global__ void accumulate_kernel(const double* __restrict__ src, double* __rest
 }
 
 // ------------------------------------------------------------ launchers
+template <int kFields>
+XsStatus launch_scalar_tiled(cudaStream_t st, const Grid& g, const float* src_rho, const float* src_temp, const XsVector& u,
+                             const XsScalarBoundary& rb, const XsScalarBoundary& tb, const XsVelocityBoundary& vb, float* out_rho,
+                             float* out_temp) {
+    static DeviceOnce configured;
+    if (!configured.run([] {
+            return cudaFuncSetAttribute(advect_scalar_pair_tile_kernel<kFields>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(scalar_tile_smem(kFields)));
+        }))
+        return XS_CUDA_ERROR;
+    advect_scalar_pair_tile_kernel<kFields><<<tile::tile_grid<ForwardTile>(g), tile::tile_block<ForwardTile>(), scalar_tile_smem(kFields), st>>>(
+        g, src_rho, src_temp, u, rb, tb, vb, out_rho, out_temp);
+    return check_launch();
+}
+
 InflowSet make_inflows(const XsInflow* inflows, uint32_t count) {
     InflowSet s{};
     s.count = inflows == nullptr ? 0u : count;
@@ -344,6 +493,7 @@ XsStatus launch_integrate(cudaStream_t st, const Grid& g, const uint32_t* mask, 
 
 XsStatus launch_advect_constrain(cudaStream_t st, const Grid& g, const uint32_t* mask, const XsVector& col, const XsVector& u,
                                  const XsVelocityBoundary& b, const XsVector& out) {
+    if (tile::tiled_advection(g, mask)) return launch_advect_tiled<true>(st, g, col, u, b, out);
     const FaceSpace fs = face_space(g);
     advect_constrain_kernel<<<blocks_for(fs.total()), kBlock, 0, st>>>(g, fs, mask, col, u, b, out);
     return check_launch();
@@ -359,6 +509,7 @@ XsStatus launch_constrain(cudaStream_t st, const Grid& g, const uint32_t* mask, 
 XsStatus launch_advect_scalar_pair(cudaStream_t st, const Grid& g, const uint32_t* mask, const float* col_rho, const float* col_temp,
                                    const float* src_rho, const float* src_temp, const XsVector& u, const XsScalarBoundary& rb,
                                    const XsScalarBoundary& tb, const XsVelocityBoundary& vb, float* out_rho, float* out_temp) {
+    if (tile::tiled_advection(g, mask)) return launch_scalar_tiled<2>(st, g, src_rho, src_temp, u, rb, tb, vb, out_rho, out_temp);
     advect_scalar_pair_kernel<<<blocks_for(cell_count(g)), kBlock, 0, st>>>(g, mask, col_rho, col_temp, src_rho, src_temp, u, rb, tb,
                                                                              vb, out_rho, out_temp);
     return check_launch();
@@ -426,6 +577,7 @@ XsStatus xs_advect_velocity_forward(cudaStream_t stream, XsGrid grid, const uint
                                     XsVelocityBoundary boundary, XsVector output) {
     if (!valid_grid(grid) || !valid(velocity) || !valid(output)) return XS_INVALID_ARGUMENT;
     const Grid g = make_grid(grid);
+    if (tile::tiled_advection(g, cell_mask)) return launch_advect_tiled<false>(stream, g, XsVector{nullptr, nullptr, nullptr}, velocity, boundary, output);
     const FaceSpace fs = face_space(g);
     advect_velocity_kernel<<<blocks_for(fs.total()), kBlock, 0, stream>>>(g, fs, cell_mask, velocity, boundary, output);
     return check_launch();
@@ -445,6 +597,8 @@ XsStatus xs_advect_scalar_forward(cudaStream_t stream, XsGrid grid, const uint32
                                   XsVelocityBoundary velocity_boundary, float* output) {
     if (!valid_grid(grid) || !source || !valid(velocity) || !output) return XS_INVALID_ARGUMENT;
     const Grid g = make_grid(grid);
+    if (tile::tiled_advection(g, cell_mask))
+        return launch_scalar_tiled<1>(stream, g, source, nullptr, velocity, scalar_boundary, scalar_boundary, velocity_boundary, output, nullptr);
     advect_scalar_kernel<<<blocks_for(cell_count(g)), kBlock, 0, stream>>>(g, cell_mask, collider_value, source, velocity, scalar_boundary,
                                                                             velocity_boundary, output);
     return check_launch();

@@ -72,6 +72,13 @@ XsStatus launch_advect_scalar_jvp(cudaStream_t st, const Grid& g, const uint32_t
 XsStatus projection_forward(cudaStream_t st, const Grid& g, const XsPressureSolve& solve, uint32_t anchor, const uint32_t* mask,
                             const XsVector& u, const XsScalarBoundary& pb, float* pressure, float* rhs, const XsVector& out,
                             void* workspace, cudaEvent_t begin = nullptr, cudaEvent_t end = nullptr, struct WarmStartNet* warm_start = nullptr,
-                            const WarmHistory* history = nullptr);
+                            const WarmHistory* history = nullptr, cudaEvent_t* stages = nullptr);
+
+// Records stage event k of an optional event array (xs_smoke_forward_step's
+// stage_events).
+inline XsStatus mark_stage(cudaStream_t st, cudaEvent_t* events, int k) {
+    if (events == nullptr || events[k] == nullptr) return XS_OK;
+    return cudaEventRecord(events[k], st) == cudaSuccess ? XS_OK : XS_CUDA_ERROR;
+}
 
 }  // namespace xs

@@ -16,9 +16,12 @@ namespace xs {
 // the PCG kind the velocity is corrected from the FP64 iterate.
 XsStatus projection_forward(cudaStream_t st, const Grid& g, const XsPressureSolve& solve, uint32_t anchor, const uint32_t* mask,
                             const XsVector& u, const XsScalarBoundary& pb, float* pressure, float* rhs, const XsVector& out,
-                            void* workspace, cudaEvent_t begin, cudaEvent_t end, WarmStartNet* warm_start, const WarmHistory* history) {
+                            void* workspace, cudaEvent_t begin, cudaEvent_t end, WarmStartNet* warm_start, const WarmHistory* history,
+                            cudaEvent_t* stages) {
+    // stages (optional): the step's events [4..8], here indexed 0..4
     XsStatus s = launch_pressure_rhs(st, g, anchor, mask, u, rhs);
     if (s != XS_OK) return s;
+    if ((s = mark_stage(st, stages, 0)) != XS_OK) return s;
     PressureWorkspace w{};
     if (begin && cudaEventRecord(begin, st) != cudaSuccess) return XS_CUDA_ERROR;
     XsPressureSolve used = solve;
@@ -66,13 +69,17 @@ XsStatus projection_forward(cudaStream_t st, const Grid& g, const XsPressureSolv
         used.initial_guess = guess;
         used.scale_guess = 1u;
     }
+    if ((s = mark_stage(st, stages, 1)) != XS_OK) return s;
     s = solve_pressure(st, g, used, anchor, mask, pb, rhs, nullptr, pressure, nullptr, workspace, &w);
     if (s != XS_OK) return s;
+    if ((s = mark_stage(st, stages, 2)) != XS_OK) return s;
     if (coarse && (s = record_coarse_iterations(st, *history, workspace, g)) != XS_OK) return s;
     if (ring && (s = history_push(st, g, anchor, mask, pb, *history, pressure)) != XS_OK) return s;
     if (end && cudaEventRecord(end, st) != cudaSuccess) return XS_CUDA_ERROR;
-    if (solve.kind == XS_SOLVER_RED_BLACK_GAUSS_SEIDEL) return launch_project(st, g, mask, u, pressure, out);
-    return launch_project64(st, g, mask, u, w.x64, out);
+    if ((s = mark_stage(st, stages, 3)) != XS_OK) return s;
+    s = solve.kind == XS_SOLVER_RED_BLACK_GAUSS_SEIDEL ? launch_project(st, g, mask, u, pressure, out) : launch_project64(st, g, mask, u, w.x64, out);
+    if (s != XS_OK) return s;
+    return mark_stage(st, stages, 4);
 }
 
 // ------------------------------------------------------------ workspace
@@ -279,7 +286,9 @@ XsStatus xs_smoke_forward_step(cudaStream_t stream, const XsSmokeModel* m, XsSta
     const Grid g = make_grid(m->grid);
     const StepWorkspace w = carve_step(workspace, g, XS_MODE_FORWARD, m->warm_start_history, m->warm_start_coarsening);
     const InflowSet inflows = make_inflows(m->inflows, m->inflow_count);
+    cudaEvent_t* ev = m->stage_events;
     XsStatus s;
+    if ((s = mark_stage(stream, ev, 0)) != XS_OK) return s;
     // sources of density and temperature, then buoyancy on the sourced fields
     s = launch_source_buoyancy(stream, g, m->cell_mask, state.density, state.temperature, control.density_source,
                                control.temperature_source, control.external_acceleration, parameters.ambient_temperature,
@@ -290,21 +299,26 @@ XsStatus xs_smoke_forward_step(cudaStream_t stream, const XsSmokeModel* m, XsSta
         s = vorticity_forward(stream, g, m->cell_mask, state.velocity, parameters.vorticity_confinement, cache.vorticity, cache.force);
         if (s != XS_OK) return s;
     }
+    if ((s = mark_stage(stream, ev, 1)) != XS_OK) return s;
     // velocity evolution: integrate, advect (through the forced velocity), constrain
     s = launch_integrate(stream, g, m->cell_mask, state.velocity, cache.force, cache.forced_velocity);
     if (s != XS_OK) return s;
+    if ((s = mark_stage(stream, ev, 2)) != XS_OK) return s;
     s = launch_advect_constrain(stream, g, m->cell_mask, m->collider_velocity, cache.forced_velocity, m->velocity_boundary,
                                 cache.advected_velocity);
     if (s != XS_OK) return s;
+    if ((s = mark_stage(stream, ev, 3)) != XS_OK) return s;
     // projection
     s = projection_forward(stream, g, m->pressure, m->pressure_anchor, m->cell_mask, cache.advected_velocity, m->pressure_boundary,
                            w.pressure, w.rhs, next_state.velocity, w.solver, m->solve_begin, m->solve_end,
-                           reinterpret_cast<WarmStartNet*>(m->warm_start), &w.history);
+                           reinterpret_cast<WarmStartNet*>(m->warm_start), &w.history, ev ? ev + 4 : nullptr);
     if (s != XS_OK) return s;
     // scalar advection of the sourced fields through the projected velocity
-    return launch_advect_scalar_pair(stream, g, m->cell_mask, m->collider_density, m->collider_temperature, cache.sourced_density,
-                                     cache.sourced_temperature, next_state.velocity, m->density_boundary, m->temperature_boundary,
-                                     m->velocity_boundary, next_state.density, next_state.temperature);
+    s = launch_advect_scalar_pair(stream, g, m->cell_mask, m->collider_density, m->collider_temperature, cache.sourced_density,
+                                  cache.sourced_temperature, next_state.velocity, m->density_boundary, m->temperature_boundary,
+                                  m->velocity_boundary, next_state.density, next_state.temperature);
+    if (s != XS_OK) return s;
+    return mark_stage(stream, ev, 9);
 }
 
 // model.cpp:351-359

@@ -325,7 +325,16 @@ typedef struct XsSmokeModel {
      * step along it (before the learned correction's step).  It removes the
      * smooth error that fine-grid CG reduces slowest. */
     uint32_t warm_start_coarsening;
+    /* optional per-stage timing of xs_smoke_forward_step (NULL: none): an
+     * array of XS_STEP_STAGES + 1 events created by the caller with timing
+     * enabled, recorded on the step's stream at the stage boundaries:
+     * [0] start, [1] sources and forces done, [2] integration, [3] advection
+     * and constraint, [4] pressure right-hand side, [5] warm start (the fine
+     * PCG launch follows), [6] fine pressure solve, [7] ring update,
+     * [8] projection, [9] scalar advection (end of the step). */
+    cudaEvent_t* stage_events;
 } XsSmokeModel;
+#define XS_STEP_STAGES 9
 
 /* State / Control / Parameters (data.ixx:117-134) */
 typedef struct XsState { float* density; float* temperature; XsVector velocity; } XsState;

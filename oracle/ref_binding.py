@@ -39,6 +39,14 @@ def _p(n):
     return type(f"P{n}", (C.Structure,), {"_fields_": [(f"p{i}", C.c_void_p) for i in range(n)]})
 
 
+class RefLaunchArgs(C.Structure):
+    _fields_ = [("u", C.c_void_p * 3), ("out", C.c_void_p * 3), ("src", C.c_void_p), ("sout", C.c_void_p), ("rhs", C.c_void_p),
+                ("pressure", C.c_void_p), ("oa", C.c_void_p * 3), ("ua", C.c_void_p * 3), ("soa", C.c_void_p), ("sa", C.c_void_p)]
+
+
+# ref_launch kernels
+ADVECT_VELOCITY, CONSTRAIN_VELOCITY, ADVECT_SCALAR, PRESSURE_RHS, RBGS_SWEEPS, PROJECT_VELOCITY, ADVECT_VELOCITY_VJP, ADVECT_SCALAR_VJP = range(8)
+
 RefState = _p(5)
 RefControl = _p(5)
 RefParams = _p(4)
@@ -70,6 +78,7 @@ def lib():
         L.ref_advect_scalar.argtypes = [C.c_void_p, C.POINTER(RefModel), C.POINTER(RefScalarBoundary), C.c_void_p, C.c_void_p,
                                         C.c_void_p * 3, C.c_void_p]
         L.ref_rbgs.argtypes = [C.c_void_p, C.POINTER(RefModel), C.c_void_p, C.c_void_p, C.c_uint32]
+        L.ref_launch.argtypes = [C.c_void_p, C.POINTER(RefModel), C.c_uint32, C.POINTER(RefLaunchArgs)]
         _lib = L
     return _lib
 
@@ -166,3 +175,16 @@ class Reference:
     def rbgs(self, rhs, pressure, sweeps):
         if self.L.ref_rbgs(self._stream(), C.byref(self.m), C.c_void_p(rhs.data_ptr()), C.c_void_p(pressure.data_ptr()), sweeps) != 0:
             raise RuntimeError("reference rbgs failed")
+
+    def launch(self, which, u=None, out=None, src=None, sout=None, rhs=None, pressure=None, oa=None, ua=None, soa=None, sa=None):
+        """Enqueues one reference launcher (ref_launch) on the current stream,
+        without synchronising: for per-kernel timing with CUDA events."""
+        a = RefLaunchArgs()
+        ptr = lambda t: None if t is None else t.data_ptr()
+        for name, ts in (("u", u), ("out", out), ("oa", oa), ("ua", ua)):
+            if ts is not None:
+                getattr(a, name)[:] = [ptr(t) for t in ts]
+        a.src, a.sout, a.rhs, a.pressure, a.soa, a.sa = ptr(src), ptr(sout), ptr(rhs), ptr(pressure), ptr(soa), ptr(sa)
+        r = self.L.ref_launch(self._stream(), C.byref(self.m), int(which), C.byref(a))
+        if r != 0:
+            raise RuntimeError(f"reference launch {which} failed ({r})")

@@ -140,7 +140,9 @@ double ref_relative_residual(cudaStream_t stream, const RefModel* m, const float
 
 // projection_forward (operators.cu:1004-1013) with the RBGS loop run until
 // the FP64 relative residual reaches `tolerance` (checked every `check`
-// sweep pairs), or `max_sweeps` pairs.  Returns sweeps taken.
+// sweep pairs), or `max_sweeps` pairs, or until a check window no longer
+// lowers the residual by 0.1 % (the FP32 iteration has reached its rounding
+// floor).  Returns sweeps taken.
 uint32_t ref_projection_converged(cudaStream_t stream, const RefModel* m, float* const u[3], float* pressure, float* rhs, float* out[3],
                                   double tolerance, uint32_t max_sweeps, uint32_t check, double* partial_scratch, double* residual_out) {
     const Grid& g = m->grid;
@@ -156,7 +158,9 @@ uint32_t ref_projection_converged(cudaStream_t stream, const RefModel* m, float*
             rbgs_kernel<<<nb, 256, 0, stream>>>(g, 0, m->pressure_anchor, m->cell_mask, m->pressure_boundary, rhs, pressure);
             rbgs_kernel<<<nb, 256, 0, stream>>>(g, 1, m->pressure_anchor, m->cell_mask, m->pressure_boundary, rhs, pressure);
         }
+        const double previous = res;
         res = ref_relative_residual(stream, m, rhs, pressure, partial_scratch);
+        if (res > 0.999 * previous) break;
     }
     for (int a = 0; a < 3; ++a) {
         const unsigned fb = static_cast<unsigned>((faces(g, a) + 255) / 256);
@@ -354,6 +358,73 @@ int ref_vorticity_forward(cudaStream_t stream, const RefModel* m, float* const u
                           {force[0], force[1], force[2]});
     } catch (const std::exception&) { return 1; }
     return cudaStreamSynchronize(stream) == cudaSuccess ? 0 : 2;
+}
+
+// One reference launcher, enqueued without synchronisation, for per-kernel
+// timing with events on the stream.  `which`:
+//   0 advect_velocity_forward (u -> out)      1 constrain_velocity_forward (u -> out)
+//   2 advect_scalar_forward (src, u -> sout)  3 pressure_rhs (u -> rhs)
+//   4 one red-black sweep pair (rhs, p)       5 project_velocity, 3 axes (u, p -> out)
+//   6 advect_velocity_vjp (u, oa -> ua)       7 advect_scalar_vjp (src, u, soa -> sa, ua)
+struct RefLaunchArgs {
+    float* u[3];
+    float* out[3];
+    const float* src;
+    float* sout;
+    float* rhs;
+    float* pressure;
+    double* oa[3];
+    double* ua[3];
+    const double* soa;
+    double* sa;
+};
+
+int ref_launch(cudaStream_t stream, const RefModel* m, uint32_t which, const RefLaunchArgs* a) {
+    try {
+        const Grid& g = m->grid;
+        const uint32_t* mask = m->cell_mask;
+        const unsigned nb = static_cast<unsigned>((cells(g) + 255) / 256);
+        switch (which) {
+            case 0:
+                advect_velocity_forward(stream, g, mask, {a->u[0], a->u[1], a->u[2]}, m->velocity_boundary, {a->out[0], a->out[1], a->out[2]});
+                break;
+            case 1:
+                constrain_velocity_forward(stream, g, mask, {m->collider_velocity[0], m->collider_velocity[1], m->collider_velocity[2]},
+                                           {a->u[0], a->u[1], a->u[2]}, m->velocity_boundary, {a->out[0], a->out[1], a->out[2]});
+                break;
+            case 2:
+                advect_scalar_forward(stream, g, mask, {m->collider_density}, {a->src}, {a->u[0], a->u[1], a->u[2]}, m->density_boundary,
+                                      m->velocity_boundary, {a->sout});
+                break;
+            case 3:
+                pressure_rhs_kernel<<<nb, 256, 0, stream>>>(g, m->pressure_anchor, mask, ConstStaggeredVectorView{a->u[0], a->u[1], a->u[2]},
+                                                            a->rhs);
+                break;
+            case 4:
+                rbgs_kernel<<<nb, 256, 0, stream>>>(g, 0, m->pressure_anchor, mask, m->pressure_boundary, a->rhs, a->pressure);
+                rbgs_kernel<<<nb, 256, 0, stream>>>(g, 1, m->pressure_anchor, mask, m->pressure_boundary, a->rhs, a->pressure);
+                break;
+            case 5:
+                for (int axis = 0; axis < 3; ++axis) {
+                    const unsigned fb = static_cast<unsigned>((faces(g, axis) + 255) / 256);
+                    project_velocity_kernel<<<fb, 256, 0, stream>>>(g, axis, mask, a->u[axis], a->pressure, a->out[axis]);
+                }
+                break;
+            case 6:
+                advect_velocity_vjp(stream, g, mask, {a->u[0], a->u[1], a->u[2]}, m->velocity_boundary, {a->oa[0], a->oa[1], a->oa[2]},
+                                    {a->ua[0], a->ua[1], a->ua[2]});
+                break;
+            case 7:
+                advect_scalar_vjp(stream, g, mask, {a->src}, {a->u[0], a->u[1], a->u[2]}, m->density_boundary, m->velocity_boundary, {a->soa},
+                                  {a->sa}, {a->ua[0], a->ua[1], a->ua[2]});
+                break;
+            default:
+                return 3;
+        }
+    } catch (const std::exception&) {
+        return 1;
+    }
+    return cudaGetLastError() == cudaSuccess ? 0 : 2;
 }
 
 // Layout check: the harness' view of the model block as 32-bit words.

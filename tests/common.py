@@ -226,3 +226,55 @@ def density_distance(density, target):
     """The loss of the differentiable plume: ||rho_T - target||_2."""
     d = np.asarray(density, np.float64) - target
     return float(np.sqrt(d @ d))
+
+
+# ---------------------------------------------------------------- parity report
+def report(name, **values):
+    """Appends one JSON line of measured errors to $XS_PARITY_REPORT (when set),
+    so that a GPU run leaves the per-field numbers behind."""
+    import json
+    path = os.environ.get("XS_PARITY_REPORT")
+    if path:
+        with open(path, "a") as f:
+            f.write(json.dumps({"test": name, **values}) + "\n")
+
+
+def field_errors(got, want):
+    """Relative L2 errors of density, temperature and the velocity field (the
+    three face components together) of two state dicts."""
+    cat = lambda s: np.concatenate([np.asarray(v, np.float64).ravel() for v in s["velocity"]])
+    return {"density": rel_l2(got["density"], want["density"]), "temperature": rel_l2(got["temperature"], want["temperature"]),
+            "velocity": rel_l2(cat(got), cat(want))}
+
+
+def reference_step(cfg, domain, state, control, params, tolerance=0.0, max_sweeps=400000):
+    """One step of the reference's own kernels (oracle/_ref) from host state
+    arrays: RBGS with the configured sweep count, or (tolerance > 0) iterated
+    until the FP64 relative residual reaches `tolerance` or stops falling.
+    Inflow spheres are emulated with sources.  Returns (next state dict,
+    sweeps, residual)."""
+    import torch
+    from oracle import ref_binding as rb
+    ref = rb.Reference(cfg, domain)
+    dev = torch.device("cuda")
+    t = lambda a: torch.as_tensor(np.asarray(a), dtype=torch.float32, device=dev).contiguous()
+    s_in = [t(a) for a in state_arrays(state)]
+    rctl = reference_control(cfg, state, control)
+    c_in = [t(rctl["density_source"]), t(rctl["temperature_source"])] + [t(a) for a in rctl["acceleration"]]
+    p_in = [torch.tensor([params[k]], dtype=torch.float32, device=dev) for k in
+            ("ambient_temperature", "density_buoyancy", "temperature_buoyancy", "vorticity_confinement")]
+    out = [torch.zeros_like(x) for x in s_in]
+    n = s_in[0].numel()
+    cache = [torch.zeros(n, device=dev) for _ in range(5)] + [torch.zeros((11, n), device=dev)] + \
+            [torch.zeros_like(x) for x in s_in[2:]] + [torch.zeros_like(x) for x in s_in[2:]]
+    sweeps, residual = ref.forward_step(s_in, c_in, p_in, out, cache, tolerance=tolerance, max_sweeps=max_sweeps)
+    torch.cuda.synchronize()
+    o = [x.cpu().numpy() for x in out]
+    return {"density": o[0], "temperature": o[1], "velocity": o[2:5]}, sweeps, residual
+
+
+def product_domain(ctx):
+    """The rasterised domain of a product context, as the reference harness takes it."""
+    d = ctx.domain
+    return {"mask": d.cell_mask, "cv": list(d.collider_velocity.components()), "cd": d.collider_density.values,
+            "ct": d.collider_temperature.values, "anchor": d.pressure_anchor}
