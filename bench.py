@@ -8,7 +8,8 @@ velocity on the sides and bottom, open top), pressure by Jacobi-PCG to a
 1e-6 relative residual.  One step is Model.forward_step through the C ABI.
 
 The plume first spins up from rest (seeded uniform velocity noise in
-+-0.01) for --spinup steps; every arm then starts from that state:
++-0.01) for --spinup steps (180: the timed window is steps 185-205 of the
+200-step plume); every arm then starts from that state:
 
   plain                   zero start (the reference's zero-initialised solve)
   history                 Galerkin start from the last 5 forward solutions
@@ -19,15 +20,29 @@ The plume first spins up from rest (seeded uniform velocity noise in
   learned+history+coarse  the ring start, the coarse-grid step, then the
                           network's step (headline)
 
-Each arm runs W warm-up steps (which also refill its ring) and K timed steps.
-``value`` is the headline arm's steps/s; every arm's steps/s and PCG
-iterations are in ``arms``.
+Each arm runs W warm-up steps (which also refill its ring) and K timed steps,
+every timed step with per-stage CUDA events (XsSmokeModel.stage_events).
+``value`` is the headline arm's steps/s; every arm's steps/s, PCG iterations
+and per-stage times are in ``arms``.  Further records of the same run:
+
+  roofline            the headline arm's dominant kernel, the fine PCG launch
+                      (stage events around it), against the measured copy peak
+  roofline_plain      the same kernel in the plain arm
+  adjoint             the 40-step VJP (checkpoints every 8) ending at step 200,
+                      with the reverse step's algorithmic bytes
+  reference_kernels   the reference's own kernels (oracle/_ref) timed per kernel
+                      on the same box and state, next to this library's
+  large_grid          512x512x256: plain and headline arms, per-stage GB/s
+  cpu_baseline        full FP64 oracle steps from the spun-up state on the
+                      host's cores
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl product|reference]
 
 With N > 1 (torchrun, one rank per GPU) every rank runs an independent
 replica of the workload (the path does not shard: replicas only), timing is
-max over ranks and ``value`` is the steps of all ranks per second.
+max over ranks and ``value`` is the steps of all ranks per second.  The
+reference arm (--impl reference) times the FP64 oracle's full steps from the
+same spun-up state on rank 0 (the other ranks exit).
 """
 from __future__ import annotations
 
@@ -50,6 +65,8 @@ GRID = 256
 HISTORY = 5
 COARSENING = 2  # coarse-grid correction of the start on the grid coarsened x2 per axis
 WEIGHTS = os.path.join(ROOT, "diff_solver_b200", "weights", "warm_start_128.npz")
+HEADLINE = "learned+history+coarse"
+LARGE_GRID = (512, 512, 256)
 
 
 def grid_shape(spec):
@@ -130,6 +147,11 @@ def measured_peaks():
     return 6650.0, "fallback"
 
 
+def counts(shape):
+    nx, ny, nz = shape
+    return nx * ny * nz, (nx + 1) * ny * nz + nx * (ny + 1) * nz + nx * ny * (nz + 1)
+
+
 # DRAM traffic of the plain solve's persistent PCG launch per algorithmic byte,
 # from one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of this
 # workload's plain solve at 256^3: 800.5 GB for 1323 CG iterations and 2
@@ -137,13 +159,50 @@ def measured_peaks():
 PCG_TRAFFIC_PER_ALGORITHMIC_BYTE_256 = 800.5 / 801.7
 
 
-def pcg_algorithmic_bytes(n_cells, iterations, refinements):
+def pcg_algorithmic_bytes(n_cells, iterations, refinements, smoothed=0):
     """Unique bytes the persistent PCG kernel must move: per CG iteration
     36 B/cell (spmv phase: read z, p_old, e; write p_new, q, e -- 24 B;
-    update phase: read z, q; write z -- 12 B); per true-residual pass 36 B
-    (read rhs 4 + x64 8, write z, p0, e, pressure 16, x64 8) plus 24 B for
-    each fold (read e, p, x64; write x64)."""
-    return n_cells * (36.0 * iterations + 36.0 * (refinements + 1) + 24.0 * refinements)
+    update phase: read z, q; write z -- 12 B), 16 B/cell more for each
+    iteration that also carries the minimal-residual smoothed sequence (read
+    and write s and y); per true-residual pass 36 B (read rhs 4 + x64 8,
+    write z, p0, e, pressure 16, x64 8) plus 24 B for each fold (read e, p,
+    x64; write x64)."""
+    return n_cells * (36.0 * iterations + 16.0 * smoothed + 36.0 * (refinements + 1) + 24.0 * refinements)
+
+
+# Algorithmic bytes of the step's stages (stage k runs between events k and
+# k + 1), as functions of the cell count N and the face count F: unique reads
+# plus writes of every array the stage's kernels must touch.
+def stage_bytes(n, f):
+    return {
+        "sources_forces": 48.0 * n,             # read rho, T, 2 sources, 3 accelerations; write 2 sourced fields, 3 forces
+        "integrate": 8.0 * f + 12.0 * n,        # read u, write u*; read the 3 force fields
+        "advect_constrain": 8.0 * f,            # read u* (staged), write the advected velocity
+        "pressure_rhs": 4.0 * f + 4.0 * n,      # read u, write the right-hand side
+        "warm_start": None,                     # ring Galerkin pass, sweeps, coarse solves, network, line steps
+        "fine_pcg": None,                       # pcg_algorithmic_bytes of the launch
+        "ring_update": None,
+        "projection": 8.0 * f + 8.0 * n,        # read u and the FP64 pressure, write u
+        "scalar_advection": 4.0 * f + 16.0 * n,  # read u (staged), 2 sourced fields; write density, temperature
+    }
+
+
+STAGES = ["sources_forces", "integrate", "advect_constrain", "pressure_rhs", "warm_start", "fine_pcg", "ring_update", "projection",
+          "scalar_advection"]
+
+
+def reverse_step_bytes(n, f, forward_iterations, adjoint_iterations):
+    """Algorithmic bytes of one checkpointed reverse step: the recomputed
+    forward step (each state of a segment is recomputed once) plus the VJP
+    step's transposes and its adjoint solve.  FP64 adjoints (8 B), FP32
+    state (4 B), accumulated targets counted read + write:
+      zeroing the scratch adjoints 8 (5N + 9F); copy of the incoming velocity
+      adjoint 16F; scalar advection adjoint (density and temperature) 20F +
+      56N; projection adjoint 40F + 16N (+ 36 B/cell per adjoint CG
+      iteration); constraint 24F; velocity advection adjoint 28F; integration
+      24F + 48N; buoyancy 112N; sources 80N: 352N + 224F in all."""
+    forward = 4.0 * (8 * n + 8 * f) + 36.0 * n * forward_iterations
+    return forward + 352.0 * n + 224.0 * f + 36.0 * n * adjoint_iterations
 
 
 def init_distributed():
@@ -179,36 +238,32 @@ def max_over_ranks(value, world):
 
 
 # --------------------------------------------------------------------- CPU
-def cpu_sample(shape=(GRID,) * 3, sample_iterations=40, gpu_iterations=None):
-    """The FP64 oracle step on the host cores: one step with the PCG capped at
-    0 and at `sample_iterations` iterations; the step time at the GPU's
-    iteration count is t0 + k * (t_k - t0) / sample_iterations."""
+def cpu_steps(state_arrays, shape, budget_s=60.0, max_steps=3, min_steps=1):
+    """Full forward steps of the FP64 CPU oracle (the same step, pressure by
+    Jacobi-PCG to 1e-6 from a zero start as the plain arm) from the given
+    host state, on all host cores, in sequence; stops after max_steps or once
+    budget_s is spent (at least min_steps).  Returns the timing record."""
     import numpy as np
+
     from oracle import binding as ob
-    threads = os.cpu_count() or 1
-    ob.set_threads(threads)
+    threads = ob.set_threads(os.cpu_count() or 1)
     cfg = workload_configuration(shape)
-    rng = np.random.default_rng(0)
-    P0 = ob.Problem(cfg, "f64", solver="pcg", iterations=0, tolerance=1e-6)
-    st = ob.zeros_state(P0.res, np.float64)
-    for a in range(3):
-        st["velocity"][a][:] = rng.uniform(-0.01, 0.01, st["velocity"][a].shape)
-    ctl = ob.zeros_control(P0.res, np.float64)
-    t = time.perf_counter()
-    P0.forward_step(st, ctl, PARAMS)
-    t0 = time.perf_counter() - t
-    Pk = ob.Problem(cfg, "f64", solver="pcg", iterations=sample_iterations, tolerance=1e-30)
-    t = time.perf_counter()
-    _, _, stats, _ = Pk.forward_step(st, ctl, PARAMS)
-    tk = time.perf_counter() - t
-    per_iteration = max(tk - t0, 0.0) / max(stats.iterations, 1)
-    k = gpu_iterations if gpu_iterations is not None else 1400
-    seconds = t0 + k * per_iteration
-    return {"value": 1.0 / seconds, "unit": UNIT, "cores": threads, "kind": "port",
-            "sample": f"FP64 oracle forward step at {'x'.join(map(str, shape))} on {threads} threads: one step with 0 and one with {sample_iterations} "
-                      f"PCG iterations ({t0:.2f} s, {tk:.2f} s), projected to {k} iterations per step "
-                      f"({per_iteration * 1e3:.1f} ms per iteration)",
-            "seconds_per_step": seconds}
+    P = ob.Problem(cfg, "f64", solver="pcg", iterations=20000, tolerance=1e-6)
+    ctl = ob.zeros_control(P.res, np.float64)
+    st = state_arrays
+    times, iterations = [], []
+    t_all = time.perf_counter()
+    while len(times) < max_steps and (len(times) < min_steps or time.perf_counter() - t_all < budget_s):
+        t = time.perf_counter()
+        st, _, stats, _ = P.forward_step(st, ctl, PARAMS)
+        times.append(time.perf_counter() - t)
+        iterations.append(int(stats.iterations))
+    seconds = statistics.mean(times)
+    return {"value": 1.0 / seconds, "unit": UNIT, "cores": threads, "kind": "port", "steps": len(times),
+            "sample": f"{len(times)} full FP64 oracle forward step(s) at {'x'.join(map(str, shape))} from the spun-up plume state, "
+                      f"pressure by Jacobi-PCG to 1e-6 from zero ({', '.join(map(str, iterations))} iterations; "
+                      f"{', '.join(f'{t:.1f}' for t in times)} s) on {threads} host threads",
+            "seconds_per_step": seconds, "iterations": iterations}
 
 
 # --------------------------------------------------------------------- product
@@ -238,9 +293,15 @@ class Rollout:
         self.cur, self.other = self.other, self.cur
 
 
+def make_events(count):
+    import torch
+    return [torch.cuda.Event(enable_timing=True) for _ in range(count)]
+
+
 def timed_arm(args, world, ro, initial, e2e=False):
-    """W warm-up and K timed steps of one arm from `initial`; per-step solve
-    windows (warm start + PCG) timed by events the step records."""
+    """W warm-up and K timed steps of one arm from `initial`; each timed step
+    records the stage events of the step (XsSmokeModel.stage_events) and the
+    solve statistics."""
     import torch
 
     from diff_solver_b200 import _native as N
@@ -255,10 +316,12 @@ def timed_arm(args, world, ro, initial, e2e=False):
     stats_off = L.xs_solve_stats_offset()
     stats_dev = ro.ctx.workspace[stats_off:stats_off + C.sizeof(N.XsSolveStats)]
     stats_host = torch.zeros((k_steps, C.sizeof(N.XsSolveStats)), dtype=torch.uint8).pin_memory()
-    events = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(k_steps)]
-    for a, b in events:
-        a.record(stream)
-        b.record(stream)
+    stages = [make_events(N.XS_STEP_STAGES + 1) for _ in range(k_steps)]
+    arrays = []
+    for evs in stages:
+        for e in evs:
+            e.record(stream)  # creates the CUDA events
+        arrays.append((C.c_void_p * len(evs))(*[e.cuda_event for e in evs]))
     barrier(world)
     torch.cuda.synchronize()
     launches0 = L.xs_launch_count()
@@ -266,22 +329,21 @@ def timed_arm(args, world, ro, initial, e2e=False):
     start.record(stream)
     with torch.cuda.stream(stream):
         for i in range(k_steps):
-            ro.ctx.native.solve_begin = events[i][0].cuda_event
-            ro.ctx.native.solve_end = events[i][1].cuda_event
+            ro.ctx.native.stage_events = C.cast(arrays[i], C.c_void_p)
             ro.step()
             stats_host[i].copy_(stats_dev, non_blocking=True)
     end.record(stream)
     torch.cuda.synchronize()
     launches = L.xs_launch_count() - launches0
     barrier(world)
-    ro.ctx.native.solve_begin = None
-    ro.ctx.native.solve_end = None
+    ro.ctx.native.stage_events = None
     per_step = [N.XsSolveStats.from_buffer_copy(bytes(stats_host[i].numpy())) for i in range(k_steps)]
+    stage_ms = {name: [evs[k].elapsed_time(evs[k + 1]) for evs in stages] for k, name in enumerate(STAGES)}
     out = dict(elapsed_ms=max_over_ranks(start.elapsed_time(end), world), launches=launches,
                iterations=[s.iterations for s in per_step], refinements=[s.refinements for s in per_step],
-               coarse_iterations=[s.coarse_iterations for s in per_step],
+               smoothed=[s.smoothed_iterations for s in per_step], coarse_iterations=[s.coarse_iterations for s in per_step],
                residuals=[s.final_residual for s in per_step], initial_residuals=[s.initial_residual for s in per_step],
-               solve_ms=[a.elapsed_time(b) for a, b in events])
+               stage_ms=stage_ms, solve_ms=[w + p for w, p in zip(stage_ms["warm_start"], stage_ms["fine_pcg"])])
     if e2e:
         # the same K steps again, from the same state after the same warm-up
         ro.load(initial)
@@ -351,76 +413,321 @@ def end_to_end(args, world, ro):
     return dict(e2e_ms=max_over_ranks(e_start.elapsed_time(e_end), world), h2d=5 * n * 4, d2h=6 * 8, metrics=metrics_host[-1].numpy())
 
 
-def product_run(args, world, rank, local):
+def load_network(args, shape):
+    from diff_solver_b200.warm_start import WarmStartNetwork
+    if not os.path.exists(args.weights):
+        raise FileNotFoundError(f"{args.weights} is missing: train it with python -m diff_solver_b200.train_warm_start")
+    # trained at 128^3, applied fully convolutionally on the grid restricted
+    # x network_factor (2 by default)
+    f = args.network_factor
+    network = WarmStartNetwork(tuple(s // f for s in shape), factor=f)
+    network.load(args.weights)
+    return network
+
+
+def spin_up(shape, network, steps, keep=()):
+    """The plume from rest (seeded velocity noise) with the headline start;
+    returns {step: state copy} for the steps in `keep` and the last."""
     import torch
-    torch.cuda.set_device(local)
-    network = None
-    if not args.no_learned:
-        from diff_solver_b200.warm_start import WarmStartNetwork
-        if not os.path.exists(args.weights):
-            raise FileNotFoundError(f"{args.weights} is missing: train it with python -m diff_solver_b200.train_warm_start")
-        # trained at 128^3, applied fully convolutionally on the grid restricted
-        # x network_factor (2 by default)
-        f = args.network_factor
-        network = WarmStartNetwork(tuple(s // f for s in args.shape), factor=f)
-        network.load(args.weights)
-    # spin-up from rest with the fastest start; its final state opens every arm
-    spin = Rollout(args.shape, HISTORY, network, args.coarsening)
+
+    from diff_solver_b200.model import tensors_of
+    spin = Rollout(shape, HISTORY, network, COARSENING)
     gen = torch.Generator(device="cuda").manual_seed(0)
     for t in spin.cur.velocity.components():
         t.uniform_(-0.01, 0.01, generator=gen)
+    saved = {}
+
+    def save(step):
+        s = spin.model.allocate_state(spin.ctx)
+        for d, src in zip(tensors_of(s), tensors_of(spin.cur)):
+            d.copy_(src)
+        saved[step] = s
+
     with torch.cuda.stream(spin.ctx.stream):
-        for _ in range(args.spinup):
+        for k in range(steps):
+            if k in keep:
+                save(k)
             spin.step()
+        save(steps)
     torch.cuda.synchronize()
-    from diff_solver_b200.model import tensors_of
-    initial = spin.model.allocate_state(spin.ctx)
-    for d, s in zip(tensors_of(initial), tensors_of(spin.cur)):
-        d.copy_(s)
+    return saved, spin
+
+
+def summarize(results, args, shape, world, headline):
+    n, faces = counts(shape)
+    peak, peak_kind = measured_peaks()
+    sb = stage_bytes(n, faces)
+    steps_total = args.steps * world
+    arms = {}
+    for name, r in results.items():
+        stage = {}
+        for s in STAGES:
+            ms = statistics.mean(r["stage_ms"][s])
+            rec = {"ms": ms}
+            if sb[s] is not None:
+                rec["bytes"] = sb[s]
+                rec["gbs"] = sb[s] / (ms / 1e3) / 1e9
+            stage[s] = rec
+        pcg_bytes = [pcg_algorithmic_bytes(n, it, rf, sm) for it, rf, sm in zip(r["iterations"], r["refinements"], r["smoothed"])]
+        stage["fine_pcg"]["bytes"] = statistics.mean(pcg_bytes)
+        stage["fine_pcg"]["gbs"] = sum(pcg_bytes) / (sum(r["stage_ms"]["fine_pcg"]) / 1e3) / 1e9
+        b_step = 4.0 * (8 * n + 8 * faces) + 40.0 * n * statistics.mean(r["iterations"])
+        arms[name] = {"steps_per_s": steps_total / (r["elapsed_ms"] / 1e3), "ms_per_step": r["elapsed_ms"] / args.steps,
+                      "pcg_iterations_per_step": r["iterations"], "mean_pcg_iterations": statistics.mean(r["iterations"]),
+                      "smoothed_iterations_per_step": r["smoothed"], "coarse_iterations_per_step": r["coarse_iterations"],
+                      "refinement_passes_per_step": r["refinements"], "solve_ms_per_step": statistics.mean(r["solve_ms"]),
+                      "initial_residuals": r["initial_residuals"], "final_residuals": r["residuals"], "gpu_launches": r["launches"],
+                      "stages": stage,
+                      "step_roofline": {"bytes_per_step": b_step, "achieved_gbs": b_step / (r["elapsed_ms"] / args.steps / 1e3) / 1e9,
+                                        "frac": b_step / (r["elapsed_ms"] / args.steps / 1e3) / 1e9 / peak}}
+
+    def pcg_roofline(arm):
+        r = results[arm]
+        pcg_bytes = [pcg_algorithmic_bytes(n, it, rf, sm) for it, rf, sm in zip(r["iterations"], r["refinements"], r["smoothed"])]
+        achieved = sum(pcg_bytes) / (sum(r["stage_ms"]["fine_pcg"]) / 1e3) / 1e9
+        kernel = "pcg_kernel<1, 1>" if arm != "plain" else "pcg_kernel<1, 0>"
+        return {"bound": "hbm", "kernel": kernel, "arm": arm, "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_kind": peak_kind, "algorithmic_bytes_per_launch": statistics.mean(pcg_bytes),
+                "launch_ms": statistics.mean(r["stage_ms"]["fine_pcg"]), "iterations_per_launch": statistics.mean(r["iterations"]),
+                "smoothed_iterations_per_launch": statistics.mean(r["smoothed"])}
+    return arms, pcg_roofline
+
+
+def adjoint_record(args, shape, network, start_state, window=40, checkpoint=8):
+    """Config 3's reverse pass: from the state at step 200 - window, the
+    window's steps with checkpoints every `checkpoint`, then the VJP of the
+    final density's L2 distance to a Gaussian target (sigma 0.1 at a seeded
+    centre) back to the window's start.  Forward and adjoint solves use the
+    headline starts (the network only in the forward solves)."""
+    import numpy as np
+    import torch
+
+    from diff_solver_b200.model import ExecutionMode, Model, fill_parameters
+    from diff_solver_b200.solver import TapeMode, simulate, vjp
+    cfg = workload_configuration(shape, HISTORY, COARSENING)
+    model = Model(cfg)
+    ctx = model.allocate_context(ExecutionMode.differentiable)
+    if network is not None:
+        ctx.set_learned_warm_start(network)
+    ctx.reset_warm_start()
+    params = fill_parameters(model.allocate_parameters(ctx), **PARAMS)
+    controls = [model.allocate_control(ctx) for _ in range(window)]
+    nx, ny, nz = shape
+    centre = np.random.default_rng(1).uniform(0.3, 0.7, 3) * np.array([1.0, ny / nx, nz / nx])
+    x = (torch.arange(nx, device="cuda", dtype=torch.float64) + 0.5) / nx
+    y = (torch.arange(ny, device="cuda", dtype=torch.float64) + 0.5) / nx
+    z = (torch.arange(nz, device="cuda", dtype=torch.float64) + 0.5) / nx
+    Z, Y, X = torch.meshgrid(z, y, x, indexing="ij")
+    target = torch.exp(-((X - centre[0]) ** 2 + (Y - centre[1]) ** 2 + (Z - centre[2]) ** 2) / (2 * 0.1 ** 2)).reshape(-1)
+    del X, Y, Z
+    ev = make_events(3)
+    torch.cuda.synchronize()
+    ev[0].record()
+    traj = simulate(model, ctx, start_state, controls, params, TapeMode.checkpoint, checkpoint)
+    ev[1].record()
+    final = traj.states[-1].density.values.double()
+    d = final - target
+    loss = torch.sqrt((d * d).sum())
+    seed = model.allocate_state_adjoint(ctx)
+    seed.density.values.copy_(d / loss)
+    grad = vjp(model, ctx, traj, controls, params, {window: seed})
+    ev[2].record()
+    torch.cuda.synchronize()
+    stats = ctx.read_solve_stats()
+    gnorm = float(sum((t.double() ** 2).sum() for t in grad.initial_state.velocity.components()) ** 0.5)
+    n, faces = counts(shape)
+    reverse_ms = ev[1].elapsed_time(ev[2]) / window
+    return {"window": window, "checkpoint": checkpoint, "steps": f"{200 - window}-200", "loss": float(loss),
+            "forward_ms": ev[0].elapsed_time(ev[1]), "vjp_ms": ev[1].elapsed_time(ev[2]), "ms_per_reverse_step": reverse_ms,
+            "gradient_norm": gnorm, "last_adjoint_solve": {"iterations": stats["iterations"], "residual": stats["final_residual"]},
+            "bytes_rule": "reverse_step_bytes(N, F, forward PCG iterations, adjoint PCG iterations)", "_n": n, "_f": faces}
+
+
+def reference_kernels_record(args, ro, shape, repeats=5):
+    """The reference's own kernels (solvers/smoke/operators.cu through
+    oracle/_ref) timed one by one with CUDA events on the state of the last
+    headline step, next to this library's kernels for the same operation.
+    Algorithmic bytes as stage_bytes (the reference's advection + constraint
+    and scalar advection count the same arrays)."""
+    import torch
+
+    from diff_solver_b200 import _native as N
+    from oracle import ref_binding as rb
+    if not rb.available():
+        return {"unavailable": "oracle/_ref is not built"}
+    n, faces = counts(shape)
+    ctx = ro.ctx
+    d = ctx.domain
+    dom = {"mask": d.cell_mask, "cv": list(d.collider_velocity.components()), "cd": d.collider_density.values,
+           "ct": d.collider_temperature.values, "anchor": d.pressure_anchor}
+    ref = rb.Reference(ro.model.configuration, dom, iterations=1)
+    dev = torch.device("cuda")
+    forced = list(ro.cache.forced_velocity.components())
+    u_next = list(ro.cur.velocity.components())
+    out = [torch.empty_like(t) for t in forced]
+    raw = [torch.empty_like(t) for t in forced]
+    src = ro.cache.sourced_density.values
+    sout = torch.empty_like(src)
+    rhs = torch.empty(n, device=dev)
+    pressure = ctx.pressure_fields()[0].clone()
+    gen = torch.Generator(device="cuda").manual_seed(3)
+    oa = [torch.randn(t.numel(), generator=gen, device=dev, dtype=torch.float64) for t in forced]
+    ua = [torch.zeros(t.numel(), device=dev, dtype=torch.float64) for t in forced]
+    soa = torch.randn(n, generator=gen, device=dev, dtype=torch.float64)
+    sa = torch.zeros(n, device=dev, dtype=torch.float64)
+    L = N.lib()
+    g = ctx.native.grid
+    vb = ctx.native.velocity_boundary
+
+    def time_it(fn):
+        fn()
+        torch.cuda.synchronize()
+        a, b = make_events(2)
+        a.record()
+        for _ in range(repeats):
+            fn()
+        b.record()
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / repeats
+
+    R = rb
+    rec = {}
+    rec["advect_constrain"] = {"reference_ms": time_it(lambda: (ref.launch(R.ADVECT_VELOCITY, u=forced, out=raw),
+                                                                ref.launch(R.CONSTRAIN_VELOCITY, u=raw, out=out)))}
+    rec["scalar_advection"] = {"reference_ms": time_it(lambda: (ref.launch(R.ADVECT_SCALAR, src=src, u=u_next, sout=sout),
+                                                                ref.launch(R.ADVECT_SCALAR, src=ro.cache.sourced_temperature.values,
+                                                                           u=u_next, sout=sout)))}
+    rec["pressure_rhs"] = {"reference_ms": time_it(lambda: ref.launch(R.PRESSURE_RHS, u=forced, rhs=rhs))}
+    rec["projection"] = {"reference_ms": time_it(lambda: ref.launch(R.PROJECT_VELOCITY, u=forced, pressure=pressure, out=out))}
+    sweep_ms = time_it(lambda: ref.launch(R.RBGS_SWEEPS, rhs=rhs, pressure=pressure))
+    rec["pressure_iteration"] = {"reference_ms": sweep_ms, "reference": "one red-black Gauss-Seidel sweep pair (rbgs_kernel x2)",
+                                 "reference_bytes": 2 * 4.0 * n * 2, "reference_gbs": 16.0 * n / (sweep_ms / 1e3) / 1e9}
+    rec["advect_velocity_vjp"] = {"reference_ms": time_it(lambda: ref.launch(R.ADVECT_VELOCITY_VJP, u=forced, oa=oa, ua=ua)),
+                                  "product_ms": time_it(lambda: N.check("vjp", L.xs_advect_velocity_vjp(ctx.stream_handle, g, None,
+                                                                                                        N.vec(forced), vb, N.vec(oa),
+                                                                                                        N.vec(ua)))),
+                                  "bytes": 4.0 * faces + 8.0 * faces + 16.0 * faces}
+    rec["advect_scalar_vjp"] = {"reference_ms": time_it(lambda: ref.launch(R.ADVECT_SCALAR_VJP, src=src, u=u_next, soa=soa, sa=sa, ua=ua)),
+                                "product_ms": time_it(lambda: N.check("svjp", L.xs_advect_scalar_vjp(
+                                    ctx.stream_handle, g, None, C.c_void_p(src.data_ptr()), N.vec(u_next), ctx.native.density_boundary, vb,
+                                    C.c_void_p(soa.data_ptr()), C.c_void_p(sa.data_ptr()), N.vec(ua)))),
+                                "bytes": 4.0 * faces + 4.0 * n + 8.0 * n + 16.0 * n + 16.0 * faces}
+    del ref
+    return rec
+
+
+def large_grid_record(args, network_large, shape=LARGE_GRID, spinup=40, warmup=3, steps=5, headline_steps=10):
+    import torch
+    saved, spin = spin_up(shape, network_large, spinup)
+    initial = saved[spinup]
     del spin
+    torch.cuda.empty_cache()
+    sub = argparse.Namespace(steps=steps, warmup=warmup)
+    results = {}
+    for name, history, net, coarsening, k in (("plain", 0, None, 0, steps), (HEADLINE, HISTORY, network_large, COARSENING, headline_steps)):
+        ro = Rollout(shape, history, net, coarsening)
+        sub.steps = k
+        results[name] = timed_arm(sub, 1, ro, initial)
+        results[name]["_steps"] = k
+        del ro
+        torch.cuda.empty_cache()
+    return results
+
+
+def product_run(args, world, rank, local):
+    import torch
+    torch.cuda.set_device(local)
+    network = None if args.no_learned else load_network(args, args.shape)
+    window = args.adjoint_window
+    keep = (max(args.spinup + 20 - window, 0),) if not args.no_adjoint else ()
+    saved, spin = spin_up(args.shape, network, args.spinup, keep)
+    initial = saved[args.spinup]
+    del spin
+    torch.cuda.empty_cache()
     arms = [("plain", 0, None, 0), ("history", HISTORY, None, 0)]
     if args.coarsening:
         arms += [("history+coarse", HISTORY, None, args.coarsening)]
     if network is not None:
         arms += [("learned", 0, network, 0), ("learned+history", HISTORY, network, 0)]
         if args.coarsening:
-            arms += [("learned+history+coarse", HISTORY, network, args.coarsening)]
+            arms += [(HEADLINE, HISTORY, network, args.coarsening)]
     if args.arms:  # a subset (profiling runs); the last one named is the headline
-        keep = args.arms.split(",")
-        unknown = [k for k in keep if k not in {a[0] for a in arms}]
+        keep_arms = args.arms.split(",")
+        unknown = [k for k in keep_arms if k not in {a[0] for a in arms}]
         if unknown:
             raise ValueError(f"unknown arms {unknown}: choose from {[a[0] for a in arms]}")
-        arms = [a for k in keep for a in arms if a[0] == k]
+        arms = [a for k in keep_arms for a in arms if a[0] == k]
     headline = arms[-1][0]
     sampler = ClockSampler(local)
     sampler.start()
     results = {}
+    extra = {}
     for name, history, net, coarsening in arms:
         ro = Rollout(args.shape, history, net, coarsening)
         results[name] = timed_arm(args, world, ro, initial, e2e=(name == headline))
+        if name == headline and not args.no_reference_kernels and world == 1:
+            extra["reference_kernels"] = reference_kernels_record(args, ro, args.shape)
         del ro
         torch.cuda.empty_cache()
     clocks = sampler.stop()
+    if not args.no_adjoint and world == 1:
+        extra["adjoint"] = adjoint_record(args, args.shape, network, saved[keep[0]], window=window)
+        torch.cuda.empty_cache()
+    if not args.no_large and world == 1 and network is not None:
+        from diff_solver_b200.warm_start import WarmStartNetwork
+        f = args.network_factor
+        big = WarmStartNetwork(tuple(s // f for s in LARGE_GRID), factor=f)
+        big.load(args.weights)
+        extra["large_grid"] = large_grid_record(args, big)
+        big.check()
+        del big
+        torch.cuda.empty_cache()
     if network is not None:
         network.check()
-    return results, headline, clocks
+    host_state = None
+    if world == 1 and not args.no_cpu_baseline:
+        from diff_solver_b200.model import tensors_of
+        t = [x.double().cpu().numpy() for x in tensors_of(initial)]
+        host_state = {"density": t[0], "temperature": t[1], "velocity": t[2:5]}
+    return results, headline, clocks, extra, host_state
+
+
+def reference_run(args):
+    """The reference arm: the FP64 oracle's full steps on the host cores, from
+    the spun-up state (generated on the GPU by the library outside the timed
+    region: the CPU cannot roll a 256^3 plume 180 steps in minutes)."""
+    import torch
+    torch.cuda.set_device(0)
+    network = None if args.no_learned else load_network(args, args.shape)
+    saved, spin = spin_up(args.shape, network, args.spinup)
+    from diff_solver_b200.model import tensors_of
+    t = [x.double().cpu().numpy() for x in tensors_of(saved[args.spinup])]
+    del spin, saved
+    host_state = {"density": t[0], "temperature": t[1], "velocity": t[2:5]}
+    return cpu_steps(host_state, args.shape, budget_s=args.cpu_budget, max_steps=min(args.steps, args.cpu_steps))
 
 
 def main():
     ap = argparse.ArgumentParser()
     ap.add_argument("--gpus", type=int, default=1)
-    # the warm-started arms' iteration counts vary from step to step (120-550 at
-    # 256^3): 20 timed steps per arm keep the mean within a few per cent
+    # the warm-started arms' iteration counts vary from step to step: 20
+    # timed steps per arm keep the mean within a few per cent
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=5)
-    ap.add_argument("--spinup", type=int, default=40, help="steps from rest before the arms start")
+    ap.add_argument("--spinup", type=int, default=180, help="steps from rest before the arms start")
     ap.add_argument("--impl", choices=["product", "reference"], default="product")
     ap.add_argument("--grid", default=str(GRID), help="N for N^3, or nx,ny,nz")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-learned", action="store_true", help="plain and history arms only")
+    ap.add_argument("--no-adjoint", action="store_true", help="skip the 40-step VJP record")
+    ap.add_argument("--no-large", action="store_true", help="skip the 512x512x256 record")
+    ap.add_argument("--no-reference-kernels", action="store_true", help="skip the per-kernel timing of the reference's kernels")
+    ap.add_argument("--adjoint-window", type=int, default=40)
+    ap.add_argument("--cpu-steps", type=int, default=3, help="most full FP64 steps the CPU legs time")
+    ap.add_argument("--cpu-budget", type=float, default=150.0, help="seconds after which the CPU legs stop adding steps")
     ap.add_argument("--weights", default=WEIGHTS, help="warm-start network parameters (.npz)")
     ap.add_argument("--coarsening", type=int, default=COARSENING, help="coarse-grid correction factor (0: off)")
-    ap.add_argument("--network-factor", type=int, default=2, help="restriction from the grid to the network's grid (1, 2 or 4)")
+    ap.add_argument("--network-factor", type=int, default=2, help="restriction from the grid to the network's grid (1 or 2)")
     ap.add_argument("--arms", default="", help="comma-separated subset of the arms, headline last (profiling; no roofline "
                                                "or CPU baseline without the plain arm)")
     args = ap.parse_args()
@@ -428,10 +735,12 @@ def main():
         args.warmup = 3
     args.shape = grid_shape(args.grid)
     world, rank, local = init_distributed()
-    n = args.shape[0] * args.shape[1] * args.shape[2]
+    n, faces = counts(args.shape)
     name = "x".join(map(str, args.shape))
-    config = {"workload": f"smoke plume {name} after a {args.spinup}-step spin-up from rest, Jacobi-PCG to rel. residual 1e-6",
-              "grid": list(args.shape), "cells": n, "dt": "0.5 dx", "steps_per_replica": args.steps, "spinup_steps": args.spinup,
+    config = {"workload": f"smoke plume {name}, timed steps {args.spinup + args.warmup}-{args.spinup + args.warmup + args.steps} after "
+                          f"rest (spin-up {args.spinup} steps), Jacobi-PCG to rel. residual 1e-6",
+              "grid": list(args.shape), "cells": n, "faces": faces, "dt": "0.5 dx", "steps_per_replica": args.steps,
+              "spinup_steps": args.spinup,
               "warm_start": f"Galerkin start over the last {HISTORY} solutions"
                             + (f", 6 Jacobi sweeps and a step along the coarse-grid correction (grid coarsened x{args.coarsening}, "
                                f"Jacobi-PCG to 1e-2 from its own two-level start)"
@@ -442,63 +751,79 @@ def main():
               "l2": f"inputs larger than L2 (state {n * 21 * 4 / 1e6:.0f} MB)", "parallelism": f"replicas{world}"}
     if args.impl == "reference":
         if rank == 0:
-            cpu = cpu_sample(args.shape, gpu_iterations=None)
-            line = {"impl": "reference", "metric": METRIC, "value": cpu["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
-                    "warmup": args.warmup, "ms_per_step": 1e3 * cpu["seconds_per_step"], "higher_is_better": True,
+            cpu = reference_run(args)
+            line = {"impl": "reference", "metric": METRIC, "value": cpu["value"], "unit": UNIT, "n_gpus": world, "steps": cpu["steps"],
+                    "warmup": 0, "ms_per_step": 1e3 * cpu["seconds_per_step"], "higher_is_better": True,
                     "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic", "config": config,
                     "cpu_baseline": {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")},
-                    "e2e": {"value": cpu["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+                    "e2e": {"value": cpu["value"], "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+                    "note": "full FP64 steps of the CPU oracle (the reference has no CPU path) from the spun-up state; "
+                            "the state is produced on the GPU before the timed region"}
             print(json.dumps(line), flush=True)
         return
-    results, headline, clocks = product_run(args, world, rank, local)
+    results, headline, clocks, extra, host_state = product_run(args, world, rank, local)
     if rank != 0:
         return
     steps_total = args.steps * world
-    arms = {}
-    for name, r in results.items():
-        arms[name] = {"steps_per_s": steps_total / (r["elapsed_ms"] / 1e3), "ms_per_step": r["elapsed_ms"] / args.steps,
-                      "pcg_iterations_per_step": r["iterations"], "mean_pcg_iterations": statistics.mean(r["iterations"]),
-                      "coarse_iterations_per_step": r["coarse_iterations"],
-                      "refinement_passes_per_step": r["refinements"],
-                      "solve_ms_per_step": statistics.mean(r["solve_ms"]), "initial_residuals": r["initial_residuals"],
-                      "final_residuals": r["residuals"], "gpu_launches": r["launches"]}
-    # whole-step roofline: B_step = 4 (8 N + 8 F) + 40 N k bytes per step (the
-    # scope table's count: fused stages once, 10 floats per cell per CG iteration)
-    nx, ny, nz = args.shape
-    faces = (nx + 1) * ny * nz + nx * (ny + 1) * nz + nx * ny * (nz + 1)
-    peak_gbs, _ = measured_peaks()
-    for name, a in arms.items():
-        b_step = 4.0 * (8 * n + 8 * faces) + 40.0 * n * a["mean_pcg_iterations"]
-        a["step_roofline"] = {"bytes_per_step": b_step, "achieved_gbs": b_step / (a["ms_per_step"] / 1e3) / 1e9,
-                              "frac": b_step / (a["ms_per_step"] / 1e3) / 1e9 / peak_gbs}
+    arms, pcg_roofline = summarize(results, args, args.shape, world, headline)
     h = results[headline]
     value = arms[headline]["steps_per_s"]
-    # roofline of the dominant kernel (the persistent PCG), from the plain arm
-    # where the solve window holds that kernel alone
-    roofline = None
-    if "plain" in results:
-        p = results["plain"]
-        peak, peak_kind = measured_peaks()
-        kbytes_each = [pcg_algorithmic_bytes(n, it, rf) for it, rf in zip(p["iterations"], p["refinements"])]
-        achieved = sum(kbytes_each) / (sum(p["solve_ms"]) / 1e3) / 1e9
-        traffic = None
-        if tuple(args.shape) == (GRID,) * 3:  # the captured workload: its measured traffic per algorithmic byte
-            traffic = PCG_TRAFFIC_PER_ALGORITHMIC_BYTE_256 * statistics.mean(kbytes_each)
-        roofline = {"bound": "hbm", "kernel": "pcg_kernel", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                    "traffic": traffic, "traffic_unit": "bytes per launch", "peak_kind": peak_kind,
-                    "algorithmic_bytes_per_launch": statistics.mean(kbytes_each),
-                    "launch_ms": statistics.mean(p["solve_ms"]), "iterations_per_launch": statistics.mean(p["iterations"]), "arm": "plain"}
+    roofline = pcg_roofline(headline)
+    traffic = None
+    if tuple(args.shape) == (GRID,) * 3:  # the captured workload: its measured traffic per algorithmic byte
+        traffic = PCG_TRAFFIC_PER_ALGORITHMIC_BYTE_256 * roofline["algorithmic_bytes_per_launch"]
+    roofline["traffic"] = traffic
+    roofline["traffic_unit"] = "bytes per launch (the plain-launch ratio of dram bytes to algorithmic bytes, measured by ncu)"
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": h["elapsed_ms"] / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 (FP64 CG reductions and iterate)", "data": "synthetic", "config": config,
             "method": headline, "speedup_vs_plain": value / arms["plain"]["steps_per_s"] if "plain" in arms else None, "arms": arms,
-            "roofline": roofline,
+            "roofline": roofline, "roofline_plain": pcg_roofline("plain") if "plain" in results else None,
             "gpu_launches": h["launches"], "clocks": clocks,
             "e2e": {"value": steps_total / (h["e2e_ms"] / 1e3), "unit": UNIT, "h2d_bytes_per_step": h["h2d"],
                     "d2h_bytes_per_step": h["d2h"]},
             "example_metrics_last_step": [float(v) for v in h["metrics"]]}
-    if world == 1 and not args.no_cpu_baseline and "plain" in arms:
-        cpu = cpu_sample(args.shape, gpu_iterations=int(arms["plain"]["mean_pcg_iterations"]))
+    peak, _ = measured_peaks()
+    if "adjoint" in extra:
+        a = extra.pop("adjoint")
+        n_, f_ = a.pop("_n"), a.pop("_f")
+        fwd_it = statistics.mean(arms[headline]["pcg_iterations_per_step"])
+        adj_it = a["last_adjoint_solve"]["iterations"]
+        b = reverse_step_bytes(n_, f_, fwd_it, adj_it)
+        a["reverse_step_bytes"] = b
+        a["reverse_step_gbs"] = b / (a["ms_per_reverse_step"] / 1e3) / 1e9
+        a["reverse_step_frac"] = a["reverse_step_gbs"] / peak
+        line["adjoint"] = a
+    if "reference_kernels" in extra:
+        rk = extra.pop("reference_kernels")
+        if "unavailable" not in rk:
+            st = arms[headline]["stages"]
+            for k in ("advect_constrain", "scalar_advection", "pressure_rhs", "projection"):
+                rk[k]["product_ms"] = st[k]["ms"]
+                rk[k]["bytes"] = st[k]["bytes"]
+            p = arms[headline]
+            rk["pressure_iteration"]["product_ms"] = st["fine_pcg"]["ms"] / max(p["mean_pcg_iterations"], 1)
+            rk["pressure_iteration"]["product"] = "one Jacobi-PCG iteration of the fine solve (36 B/cell)"
+            for k, r in rk.items():
+                if "bytes" in r and "product_ms" in r:
+                    r["product_gbs"] = r["bytes"] / (r["product_ms"] / 1e3) / 1e9
+                    r["reference_gbs"] = r["bytes"] / (r["reference_ms"] / 1e3) / 1e9
+                if "product_ms" in r and "reference_ms" in r:
+                    r["speedup"] = r["reference_ms"] / r["product_ms"]
+        line["reference_kernels"] = rk
+    if "large_grid" in extra:
+        lg = extra.pop("large_grid")
+        sub = argparse.Namespace(steps=1)
+        rec = {"grid": list(LARGE_GRID), "spinup_steps": 40, "arms": {}}
+        for name, r in lg.items():
+            sub.steps = r.pop("_steps")
+            a_, pr = summarize({name: r}, sub, LARGE_GRID, 1, name)
+            rec["arms"][name] = {k: a_[name][k] for k in ("steps_per_s", "ms_per_step", "mean_pcg_iterations", "pcg_iterations_per_step",
+                                                           "coarse_iterations_per_step", "stages", "step_roofline")}
+            rec["arms"][name]["pcg_roofline"] = pr(name)
+        line["large_grid"] = rec
+    if host_state is not None and "plain" in arms:
+        cpu = cpu_steps(host_state, args.shape, budget_s=30.0, max_steps=1)
         line["cpu_baseline"] = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
     print(json.dumps(line), flush=True)
 

@@ -37,6 +37,10 @@ class XsVector(C.Structure):
 XsAdjointVector = XsVector  # same layout: three pointers
 
 
+class XsVec3(C.Structure):
+    _fields_ = [("x", C.c_float), ("y", C.c_float), ("z", C.c_float)]
+
+
 class XsInflow(C.Structure):
     _fields_ = [("center", C.c_float * 3), ("radius", C.c_float), ("density", C.c_float), ("temperature", C.c_float)]
 
@@ -49,7 +53,7 @@ class XsPressureSolve(C.Structure):
 class XsSolveStats(C.Structure):
     _fields_ = [("iterations", C.c_uint32), ("status", C.c_uint32), ("refinements", C.c_uint32), ("warm_start_used", C.c_uint32),
                 ("rhs_norm", C.c_double), ("initial_residual", C.c_double), ("final_residual", C.c_double),
-                ("guess_scale", C.c_double), ("coarse_iterations", C.c_uint32), ("reserved", C.c_uint32)]
+                ("guess_scale", C.c_double), ("coarse_iterations", C.c_uint32), ("smoothed_iterations", C.c_uint32)]
 
     def as_dict(self):
         return {k: getattr(self, k) for k, _ in self._fields_}
@@ -142,6 +146,8 @@ SIGNATURES = {
                                XsParameters, XsState, _V]),
     "xs_smoke_vjp_step": (_S, [_V, C.POINTER(XsSmokeModel), XsState, XsParameters, XsState, XsStepCache, XsState, XsState,
                                XsControl, XsParameters, _V]),
+    "xs_smoke_write_control": (_S, [_V, _G, C.c_uint64, C.c_float, XsVec3, XsVec3, C.c_float, C.c_float, C.c_float, XsVec3, XsVec3, _V, _V,
+                                     XsVector]),
     "xs_smoke_reduce_metrics": (_S, [_V, C.POINTER(XsSmokeModel), _V, _V, XsVector, XsVector, _V]),
     "xs_smoke_read_solve_stats": (_S, [_V, C.POINTER(XsSmokeModel), _V, C.c_uint32, C.POINTER(XsSolveStats),
                                        C.POINTER(XsSolveStats)]),

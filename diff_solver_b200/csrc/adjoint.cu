@@ -129,8 +129,8 @@ __device__ __forceinline__ void advect_velocity_vjp_face(int a, int x, int y, in
 }
 
 // operators.cu:415-439 for all three components in one launch.
-__global__ void advect_velocity_vjp_kernel(Grid g, uint64_t f0, uint64_t f1, uint64_t f2, const uint32_t* __restrict__ mask, XsVector u,
-                                           XsVelocityBoundary vb, XsAdjointVector oa, XsAdjointVector ua) {
+__global__ void advect_velocity_vjp_kernel(const __grid_constant__ Grid g, uint64_t f0, uint64_t f1, uint64_t f2, const uint32_t* __restrict__ mask, XsVector u,
+                                           const __grid_constant__ XsVelocityBoundary vb, XsAdjointVector oa, XsAdjointVector ua) {
     const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= f0 + f1 + f2) return;
     int a;
@@ -159,15 +159,16 @@ constexpr size_t kScalarVjpSmem = 5 * AdjointTile::kNodes * (sizeof(double) + si
 // through the midpoint to the start (exact start weights).
 template <int A>
 __device__ __forceinline__ void staged_trace_adjoint(const Vec3& mid, const Sample (&m)[3], const Vec3& der, const Vec3& src_gradient,
-                                                     double o, int li, double* const (&acc)[3], const tile::Origin& org, const Grid& g,
-                                                     const XsVelocityBoundary& vb, const XsAdjointVector& ua, bool cell) {
+                                                     double o, int li, double* const (&acc)[3], const tile::Origin& org,
+                                                     const tile::TileConsts& k, const Grid& g, const XsVelocityBoundary& vb,
+                                                     const XsAdjointVector& ua, bool cell) {
     using S = AdjointTile;
     const double v1x = -static_cast<double>(der.x * g.dt * src_gradient.x) * o;
     const double v1y = -static_cast<double>(der.y * g.dt * src_gradient.y) * o;
     const double v1z = -static_cast<double>(der.z * g.dt * src_gradient.z) * o;
-    tile::staged_face_scatter<S, 0>(acc[0], ua.x, mid, v1x, org, g, vb);
-    tile::staged_face_scatter<S, 1>(acc[1], ua.y, mid, v1y, org, g, vb);
-    tile::staged_face_scatter<S, 2>(acc[2], ua.z, mid, v1z, org, g, vb);
+    tile::staged_face_scatter<S, 0>(acc[0], ua.x, mid, v1x, org, k, g, vb);
+    tile::staged_face_scatter<S, 1>(acc[1], ua.y, mid, v1y, org, k, g, vb);
+    tile::staged_face_scatter<S, 2>(acc[2], ua.z, mid, v1z, org, k, g, vb);
     const double mx = m[0].gradient.x * v1x + m[1].gradient.x * v1y + m[2].gradient.x * v1z;
     const double my = m[0].gradient.y * v1x + m[1].gradient.y * v1y + m[2].gradient.y * v1z;
     const double mz = m[0].gradient.z * v1x + m[1].gradient.z * v1y + m[2].gradient.z * v1z;
@@ -186,22 +187,23 @@ __device__ __forceinline__ void staged_trace_adjoint(const Vec3& mid, const Samp
 // Midpoint samples (values and gradients) and the clamped end of the trace
 // from a start with known velocity.
 __device__ __forceinline__ Vec3 staged_trace_with_samples(const tile::StagedVelocity& sv, const Vec3& s, const Vec3& v0, const tile::Origin& org,
-                                                          const Grid& g, const XsVelocityBoundary& vb, Vec3& mid, Sample (&m)[3], Vec3& der) {
+                                                          const tile::TileConsts& k, const Grid& g, const XsVelocityBoundary& vb, Vec3& mid,
+                                                          Sample (&m)[3], Vec3& der) {
     using S = AdjointTile;
     mid = Vec3{s.x - 0.5f * g.dt * v0.x, s.y - 0.5f * g.dt * v0.y, s.z - 0.5f * g.dt * v0.z};
-    m[0] = tile::staged_face<S, 0, true>(sv.s[0], sv.u.x, mid, org, g, vb);
-    m[1] = tile::staged_face<S, 1, true>(sv.s[1], sv.u.y, mid, org, g, vb);
-    m[2] = tile::staged_face<S, 2, true>(sv.s[2], sv.u.z, mid, org, g, vb);
+    m[0] = tile::staged_face<S, 0, true>(sv.s[0], sv.u.x, mid, org, k, g, vb);
+    m[1] = tile::staged_face<S, 1, true>(sv.s[1], sv.u.y, mid, org, k, g, vb);
+    m[2] = tile::staged_face<S, 2, true>(sv.s[2], sv.u.z, mid, org, k, g, vb);
     Vec3 raw{s.x - g.dt * m[0].value, s.y - g.dt * m[1].value, s.z - g.dt * m[2].value};
     der = Vec3{1.0f, 1.0f, 1.0f};
-    tile::clamp_trace(raw, der, g, vb);
+    tile::clamp_trace(raw, der, k);
     return raw;
 }
 
 template <int A>
 __device__ __forceinline__ void advect_velocity_vjp_tile_face(int x, int y, int z, int li, const tile::StagedVelocity& sv,
-                                                              double* const (&acc)[3], const tile::Origin& org, const Grid& g,
-                                                              const XsVelocityBoundary& vb, const XsAdjointVector& oa,
+                                                              double* const (&acc)[3], const tile::Origin& org, const tile::TileConsts& k,
+                                                              const Grid& g, const XsVelocityBoundary& vb, const XsAdjointVector& oa,
                                                               const XsAdjointVector& ua) {
     using S = AdjointTile;
     const double o = component<const double>(oa.x, oa.y, oa.z, A)[tile::index32(x, y, z, extent(g, A, 0), extent(g, A, 1))];
@@ -209,13 +211,13 @@ __device__ __forceinline__ void advect_velocity_vjp_tile_face(int x, int y, int 
     const Vec3 s = face_position(A, x, y, z, g);
     Vec3 mid, der;
     Sample m[3];
-    const Vec3 end = staged_trace_with_samples(sv, s, tile::face_start_velocity<S, A>(sv, li), org, g, vb, mid, m, der);
-    const Sample src = tile::staged_face<S, A, true>(sv.s[A], component<const float>(sv.u.x, sv.u.y, sv.u.z, A), end, org, g, vb);
-    tile::staged_face_scatter<S, A>(acc[A], component<double>(ua.x, ua.y, ua.z, A), end, o, org, g, vb);
-    staged_trace_adjoint<A>(mid, m, der, src.gradient, o, li, acc, org, g, vb, ua, false);
+    const Vec3 end = staged_trace_with_samples(sv, s, tile::face_start_velocity<S, A>(sv, li), org, k, g, vb, mid, m, der);
+    const Sample src = tile::staged_face<S, A, true>(sv.s[A], component<const float>(sv.u.x, sv.u.y, sv.u.z, A), end, org, k, g, vb);
+    tile::staged_face_scatter<S, A>(acc[A], component<double>(ua.x, ua.y, ua.z, A), end, o, org, k, g, vb);
+    staged_trace_adjoint<A>(mid, m, der, src.gradient, o, li, acc, org, k, g, vb, ua, false);
 }
 
-__global__ void __launch_bounds__(AdjointTile::kThreads, 2) advect_velocity_vjp_tile_kernel(Grid g, XsVector u, XsVelocityBoundary vb,
+__global__ void __launch_bounds__(AdjointTile::kThreads, 2) advect_velocity_vjp_tile_kernel(const __grid_constant__ Grid g, XsVector u, const __grid_constant__ XsVelocityBoundary vb,
                                                                                           XsAdjointVector oa, XsAdjointVector ua) {
     using S = AdjointTile;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -232,6 +234,7 @@ __global__ void __launch_bounds__(AdjointTile::kThreads, 2) advect_velocity_vjp_
     tile::stage_wait();
     __syncthreads();
     const tile::StagedVelocity sv{{box, box + S::kNodes, box + 2 * S::kNodes}, u};
+    const tile::TileConsts k = tile::tile_consts(g, vb);
     const int x = static_cast<int>(blockIdx.x) * S::TX + static_cast<int>(threadIdx.x);
     const int y = static_cast<int>(blockIdx.y) * S::TY + static_cast<int>(threadIdx.y);
     if (x < g.nx && y < g.ny) {
@@ -240,9 +243,9 @@ __global__ void __launch_bounds__(AdjointTile::kThreads, 2) advect_velocity_vjp_
             const int z = static_cast<int>(blockIdx.z) * S::TZ + kz;
             if (z >= g.nz) break;
             const int li = tile::local_index<S>(kz);
-            advect_velocity_vjp_tile_face<0>(x, y, z, li, sv, acc, org, g, vb, oa, ua);
-            advect_velocity_vjp_tile_face<1>(x, y, z, li, sv, acc, org, g, vb, oa, ua);
-            advect_velocity_vjp_tile_face<2>(x, y, z, li, sv, acc, org, g, vb, oa, ua);
+            advect_velocity_vjp_tile_face<0>(x, y, z, li, sv, acc, org, k, g, vb, oa, ua);
+            advect_velocity_vjp_tile_face<1>(x, y, z, li, sv, acc, org, k, g, vb, oa, ua);
+            advect_velocity_vjp_tile_face<2>(x, y, z, li, sv, acc, org, k, g, vb, oa, ua);
         }
     }
     __syncthreads();
@@ -252,7 +255,7 @@ __global__ void __launch_bounds__(AdjointTile::kThreads, 2) advect_velocity_vjp_
 }
 
 // The faces at the upper end of their own axis, general form.
-__global__ void advect_velocity_vjp_upper_kernel(Grid g, const uint32_t* __restrict__ mask, XsVector u, XsVelocityBoundary vb,
+__global__ void advect_velocity_vjp_upper_kernel(const __grid_constant__ Grid g, const uint32_t* __restrict__ mask, XsVector u, const __grid_constant__ XsVelocityBoundary vb,
                                                  XsAdjointVector oa, XsAdjointVector ua) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t sx = static_cast<uint32_t>(g.ny) * g.nz, sy = static_cast<uint32_t>(g.nx) * g.nz, sz = static_cast<uint32_t>(g.nx) * g.ny;
@@ -276,12 +279,12 @@ __global__ void advect_velocity_vjp_upper_kernel(Grid g, const uint32_t* __restr
 // Density and temperature together (operators.cu:537-561 twice on one
 // trace): u and both sources staged, the velocity and both source adjoints
 // accumulated in the box.
-__global__ void __launch_bounds__(AdjointTile::kThreads, 1) advect_scalar_vjp_tile_kernel(Grid g, const float* __restrict__ src,
-                                                                                        XsScalarBoundary sb, const double* __restrict__ oa,
+__global__ void __launch_bounds__(AdjointTile::kThreads, 1) advect_scalar_vjp_tile_kernel(const __grid_constant__ Grid g, const float* __restrict__ src,
+                                                                                        const __grid_constant__ XsScalarBoundary sb, const double* __restrict__ oa,
                                                                                         double* __restrict__ sa, const float* __restrict__ src2,
-                                                                                        XsScalarBoundary sb2, const double* __restrict__ oa2,
+                                                                                        const __grid_constant__ XsScalarBoundary sb2, const double* __restrict__ oa2,
                                                                                         double* __restrict__ sa2, XsVector u,
-                                                                                        XsVelocityBoundary vb, XsAdjointVector ua) {
+                                                                                        const __grid_constant__ XsVelocityBoundary vb, XsAdjointVector ua) {
     using S = AdjointTile;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double* const acc[3] = {reinterpret_cast<double*>(smem_raw), reinterpret_cast<double*>(smem_raw) + S::kNodes,
@@ -299,6 +302,7 @@ __global__ void __launch_bounds__(AdjointTile::kThreads, 1) advect_scalar_vjp_ti
     tile::stage_wait();
     __syncthreads();
     const tile::StagedVelocity sv{{box, box + S::kNodes, box + 2 * S::kNodes}, u};
+    const tile::TileConsts k = tile::tile_consts(g, vb);
     const int x = static_cast<int>(blockIdx.x) * S::TX + static_cast<int>(threadIdx.x);
     const int y = static_cast<int>(blockIdx.y) * S::TY + static_cast<int>(threadIdx.y);
     if (x < g.nx && y < g.ny) {
@@ -314,14 +318,14 @@ __global__ void __launch_bounds__(AdjointTile::kThreads, 1) advect_scalar_vjp_ti
             const Vec3 s = cell_position(x, y, z, g);
             Vec3 mid, der;
             Sample m[3];
-            const Vec3 end = staged_trace_with_samples(sv, s, tile::cell_start_velocity<S>(sv, li), org, g, vb, mid, m, der);
-            const Sample smp = tile::staged_scalar<S, true>(box + 3 * S::kNodes, src, end, org, g, sb);
-            tile::staged_scalar_scatter<S>(sacc[0], sa, end, o1, org, g, sb);
-            if (o1 != 0.0) staged_trace_adjoint<0>(mid, m, der, smp.gradient, o1, li, acc, org, g, vb, ua, true);
+            const Vec3 end = staged_trace_with_samples(sv, s, tile::cell_start_velocity<S>(sv, li), org, k, g, vb, mid, m, der);
+            const Sample smp = tile::staged_scalar<S, true>(box + 3 * S::kNodes, src, end, org, k, g, sb);
+            tile::staged_scalar_scatter<S>(sacc[0], sa, end, o1, org, k, g, sb);
+            if (o1 != 0.0) staged_trace_adjoint<0>(mid, m, der, smp.gradient, o1, li, acc, org, k, g, vb, ua, true);
             if (two && o2 != 0.0) {
-                const Sample smp2 = tile::staged_scalar<S, true>(box + 4 * S::kNodes, src2, end, org, g, sb2);
-                tile::staged_scalar_scatter<S>(sacc[1], sa2, end, o2, org, g, sb2);
-                staged_trace_adjoint<0>(mid, m, der, smp2.gradient, o2, li, acc, org, g, vb, ua, true);
+                const Sample smp2 = tile::staged_scalar<S, true>(box + 4 * S::kNodes, src2, end, org, k, g, sb2);
+                tile::staged_scalar_scatter<S>(sacc[1], sa2, end, o2, org, k, g, sb2);
+                staged_trace_adjoint<0>(mid, m, der, smp2.gradient, o2, li, acc, org, k, g, vb, ua, true);
             }
         }
     }
@@ -335,10 +339,10 @@ __global__ void __launch_bounds__(AdjointTile::kThreads, 1) advect_scalar_vjp_ti
 
 // operators.cu:537-561; density and temperature share one trace when both
 // adjoints are requested (sa2/oa2 non-null).
-__global__ void advect_scalar_vjp_kernel(Grid g, const uint32_t* __restrict__ mask, const float* __restrict__ src, XsScalarBoundary sb,
+__global__ void advect_scalar_vjp_kernel(const __grid_constant__ Grid g, const uint32_t* __restrict__ mask, const float* __restrict__ src, const __grid_constant__ XsScalarBoundary sb,
                                          const double* __restrict__ oa, double* __restrict__ sa, const float* __restrict__ src2,
-                                         XsScalarBoundary sb2, const double* __restrict__ oa2, double* __restrict__ sa2, XsVector u,
-                                         XsVelocityBoundary vb, XsAdjointVector ua) {
+                                         const __grid_constant__ XsScalarBoundary sb2, const double* __restrict__ oa2, double* __restrict__ sa2, XsVector u,
+                                         const __grid_constant__ XsVelocityBoundary vb, XsAdjointVector ua) {
     const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= cell_count(g) || is_solid(mask, i)) return;
     const double o1 = oa[i];

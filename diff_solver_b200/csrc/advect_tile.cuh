@@ -83,28 +83,31 @@ __device__ __forceinline__ void cp_async4(float* dst, const float* src) {
 __device__ __forceinline__ void stage_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // Stages face component A over the box: one warp per box row (x-contiguous,
-// coalesced), two passes for the row's SX nodes.  The caller runs
-// stage_wait() and __syncthreads() before reading the box.
+// coalesced), two passes for the row's SX nodes.  Nodes inside the array are
+// copied asynchronously; only nodes beyond the domain edge take the
+// boundary rules (a box that crosses the edge keeps the fast copy for the
+// rest of its nodes).  The caller runs stage_wait() and __syncthreads()
+// before reading the box.
 template <class S, int A>
 __device__ __forceinline__ void stage_face(float* __restrict__ s, const float* __restrict__ v, const Origin& o, const Grid& g,
                                            const XsVelocityBoundary& b) {
     const int ex = extent(g, A, 0), ey = extent(g, A, 1), ez = extent(g, A, 2);
     const int lane = threadIdx.x, warp = threadIdx.y;
-    if (box_inside<S>(o, ex, ey, ez)) {
 #pragma unroll
-        for (int r = 0; r < S::kRows / S::TY; ++r) {
-            const int row = warp + r * S::TY;
-            const float* src = v + index32(o.x, o.y + row % S::SY, o.z + row / S::SY, ex, ey);
-            float* dst = s + row * S::SX;
-            cp_async4(dst + lane, src + lane);
-            if (lane < S::SX - 32) cp_async4(dst + 32 + lane, src + 32 + lane);
-        }
-    } else {
-        for (int row = warp; row < S::kRows; row += S::TY) {
-            const int y = o.y + row % S::SY, z = o.z + row / S::SY;
-            float* dst = s + row * S::SX;
-            dst[lane] = load_face(v, A, o.x + lane, y, z, g, b);
-            if (lane < S::SX - 32) dst[32 + lane] = load_face(v, A, o.x + 32 + lane, y, z, g, b);
+    for (int r = 0; r < S::kRows / S::TY; ++r) {
+        const int row = warp + r * S::TY;
+        const int y = o.y + row % S::SY, z = o.z + row / S::SY;
+        const bool row_in = static_cast<unsigned>(y) < static_cast<unsigned>(ey) && static_cast<unsigned>(z) < static_cast<unsigned>(ez);
+        float* dst = s + row * S::SX;
+#pragma unroll
+        for (int half = 0; half < 2; ++half) {
+            const int lx = lane + 32 * half;
+            if (half == 1 && lx >= S::SX) break;
+            const int x = o.x + lx;
+            if (row_in && static_cast<unsigned>(x) < static_cast<unsigned>(ex))
+                cp_async4(dst + lx, v + index32(x, y, z, ex, ey));
+            else
+                dst[lx] = load_face(v, A, x, y, z, g, b);
         }
     }
 }
@@ -114,21 +117,21 @@ template <class S>
 __device__ __forceinline__ void stage_cells(float* __restrict__ s, const float* __restrict__ v, const Origin& o, const Grid& g,
                                             const XsScalarBoundary& b) {
     const int lane = threadIdx.x, warp = threadIdx.y;
-    if (box_inside<S>(o, g.nx, g.ny, g.nz)) {
 #pragma unroll
-        for (int r = 0; r < S::kRows / S::TY; ++r) {
-            const int row = warp + r * S::TY;
-            const float* src = v + index32(o.x, o.y + row % S::SY, o.z + row / S::SY, g.nx, g.ny);
-            float* dst = s + row * S::SX;
-            cp_async4(dst + lane, src + lane);
-            if (lane < S::SX - 32) cp_async4(dst + 32 + lane, src + 32 + lane);
-        }
-    } else {
-        for (int row = warp; row < S::kRows; row += S::TY) {
-            const int y = o.y + row % S::SY, z = o.z + row / S::SY;
-            float* dst = s + row * S::SX;
-            dst[lane] = load_scalar(v, o.x + lane, y, z, g, b);
-            if (lane < S::SX - 32) dst[32 + lane] = load_scalar(v, o.x + 32 + lane, y, z, g, b);
+    for (int r = 0; r < S::kRows / S::TY; ++r) {
+        const int row = warp + r * S::TY;
+        const int y = o.y + row % S::SY, z = o.z + row / S::SY;
+        const bool row_in = static_cast<unsigned>(y) < static_cast<unsigned>(g.ny) && static_cast<unsigned>(z) < static_cast<unsigned>(g.nz);
+        float* dst = s + row * S::SX;
+#pragma unroll
+        for (int half = 0; half < 2; ++half) {
+            const int lx = lane + 32 * half;
+            if (half == 1 && lx >= S::SX) break;
+            const int x = o.x + lx;
+            if (row_in && static_cast<unsigned>(x) < static_cast<unsigned>(g.nx))
+                cp_async4(dst + lx, v + index32(x, y, z, g.nx, g.ny));
+            else
+                dst[lx] = load_scalar(v, x, y, z, g, b);
         }
     }
 }
@@ -156,24 +159,37 @@ __device__ __forceinline__ int box_corner(int x0, int y0, int z0, const Origin& 
 }
 
 // Stencils that leave the box: sample_face's own global-memory path, out
-// of line (the whole sample returned by value keeps the box stencil of the
-// common path in registers).
-static __device__ __noinline__ Sample global_face_sample(const float* __restrict__ v, int axis, const Vec3& p, const Grid& g,
+// of line.  The tile kernels declare their grid and boundary parameters
+// __grid_constant__: a kernel parameter passed out of line by reference
+// would otherwise be copied to local memory, and every use of it on the
+// common path would read that copy.
+static __device__ __noinline__ Sample global_face_sample(const float* __restrict__ v, int axis, Vec3 p, const Grid& g,
                                                          const XsVelocityBoundary& b) {
     return sample_face<true>(v, axis, p, g, b);
 }
 
-static __device__ __noinline__ Sample global_scalar_sample(const float* __restrict__ v, const Vec3& p, const Grid& g, const XsScalarBoundary& b) {
+static __device__ __noinline__ Sample global_scalar_sample(const float* __restrict__ v, Vec3 p, const Grid& g, const XsScalarBoundary& b) {
     return sample_scalar<true>(v, p, g, b);
+}
+
+// Per-thread constants of the tile kernels (power-of-two spacing).
+struct TileConsts {
+    float r;           // 1 / h, exact
+    Vec3 extent;       // n h per axis (the trace's clamp)
+    bool periodic[3];
+};
+
+__device__ __forceinline__ TileConsts tile_consts(const Grid& g, const XsVelocityBoundary& b) {
+    return TileConsts{1.0f / g.h, Vec3{g.nx * g.h, g.ny * g.h, g.nz * g.h}, {periodic(b, 0), periodic(b, 1), periodic(b, 2)}};
 }
 
 // sample_face<kGradient> (operators.cu:166-194) of face component A with the
 // stencil read from its staged box.
 template <class S, int A, bool kGradient>
 __device__ __forceinline__ Sample staged_face(const float* __restrict__ s, const float* __restrict__ v, const Vec3& p, const Origin& o,
-                                              const Grid& g, const XsVelocityBoundary& b) {
+                                              const TileConsts& k, const Grid& g, const XsVelocityBoundary& b) {
     float gx, gy, gz;
-    grid_coordinates(p, g.h, A, gx, gy, gz);
+    grid_coordinates_pow2(p, k.r, A, gx, gy, gz);
     const int x0 = static_cast<int>(floorf(gx)), y0 = static_cast<int>(floorf(gy)), z0 = static_cast<int>(floorf(gz));
     const int c = box_corner<S>(x0, y0, z0, o);
     Sample r;
@@ -191,9 +207,9 @@ __device__ __forceinline__ Sample staged_face(const float* __restrict__ s, const
 // sample_scalar<kGradient> (operators.cu:136-164) from a staged box.
 template <class S, bool kGradient>
 __device__ __forceinline__ Sample staged_scalar(const float* __restrict__ s, const float* __restrict__ v, const Vec3& p, const Origin& o,
-                                                const Grid& g, const XsScalarBoundary& b) {
+                                                const TileConsts& k, const Grid& g, const XsScalarBoundary& b) {
     float gx, gy, gz;
-    grid_coordinates(p, g.h, -1, gx, gy, gz);
+    grid_coordinates_pow2(p, k.r, -1, gx, gy, gz);
     const int x0 = static_cast<int>(floorf(gx)), y0 = static_cast<int>(floorf(gy)), z0 = static_cast<int>(floorf(gz));
     const int c = box_corner<S>(x0, y0, z0, o);
     Sample r;
@@ -217,10 +233,10 @@ struct StagedVelocity {
 // sample_velocity (operators.cu:242-244) from the boxes, values or samples
 // with gradients.
 template <class S>
-__device__ __forceinline__ Vec3 staged_velocity(const StagedVelocity& sv, const Vec3& p, const Origin& o, const Grid& g,
+__device__ __forceinline__ Vec3 staged_velocity(const StagedVelocity& sv, const Vec3& p, const Origin& o, const TileConsts& k, const Grid& g,
                                                 const XsVelocityBoundary& b) {
-    return Vec3{staged_face<S, 0, false>(sv.s[0], sv.u.x, p, o, g, b).value, staged_face<S, 1, false>(sv.s[1], sv.u.y, p, o, g, b).value,
-                staged_face<S, 2, false>(sv.s[2], sv.u.z, p, o, g, b).value};
+    return Vec3{staged_face<S, 0, false>(sv.s[0], sv.u.x, p, o, k, g, b).value, staged_face<S, 1, false>(sv.s[1], sv.u.y, p, o, k, g, b).value,
+                staged_face<S, 2, false>(sv.s[2], sv.u.z, p, o, k, g, b).value};
 }
 
 // Velocity at the position of face A (integer coordinates at box offset li)
@@ -261,24 +277,30 @@ __device__ __forceinline__ Vec3 cell_start_velocity(const StagedVelocity& sv, in
 }
 
 // The clamp of trace_rk2 (operators.cu:268-270): non-periodic axes clamp to
-// the domain and zero that axis' derivative.
-__device__ __forceinline__ void clamp_trace(Vec3& raw, Vec3& der, const Grid& g, const XsVelocityBoundary& b) {
-    const Vec3 mx{g.nx * g.h, g.ny * g.h, g.nz * g.h};
-    if (!periodic(b, 0) && (raw.x < 0.0f || raw.x > mx.x)) { raw.x = fminf(fmaxf(raw.x, 0.0f), mx.x); der.x = 0.0f; }
-    if (!periodic(b, 1) && (raw.y < 0.0f || raw.y > mx.y)) { raw.y = fminf(fmaxf(raw.y, 0.0f), mx.y); der.y = 0.0f; }
-    if (!periodic(b, 2) && (raw.z < 0.0f || raw.z > mx.z)) { raw.z = fminf(fmaxf(raw.z, 0.0f), mx.z); der.z = 0.0f; }
+// the domain and zero that axis' derivative.  Branch-free: inside the domain
+// the clamp returns the coordinate itself.
+__device__ __forceinline__ float clamp_axis(float v, float hi, bool per, float& der) {
+    const bool out = !per && (v < 0.0f || v > hi);
+    der = out ? 0.0f : der;
+    return per ? v : fminf(fmaxf(v, 0.0f), hi);
+}
+
+__device__ __forceinline__ void clamp_trace(Vec3& raw, Vec3& der, const TileConsts& k) {
+    raw.x = clamp_axis(raw.x, k.extent.x, k.periodic[0], der.x);
+    raw.y = clamp_axis(raw.y, k.extent.y, k.periodic[1], der.y);
+    raw.z = clamp_axis(raw.z, k.extent.z, k.periodic[2], der.z);
 }
 
 // trace_rk2 (operators.cu:256-276) from the boxes for a domain without
 // colliders (no bisection), given the velocity at the start.
 template <class S>
-__device__ __forceinline__ Vec3 staged_trace(const StagedVelocity& sv, const Vec3& s, const Vec3& v0, const Origin& o, const Grid& g,
-                                             const XsVelocityBoundary& b) {
+__device__ __forceinline__ Vec3 staged_trace(const StagedVelocity& sv, const Vec3& s, const Vec3& v0, const Origin& o, const TileConsts& k,
+                                             const Grid& g, const XsVelocityBoundary& b) {
     const Vec3 mid{s.x - 0.5f * g.dt * v0.x, s.y - 0.5f * g.dt * v0.y, s.z - 0.5f * g.dt * v0.z};
-    const Vec3 v1 = staged_velocity<S>(sv, mid, o, g, b);
+    const Vec3 v1 = staged_velocity<S>(sv, mid, o, k, g, b);
     Vec3 raw{s.x - g.dt * v1.x, s.y - g.dt * v1.y, s.z - g.dt * v1.z};
     Vec3 der{1.0f, 1.0f, 1.0f};
-    clamp_trace(raw, der, g, b);
+    clamp_trace(raw, der, k);
     return raw;
 }
 
@@ -286,12 +308,11 @@ __device__ __forceinline__ Vec3 staged_trace(const StagedVelocity& sv, const Vec
 // scatter_face (operators.cu:217-240) of one trilinear stencil into the FP64
 // box of component B: the same products adj * wx * wy * wz; stencils outside
 // the box go to global memory directly (with the reference's rules).
-static __device__ __noinline__ void global_face_scatter(double* __restrict__ v, int axis, const Vec3& p, double adj, const Grid& g,
+static __device__ __noinline__ void global_face_scatter(double* __restrict__ v, int axis, Vec3 p, double adj, const Grid& g,
                                                         const XsVelocityBoundary& b) {
     scatter_face(v, axis, p, adj, g, b);
 }
-static __device__ __noinline__ void global_scalar_scatter(double* __restrict__ v, const Vec3& p, double adj, const Grid& g,
-                                                          const XsScalarBoundary& b) {
+static __device__ __noinline__ void global_scalar_scatter(double* __restrict__ v, Vec3 p, double adj, const Grid& g, const XsScalarBoundary& b) {
     scatter_scalar(v, p, adj, g, b);
 }
 
@@ -310,10 +331,10 @@ __device__ __forceinline__ void box_scatter(double* __restrict__ acc, int c, dou
 
 template <class S, int B>
 __device__ __forceinline__ void staged_face_scatter(double* __restrict__ acc, double* __restrict__ v, const Vec3& p, double adj, const Origin& o,
-                                                    const Grid& g, const XsVelocityBoundary& b) {
+                                                    const TileConsts& k, const Grid& g, const XsVelocityBoundary& b) {
     if (adj == 0.0) return;
     float gx, gy, gz;
-    grid_coordinates(p, g.h, B, gx, gy, gz);
+    grid_coordinates_pow2(p, k.r, B, gx, gy, gz);
     const int x0 = static_cast<int>(floorf(gx)), y0 = static_cast<int>(floorf(gy)), z0 = static_cast<int>(floorf(gz));
     const int c = box_corner<S>(x0, y0, z0, o);
     if (c >= 0)
@@ -324,10 +345,10 @@ __device__ __forceinline__ void staged_face_scatter(double* __restrict__ acc, do
 
 template <class S>
 __device__ __forceinline__ void staged_scalar_scatter(double* __restrict__ acc, double* __restrict__ v, const Vec3& p, double adj, const Origin& o,
-                                                      const Grid& g, const XsScalarBoundary& b) {
+                                                      const TileConsts& k, const Grid& g, const XsScalarBoundary& b) {
     if (adj == 0.0) return;
     float gx, gy, gz;
-    grid_coordinates(p, g.h, -1, gx, gy, gz);
+    grid_coordinates_pow2(p, k.r, -1, gx, gy, gz);
     const int x0 = static_cast<int>(floorf(gx)), y0 = static_cast<int>(floorf(gy)), z0 = static_cast<int>(floorf(gz));
     const int c = box_corner<S>(x0, y0, z0, o);
     if (c >= 0)

@@ -205,18 +205,21 @@ __device__ __forceinline__ Sample trilinear(const float v[2][2][2], float tx, fl
 // one multiply instead of a division sequence (the advection kernels issue
 // 21 of these per face and are instruction-issue bound).  Other spacings
 // divide.
+// With the exact reciprocal r = 1/h of a power-of-two spacing given (the
+// tile kernels compute it once per thread):
+__device__ __forceinline__ void grid_coordinates_pow2(const Vec3& p, float r, int axis, float& gx, float& gy, float& gz) {
+    const float x = p.x * r, y = p.y * r, z = p.z * r;
+    gx = x - (axis == 0 ? 0.0f : 0.5f);
+    gy = y - (axis == 1 ? 0.0f : 0.5f);
+    gz = z - (axis == 2 ? 0.0f : 0.5f);
+}
+
 __device__ __forceinline__ void grid_coordinates(const Vec3& p, float h, int axis, float& gx, float& gy, float& gz) {
-    float x, y, z;
     if ((__float_as_uint(h) & 0x007FFFFFu) == 0u) {
-        const float r = 1.0f / h;
-        x = p.x * r;
-        y = p.y * r;
-        z = p.z * r;
-    } else {
-        x = p.x / h;
-        y = p.y / h;
-        z = p.z / h;
+        grid_coordinates_pow2(p, 1.0f / h, axis, gx, gy, gz);
+        return;
     }
+    const float x = p.x / h, y = p.y / h, z = p.z / h;
     gx = x - (axis == 0 ? 0.0f : 0.5f);
     gy = y - (axis == 1 ? 0.0f : 0.5f);
     gz = z - (axis == 2 ? 0.0f : 0.5f);
@@ -251,7 +254,10 @@ __device__ __forceinline__ void load_stencil(const float* __restrict__ v, int x0
 // gather loops of the advection kernels fit the instruction cache (inlined
 // eight times per sample they made the kernels instruction-fetch bound).
 // They return the whole sample by value: a stencil array passed out of line
-// by reference would live in local memory on the interior path as well.
+// by reference would live in local memory on the interior path as well.  The
+// kernels that reach them declare their grid and boundary parameters
+// __grid_constant__, so the references here point into the parameter bank
+// instead of forcing a local copy of those structs.
 static __device__ __noinline__ Sample edge_scalar_sample(const float* __restrict__ v, int x0, int y0, int z0, float tx, float ty, float tz,
                                                          const Grid& g, const XsScalarBoundary& b) {
     float v8[2][2][2];

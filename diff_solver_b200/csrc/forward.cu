@@ -154,7 +154,7 @@ __device__ __forceinline__ float advect_face(int a, int x, int y, int z, const G
     return sample_face<false>(component<const float>(u.x, u.y, u.z, a), a, t.position, g, b).value;
 }
 
-__global__ void advect_velocity_kernel(Grid g, FaceSpace fs, const uint32_t* __restrict__ mask, XsVector u, XsVelocityBoundary b,
+__global__ void advect_velocity_kernel(const __grid_constant__ Grid g, FaceSpace fs, const uint32_t* __restrict__ mask, XsVector u, const __grid_constant__ XsVelocityBoundary b,
                                        XsVector out) {
     const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= fs.total()) return;
@@ -217,8 +217,8 @@ __device__ __forceinline__ float advect_constrain_face(int a, int x, int y, int 
 // General form (colliders, any spacing), one thread per face.  Latency-bound
 // on its ~56 L1 gathers per face: the launch bounds trade a few registers for
 // a fourth resident block per SM.
-__global__ void __launch_bounds__(kBlock, 4) advect_constrain_kernel(Grid g, FaceSpace fs, const uint32_t* __restrict__ mask, XsVector col, XsVector u,
-                                        XsVelocityBoundary b, XsVector out) {
+__global__ void __launch_bounds__(kBlock, 4) advect_constrain_kernel(const __grid_constant__ Grid g, FaceSpace fs, const uint32_t* __restrict__ mask, XsVector col, XsVector u,
+                                        const __grid_constant__ XsVelocityBoundary b, XsVector out) {
     const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= fs.total()) return;
     uint64_t local;
@@ -239,13 +239,14 @@ using ForwardTile = tile::Shape<32, 8, 4>;
 
 template <int A, bool kConstrain>
 __device__ __forceinline__ void advect_constrain_tile_face(int x, int y, int z, int li, const tile::StagedVelocity& sv, const tile::Origin& o,
-                                                           const Grid& g, const XsVelocityBoundary& b, float* __restrict__ out) {
+                                                           const tile::TileConsts& k, const Grid& g, const XsVelocityBoundary& b,
+                                                           float* __restrict__ out) {
     using S = ForwardTile;
     float v;
     if (!kConstrain || !constrained_boundary(A, x, y, z, g, b, v)) {
         const Vec3 s = face_position(A, x, y, z, g);
-        const Vec3 p = tile::staged_trace<S>(sv, s, tile::face_start_velocity<S, A>(sv, li), o, g, b);
-        v = tile::staged_face<S, A, false>(sv.s[A], component<const float>(sv.u.x, sv.u.y, sv.u.z, A), p, o, g, b).value;
+        const Vec3 p = tile::staged_trace<S>(sv, s, tile::face_start_velocity<S, A>(sv, li), o, k, g, b);
+        v = tile::staged_face<S, A, false>(sv.s[A], component<const float>(sv.u.x, sv.u.y, sv.u.z, A), p, o, k, g, b).value;
     }
     const uint32_t ex = static_cast<uint32_t>(extent(g, A, 0)), ey = static_cast<uint32_t>(extent(g, A, 1));
     out[static_cast<uint32_t>(x) + ex * (static_cast<uint32_t>(y) + ey * static_cast<uint32_t>(z))] = v;
@@ -253,7 +254,7 @@ __device__ __forceinline__ void advect_constrain_tile_face(int x, int y, int z, 
 
 // kConstrain = false: the raw advected field of advect_velocity_kernel.
 template <bool kConstrain>
-__global__ void __launch_bounds__(ForwardTile::kThreads, 4) advect_constrain_tile_kernel(Grid g, XsVector u, XsVelocityBoundary b, XsVector out) {
+__global__ void __launch_bounds__(ForwardTile::kThreads, 4) advect_constrain_tile_kernel(const __grid_constant__ Grid g, XsVector u, const __grid_constant__ XsVelocityBoundary b, XsVector out) {
     using S = ForwardTile;
     __shared__ float box[3][S::kNodes];
     const tile::Origin o = tile::tile_origin<S>();
@@ -263,6 +264,7 @@ __global__ void __launch_bounds__(ForwardTile::kThreads, 4) advect_constrain_til
     tile::stage_wait();
     __syncthreads();
     const tile::StagedVelocity sv{{box[0], box[1], box[2]}, u};
+    const tile::TileConsts k = tile::tile_consts(g, b);
     const int x = static_cast<int>(blockIdx.x) * S::TX + static_cast<int>(threadIdx.x);
     const int y = static_cast<int>(blockIdx.y) * S::TY + static_cast<int>(threadIdx.y);
     if (x >= g.nx || y >= g.ny) return;
@@ -271,16 +273,16 @@ __global__ void __launch_bounds__(ForwardTile::kThreads, 4) advect_constrain_til
         const int z = static_cast<int>(blockIdx.z) * S::TZ + kz;
         if (z >= g.nz) break;
         const int li = tile::local_index<S>(kz);
-        advect_constrain_tile_face<0, kConstrain>(x, y, z, li, sv, o, g, b, out.x);
-        advect_constrain_tile_face<1, kConstrain>(x, y, z, li, sv, o, g, b, out.y);
-        advect_constrain_tile_face<2, kConstrain>(x, y, z, li, sv, o, g, b, out.z);
+        advect_constrain_tile_face<0, kConstrain>(x, y, z, li, sv, o, k, g, b, out.x);
+        advect_constrain_tile_face<1, kConstrain>(x, y, z, li, sv, o, k, g, b, out.y);
+        advect_constrain_tile_face<2, kConstrain>(x, y, z, li, sv, o, k, g, b, out.z);
     }
 }
 
 // The faces at the upper end of their own axis (ny nz + nx nz + nx ny of
 // them), general form.
 template <bool kConstrain>
-__global__ void advect_constrain_upper_kernel(Grid g, const uint32_t* __restrict__ mask, XsVector col, XsVector u, XsVelocityBoundary b,
+__global__ void advect_constrain_upper_kernel(const __grid_constant__ Grid g, const uint32_t* __restrict__ mask, XsVector col, XsVector u, const __grid_constant__ XsVelocityBoundary b,
                                               XsVector out) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t sx = static_cast<uint32_t>(g.ny) * g.nz, sy = static_cast<uint32_t>(g.nx) * g.nz, sz = static_cast<uint32_t>(g.nx) * g.ny;
@@ -314,8 +316,8 @@ XsStatus launch_advect_tiled(cudaStream_t st, const Grid& g, const XsVector& col
 }
 
 // operators.cu:499-507
-__global__ void advect_scalar_kernel(Grid g, const uint32_t* __restrict__ mask, const float* __restrict__ collider,
-                                     const float* __restrict__ src, XsVector u, XsScalarBoundary sb, XsVelocityBoundary vb,
+__global__ void advect_scalar_kernel(const __grid_constant__ Grid g, const uint32_t* __restrict__ mask, const float* __restrict__ collider,
+                                     const float* __restrict__ src, XsVector u, const __grid_constant__ XsScalarBoundary sb, const __grid_constant__ XsVelocityBoundary vb,
                                      float* __restrict__ out) {
     const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= cell_count(g)) return;
@@ -328,10 +330,10 @@ __global__ void advect_scalar_kernel(Grid g, const uint32_t* __restrict__ mask, 
 
 // Density and temperature advected along one shared trace (the reference
 // traces twice, model.cpp:347-348).
-__global__ void __launch_bounds__(kBlock, 5) advect_scalar_pair_kernel(Grid g, const uint32_t* __restrict__ mask, const float* __restrict__ col_rho,
+__global__ void __launch_bounds__(kBlock, 4) advect_scalar_pair_kernel(const __grid_constant__ Grid g, const uint32_t* __restrict__ mask, const float* __restrict__ col_rho,
                                           const float* __restrict__ col_temp, const float* __restrict__ src_rho,
-                                          const float* __restrict__ src_temp, XsVector u, XsScalarBoundary rb,
-                                          XsScalarBoundary tb, XsVelocityBoundary vb, float* __restrict__ out_rho,
+                                          const float* __restrict__ src_temp, XsVector u, const __grid_constant__ XsScalarBoundary rb,
+                                          const __grid_constant__ XsScalarBoundary tb, const __grid_constant__ XsVelocityBoundary vb, float* __restrict__ out_rho,
                                           float* __restrict__ out_temp) {
     const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= cell_count(g)) return;
@@ -355,10 +357,10 @@ __global__ void __launch_bounds__(kBlock, 5) advect_scalar_pair_kernel(Grid g, c
 constexpr size_t scalar_tile_smem(int fields) { return (3 + fields) * sizeof(float) * ForwardTile::kNodes; }
 
 template <int kFields>
-__global__ void __launch_bounds__(ForwardTile::kThreads, 3) advect_scalar_pair_tile_kernel(Grid g, const float* __restrict__ src_rho,
+__global__ void __launch_bounds__(ForwardTile::kThreads, 3) advect_scalar_pair_tile_kernel(const __grid_constant__ Grid g, const float* __restrict__ src_rho,
                                                                                       const float* __restrict__ src_temp, XsVector u,
-                                                                                      XsScalarBoundary rb, XsScalarBoundary tb,
-                                                                                      XsVelocityBoundary vb, float* __restrict__ out_rho,
+                                                                                      const __grid_constant__ XsScalarBoundary rb, const __grid_constant__ XsScalarBoundary tb,
+                                                                                      const __grid_constant__ XsVelocityBoundary vb, float* __restrict__ out_rho,
                                                                                       float* __restrict__ out_temp) {
     using S = ForwardTile;
     extern __shared__ float smem[];
@@ -372,6 +374,7 @@ __global__ void __launch_bounds__(ForwardTile::kThreads, 3) advect_scalar_pair_t
     tile::stage_wait();
     __syncthreads();
     const tile::StagedVelocity sv{{box[0], box[1], box[2]}, u};
+    const tile::TileConsts k = tile::tile_consts(g, vb);
     const int x = static_cast<int>(blockIdx.x) * S::TX + static_cast<int>(threadIdx.x);
     const int y = static_cast<int>(blockIdx.y) * S::TY + static_cast<int>(threadIdx.y);
     if (x >= g.nx || y >= g.ny) return;
@@ -381,11 +384,11 @@ __global__ void __launch_bounds__(ForwardTile::kThreads, 3) advect_scalar_pair_t
         if (z >= g.nz) break;
         const int li = tile::local_index<S>(kz);
         const Vec3 s = cell_position(x, y, z, g);
-        const Vec3 p = tile::staged_trace<S>(sv, s, tile::cell_start_velocity<S>(sv, li), o, g, vb);
+        const Vec3 p = tile::staged_trace<S>(sv, s, tile::cell_start_velocity<S>(sv, li), o, k, g, vb);
         const uint32_t i = static_cast<uint32_t>(x) + static_cast<uint32_t>(g.nx) * (static_cast<uint32_t>(y) + static_cast<uint32_t>(g.ny) *
                                                                                                                 static_cast<uint32_t>(z));
-        out_rho[i] = tile::staged_scalar<S, false>(box[3], src_rho, p, o, g, rb).value;
-        if (kFields == 2) out_temp[i] = tile::staged_scalar<S, false>(box[4], src_temp, p, o, g, tb).value;
+        out_rho[i] = tile::staged_scalar<S, false>(box[3], src_rho, p, o, k, g, rb).value;
+        if (kFields == 2) out_temp[i] = tile::staged_scalar<S, false>(box[4], src_temp, p, o, k, g, tb).value;
     }
 }
 
@@ -452,6 +455,97 @@ __global__ void accumulate_kernel(const double* __restrict__ src, double* __rest
     if (i < n) dst[i] += src[i];
 }
 
+// ------------------------------------------------ collider-free face passes
+// Faces of all three components addressed in 3D: blockIdx.z runs over the
+// z-slices of u, then v, then w (each component's own z extent); threads
+// cover (x, y) with x fastest, so loads and stores are coalesced and no index
+// is decoded.  The arithmetic is the general kernels' (bit-identical).
+struct FaceSlice {
+    int a, z;
+};
+
+__device__ __forceinline__ FaceSlice face_slice(const Grid& g) {
+    const int zi = static_cast<int>(blockIdx.z);
+    const int z0 = g.nz, z1 = 2 * g.nz;  // u and v have nz slices, w has nz + 1
+    if (zi < z0) return FaceSlice{0, zi};
+    if (zi < z1) return FaceSlice{1, zi - z0};
+    return FaceSlice{2, zi - z1};
+}
+
+inline dim3 face_pass_grid(const Grid& g) {
+    return dim3(static_cast<unsigned>((g.nx + 1 + 31) / 32), static_cast<unsigned>((g.ny + 1 + 7) / 8), static_cast<unsigned>(3 * g.nz + 1));
+}
+
+// operators.cu:358-364 without colliders, for face component A: the mean of
+// the one or two in-grid cell forces beside the face (division by a count
+// of 2 is the exact product with 0.5).
+template <int A>
+__device__ __forceinline__ void integrate_face(const Grid& g, int x, int y, int z, const XsVector& u, const XsVector& f, const XsVector& out) {
+    const int ex = extent(g, A, 0), ey = extent(g, A, 1);
+    if (x >= ex || y >= ey) return;
+    const uint32_t i = tile::index32(x, y, z, ex, ey);
+    const float* fa = component<const float>(f.x, f.y, f.z, A);
+    const int c = A == 0 ? x : (A == 1 ? y : z);
+    const int n = A == 0 ? g.nx : (A == 1 ? g.ny : g.nz);
+    const uint32_t upper = tile::index32(x, y, z, g.nx, g.ny);
+    const uint32_t lower = upper - static_cast<uint32_t>(A == 0 ? 1 : (A == 1 ? g.nx : g.nx * g.ny));
+    float sum = 0.0f, mean;
+    if (c == 0) {
+        sum += __ldg(fa + upper);
+        mean = sum;
+    } else if (c == n) {
+        sum += __ldg(fa + lower);
+        mean = sum;
+    } else {
+        sum += __ldg(fa + lower);
+        sum += __ldg(fa + upper);
+        mean = sum * 0.5f;
+    }
+    component(out.x, out.y, out.z, A)[i] = component<const float>(u.x, u.y, u.z, A)[i] + g.dt * mean;
+}
+
+__global__ void __launch_bounds__(256) integrate_faces_kernel(const __grid_constant__ Grid g, XsVector u, XsVector f, XsVector out) {
+    const FaceSlice fsl = face_slice(g);
+    const int x = static_cast<int>(blockIdx.x * 32 + threadIdx.x), y = static_cast<int>(blockIdx.y * 8 + threadIdx.y);
+    if (fsl.a == 0) integrate_face<0>(g, x, y, fsl.z, u, f, out);
+    else if (fsl.a == 1) integrate_face<1>(g, x, y, fsl.z, u, f, out);
+    else integrate_face<2>(g, x, y, fsl.z, u, f, out);
+}
+
+// operators.cu:912-920 with the FP64 pressure iterate, without colliders, for
+// face component A.  For a power-of-two spacing the FP64 division by h is the
+// exact product with inv_h = 1/h (computed on the host; the same IEEE result).
+template <int A, bool kPow2>
+__device__ __forceinline__ void project64_face(const Grid& g, double inv_h, int x, int y, int z, const XsVector& u, const double* __restrict__ p,
+                                               const XsVector& out) {
+    const int ex = extent(g, A, 0), ey = extent(g, A, 1);
+    if (x >= ex || y >= ey) return;
+    const uint32_t i = tile::index32(x, y, z, ex, ey);
+    const float* ua = component<const float>(u.x, u.y, u.z, A);
+    float* oa = component(out.x, out.y, out.z, A);
+    const int c = A == 0 ? x : (A == 1 ? y : z);
+    const int n = A == 0 ? g.nx : (A == 1 ? g.ny : g.nz);
+    if (c == 0 || c == n) {  // projectable_face: both cells in the grid
+        oa[i] = ua[i];
+        return;
+    }
+    const uint32_t second = tile::index32(x, y, z, g.nx, g.ny);
+    const uint32_t first = second - static_cast<uint32_t>(A == 0 ? 1 : (A == 1 ? g.nx : g.nx * g.ny));
+    const double dp = __ldg(p + second) - __ldg(p + first);
+    const double scaled = static_cast<double>(g.dt) * dp;
+    oa[i] = static_cast<float>(static_cast<double>(ua[i]) - (kPow2 ? scaled * inv_h : scaled / static_cast<double>(g.h)));
+}
+
+template <bool kPow2>
+__global__ void __launch_bounds__(256) project64_faces_kernel(const __grid_constant__ Grid g, double inv_h, XsVector u, const double* __restrict__ p,
+                                                              XsVector out) {
+    const FaceSlice fsl = face_slice(g);
+    const int x = static_cast<int>(blockIdx.x * 32 + threadIdx.x), y = static_cast<int>(blockIdx.y * 8 + threadIdx.y);
+    if (fsl.a == 0) project64_face<0, kPow2>(g, inv_h, x, y, fsl.z, u, p, out);
+    else if (fsl.a == 1) project64_face<1, kPow2>(g, inv_h, x, y, fsl.z, u, p, out);
+    else project64_face<2, kPow2>(g, inv_h, x, y, fsl.z, u, p, out);
+}
+
 // ------------------------------------------------------------ launchers
 template <int kFields>
 XsStatus launch_scalar_tiled(cudaStream_t st, const Grid& g, const float* src_rho, const float* src_temp, const XsVector& u,
@@ -486,6 +580,10 @@ XsStatus launch_source_buoyancy(cudaStream_t st, const Grid& g, const uint32_t* 
 }
 
 XsStatus launch_integrate(cudaStream_t st, const Grid& g, const uint32_t* mask, const XsVector& u, const XsVector& f, const XsVector& out) {
+    if (mask == nullptr) {
+        integrate_faces_kernel<<<face_pass_grid(g), dim3(32, 8), 0, st>>>(g, u, f, out);
+        return check_launch();
+    }
     const FaceSpace fs = face_space(g);
     integrate_kernel<<<blocks_for(fs.total()), kBlock, 0, st>>>(g, fs, mask, u, f, out);
     return check_launch();
@@ -527,6 +625,14 @@ XsStatus launch_project(cudaStream_t st, const Grid& g, const uint32_t* mask, co
 }
 
 XsStatus launch_project64(cudaStream_t st, const Grid& g, const uint32_t* mask, const XsVector& u, const double* p, const XsVector& out) {
+    if (mask == nullptr) {
+        const double inv_h = 1.0 / static_cast<double>(g.h);
+        if (tile::tiled_advection(g, mask))
+            project64_faces_kernel<true><<<face_pass_grid(g), dim3(32, 8), 0, st>>>(g, inv_h, u, p, out);
+        else
+            project64_faces_kernel<false><<<face_pass_grid(g), dim3(32, 8), 0, st>>>(g, inv_h, u, p, out);
+        return check_launch();
+    }
     const FaceSpace fs = face_space(g);
     project64_kernel<<<blocks_for(fs.total()), kBlock, 0, st>>>(g, fs, mask, u, p, out);
     return check_launch();

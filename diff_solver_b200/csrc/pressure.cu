@@ -822,7 +822,7 @@ __global__ void __launch_bounds__(kBlock, kSmooth ? 3 : 4) pcg_kernel(PcgArgs a)
     // iterations of a pass then move 16 bytes per cell less (same iteration
     // count within 2 in FP64 experiments at 128^3).
     const double smooth_begin2 = 100.0 * target2;
-    uint32_t iterations = 0, refinements = 0;
+    uint32_t iterations = 0, refinements = 0, smoothed_iterations = 0;
     uint32_t status = XS_OK;
     while (true) {
         if (!(rr <= target2)) {
@@ -861,6 +861,7 @@ __global__ void __launch_bounds__(kBlock, kSmooth ? 3 : 4) pcg_kernel(PcgArgs a)
             else update_phase<kSmooth>(a, alpha, smode != kSmoothOff, v4);
             if (!grid_reduce<4>(st, a.partials, v4, red)) return;
             ++iterations;
+            if (smode != kSmoothOff) ++smoothed_iterations;
             beta = static_cast<float>(v4[0] / rz);
             rz = v4[0];
             if (!isfinite(v4[1])) { broke = true; break; }
@@ -906,6 +907,7 @@ __global__ void __launch_bounds__(kBlock, kSmooth ? 3 : 4) pcg_kernel(PcgArgs a)
         st->stats.initial_residual = initial;
         st->stats.final_residual = bb > 0.0 ? sqrt(rr / bb) : 0.0;
         st->stats.guess_scale = scale;
+        st->stats.smoothed_iterations = smoothed_iterations;
     }
 }
 

@@ -235,8 +235,10 @@ __global__ void reduce_metrics_kernel(Grid g, const uint32_t* __restrict__ mask,
     }
 }
 
+// The example zeroes its metrics buffer before each reduction
+// (simulation.cpp:97-98): sums and maxima start at 0.
 __global__ void metrics_init_kernel(double* metrics) {
-    if (threadIdx.x < 6) metrics[threadIdx.x] = (threadIdx.x >= 1 && threadIdx.x <= 3) ? -INFINITY : 0.0;
+    if (threadIdx.x < 6) metrics[threadIdx.x] = 0.0;
 }
 
 }  // namespace xs

@@ -72,8 +72,8 @@ __device__ __forceinline__ Vec3 trace_tangent(const Vec3& s, const XsVector& u, 
 }
 
 // operators.cu:390-413 for all three components in one launch.
-__global__ void advect_velocity_jvp_kernel(Grid g, uint64_t f0, uint64_t f1, uint64_t f2, const uint32_t* __restrict__ mask, XsVector u,
-                                           XsVector ut, XsVelocityBoundary vb, XsVector out) {
+__global__ void advect_velocity_jvp_kernel(const __grid_constant__ Grid g, uint64_t f0, uint64_t f1, uint64_t f2, const uint32_t* __restrict__ mask, XsVector u,
+                                           XsVector ut, const __grid_constant__ XsVelocityBoundary vb, XsVector out) {
     const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= f0 + f1 + f2) return;
     int a;
@@ -92,10 +92,10 @@ __global__ void advect_velocity_jvp_kernel(Grid g, uint64_t f0, uint64_t f1, uin
 }
 
 // operators.cu:509-535; the second scalar (src2 non-null) shares the trace.
-__global__ void advect_scalar_jvp_kernel(Grid g, const uint32_t* __restrict__ mask, const float* __restrict__ src,
-                                         const float* __restrict__ src_t, XsScalarBoundary sb, float* __restrict__ out,
-                                         const float* __restrict__ src2, const float* __restrict__ src2_t, XsScalarBoundary sb2,
-                                         float* __restrict__ out2, XsVector u, XsVector ut, XsVelocityBoundary vb) {
+__global__ void advect_scalar_jvp_kernel(const __grid_constant__ Grid g, const uint32_t* __restrict__ mask, const float* __restrict__ src,
+                                         const float* __restrict__ src_t, const __grid_constant__ XsScalarBoundary sb, float* __restrict__ out,
+                                         const float* __restrict__ src2, const float* __restrict__ src2_t, const __grid_constant__ XsScalarBoundary sb2,
+                                         float* __restrict__ out2, XsVector u, XsVector ut, const __grid_constant__ XsVelocityBoundary vb) {
     const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= cell_count(g)) return;
     if (is_solid(mask, i)) {

@@ -71,6 +71,7 @@ typedef struct XsVelocityBoundary {
 
 /* CenteredVectorView / StaggeredVectorView (cuda_types.h:45-79) */
 typedef struct XsVector { float* x; float* y; float* z; } XsVector;
+typedef struct XsVec3 { float x, y, z; } XsVec3;
 /* CenteredVectorAdjointView / StaggeredVectorAdjointView (:95-129) */
 typedef struct XsAdjointVector { double* x; double* y; double* z; } XsAdjointVector;
 
@@ -117,7 +118,7 @@ typedef struct XsSolveStats {
     double final_residual;        /* ||b - A p||_2 / ||b||_2, p in FP64 */
     double guess_scale;           /* alpha applied to the guess (1 if unscaled, 0 if none) */
     uint32_t coarse_iterations;   /* CG iterations of the coarse-grid correction of the start (0: none) */
-    uint32_t reserved;
+    uint32_t smoothed_iterations; /* iterations that also updated the minimal-residual smoothed sequence */
 } XsSolveStats;
 
 /* ------------------------------------------------------------------------ */
@@ -376,7 +377,20 @@ XsStatus xs_smoke_vjp_step(cudaStream_t stream, const XsSmokeModel* model, XsSta
 /* The example driver's per-step metrics (examples/smoke/forward/
  * simulation.cu:59-85) into metrics[6] (device): density sum, density max,
  * temperature max, max centred speed, sum of squared divergence before and
- * after projection, over fluid cells.  Overwrites metrics. */
+ * after projection, over fluid cells.  Overwrites metrics; the maxima start
+ * at 0, as the example zeroes its metrics buffer before the reduction
+ * (simulation.cpp:97-98). */
+/* The example driver's controls (examples/smoke/forward/simulation.cu:35-57,
+ * launch_write_control): at step `step` (time step * dt), two Gaussian jets
+ * of the given radius whose amplitudes 0.75 + 0.25 sin(2 pi t / period)
+ * pulse in antiphase; per cell, the density and temperature sources are the
+ * rates times the summed jet weights and the external acceleration is the
+ * weighted sum of the jets' accelerations.  Overwrites all five fields. */
+XsStatus xs_smoke_write_control(cudaStream_t stream, XsGrid grid, uint64_t step, float pulse_period, XsVec3 left_center,
+                                XsVec3 right_center, float source_radius, float density_source_rate, float temperature_source_rate,
+                                XsVec3 left_acceleration, XsVec3 right_acceleration, float* density_source, float* temperature_source,
+                                XsVector external_acceleration);
+
 XsStatus xs_smoke_reduce_metrics(cudaStream_t stream, const XsSmokeModel* model, const float* density, const float* temperature,
                                  XsVector pre_projection_velocity, XsVector post_projection_velocity, double* metrics);
 

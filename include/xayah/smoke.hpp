@@ -192,6 +192,8 @@ public:
     // times its factor is this model's grid); nullptr: none.  The guess is
     // energy-scaled and PCG falls back to zero when it does not help.
     void set_learned_warm_start(XsWarmStartNet* net) { native_.warm_start = net; }
+    // The model block the C ABI's step-level entry points take.
+    [[nodiscard]] const XsSmokeModel& native() const { return native_; }
 
 private:
     ExecutionMode mode_{ExecutionMode::forward};

@@ -79,6 +79,11 @@ def lib():
                                         C.c_void_p * 3, C.c_void_p]
         L.ref_rbgs.argtypes = [C.c_void_p, C.POINTER(RefModel), C.c_void_p, C.c_void_p, C.c_uint32]
         L.ref_launch.argtypes = [C.c_void_p, C.POINTER(RefModel), C.c_uint32, C.POINTER(RefLaunchArgs)]
+        F3 = C.c_float * 3
+        L.ref_write_control.argtypes = [C.c_void_p, C.POINTER(RefModel), C.c_uint64, C.c_float, F3, F3, C.c_float, C.c_float, C.c_float, F3, F3,
+                                        C.c_void_p, C.c_void_p, C.c_void_p * 3]
+        L.ref_reduce_metrics.argtypes = [C.c_void_p, C.POINTER(RefModel), C.c_void_p, C.c_void_p, C.c_void_p * 3, C.c_void_p * 3,
+                                         C.c_void_p]
         _lib = L
     return _lib
 
@@ -188,3 +193,25 @@ class Reference:
         r = self.L.ref_launch(self._stream(), C.byref(self.m), int(which), C.byref(a))
         if r != 0:
             raise RuntimeError(f"reference launch {which} failed ({r})")
+
+    def write_control(self, step, o, density_source, temperature_source, acceleration):
+        """The example driver's launch_write_control (simulation.cu:88-92) for
+        options `o` (any object with the ForwardSimulationOptions fields)."""
+        F3 = C.c_float * 3
+        v = lambda t: F3(*[float(c) for c in t])
+        r = self.L.ref_write_control(self._stream(), C.byref(self.m), int(step), float(o.pulse_period), v(o.left_source_center),
+                                     v(o.right_source_center), float(o.source_radius), float(o.density_source_rate),
+                                     float(o.temperature_source_rate), v(o.left_acceleration), v(o.right_acceleration),
+                                     C.c_void_p(density_source.data_ptr()), C.c_void_p(temperature_source.data_ptr()),
+                                     (C.c_void_p * 3)(*[t.data_ptr() for t in acceleration]))
+        if r != 0:
+            raise RuntimeError(f"reference write_control failed ({r})")
+
+    def reduce_metrics(self, density, temperature, pre, post, metrics):
+        """The example driver's launch_reduce_metrics (simulation.cu:95-100)
+        into a zeroed metrics[6] (FP64, device)."""
+        r = self.L.ref_reduce_metrics(self._stream(), C.byref(self.m), C.c_void_p(density.data_ptr()), C.c_void_p(temperature.data_ptr()),
+                                      (C.c_void_p * 3)(*[t.data_ptr() for t in pre]), (C.c_void_p * 3)(*[t.data_ptr() for t in post]),
+                                      C.c_void_p(metrics.data_ptr()))
+        if r != 0:
+            raise RuntimeError(f"reference reduce_metrics failed ({r})")

@@ -9,6 +9,9 @@
 // `import std` and cannot be built with this toolchain; this file replaces
 // only their call order.  Built by oracle/build_ref.sh into oracle/_ref/.
 #include "operators.cu"
+// The forward example driver's kernels (examples/smoke/forward/simulation.cu:
+// write_control, reduce_metrics), also included unmodified.
+#include "simulation.cu"
 
 #include <cmath>
 #include <cstdint>
@@ -425,6 +428,32 @@ int ref_launch(cudaStream_t stream, const RefModel* m, uint32_t which, const Ref
         return 1;
     }
     return cudaGetLastError() == cudaSuccess ? 0 : 2;
+}
+
+// The example driver's launchers (simulation.cu:88-100).
+int ref_write_control(cudaStream_t stream, const RefModel* m, uint64_t step, float pulse_period, const float* left_center,
+                      const float* right_center, float source_radius, float density_rate, float temperature_rate, const float* left_acc,
+                      const float* right_acc, float* density_source, float* temperature_source, float* acceleration[3]) {
+    namespace ex = xayah::smoke::examples::forward::simulation_cuda;
+    try {
+        ex::launch_write_control(stream, m->grid, step, pulse_period, Vector{left_center[0], left_center[1], left_center[2]},
+                                 Vector{right_center[0], right_center[1], right_center[2]}, source_radius, density_rate, temperature_rate,
+                                 Vector{left_acc[0], left_acc[1], left_acc[2]}, Vector{right_acc[0], right_acc[1], right_acc[2]}, density_source,
+                                 temperature_source, CenteredVectorView{acceleration[0], acceleration[1], acceleration[2]});
+    } catch (const std::exception&) { return 1; }
+    return cudaStreamSynchronize(stream) == cudaSuccess ? 0 : 2;
+}
+
+// reduce_metrics into metrics[6], zeroed first as simulation.cpp:97 does.
+int ref_reduce_metrics(cudaStream_t stream, const RefModel* m, const float* density, const float* temperature, float* const pre[3],
+                       float* const post[3], double* metrics) {
+    namespace ex = xayah::smoke::examples::forward::simulation_cuda;
+    try {
+        cudaMemsetAsync(metrics, 0, 6 * sizeof(double), stream);
+        ex::launch_reduce_metrics(stream, m->grid, m->cell_mask, density, temperature, ConstStaggeredVectorView{pre[0], pre[1], pre[2]},
+                                  ConstStaggeredVectorView{post[0], post[1], post[2]}, metrics);
+    } catch (const std::exception&) { return 1; }
+    return cudaStreamSynchronize(stream) == cudaSuccess ? 0 : 2;
 }
 
 // Layout check: the harness' view of the model block as 32-bit words.

@@ -202,3 +202,15 @@ def test_tiled_advection_is_bit_identical_to_the_general_kernels(cuda, name, res
     torch.cuda.synchronize()
     for a in range(3):
         assert torch.equal(tiled[a].view(torch.int32), raw[a].view(torch.int32)), (name, "raw", a)
+    # integration: the 3D-indexed collider-free kernel against the general one
+    u0 = [torch.as_tensor(np.asarray(a, np.float32), device=dev).contiguous() for a in st["velocity"]]
+    force = [torch.as_tensor(a, device=dev).contiguous() for a in k["force"]]
+    integrated = {}
+    for key, m in (("fast", None), ("general", mask)):
+        o = [torch.zeros_like(a) for a in u0]
+        N.check("integrate", L.xs_integrate_velocity_forward(None, g, m, N.vec(u0), N.vec(force), N.vec(o)))
+        integrated[key] = o
+    torch.cuda.synchronize()
+    for a in range(3):
+        assert torch.equal(integrated["fast"][a].view(torch.int32), integrated["general"][a].view(torch.int32)), (name, "integrate", a)
+        assert np.array_equal(integrated["fast"][a].cpu().numpy().view(np.uint32), k["forced_velocity"][a].view(np.uint32))

@@ -72,3 +72,53 @@ def test_checkpointed_vjp_matches_fp64_finite_differences(cuda, steps, interval,
         fd = (loss([u + eps * di for u, di in zip(u0, d)]) - loss([u - eps * di for u, di in zip(u0, d)])) / (2 * eps)
         rels.append(abs(fd - gd) / max(abs(fd), 1e-30))
     assert max(rels) < 1e-3, rels
+
+
+def test_plume_vjp_matches_oracle_finite_differences(cuda):
+    """The differentiable plume as specified (tests/common.py:
+    differentiable_plume): 128^3, 50 steps, loss = ||rho_50 - target||_2, the
+    gradient with respect to the initial velocity from the checkpointed VJP
+    (every 10 steps, recompute in between), against FP64 central finite
+    differences (eps = 1e-3) of the CPU oracle along the first seeded unit
+    directions, precomputed by tests/golden/make_fd.py (pressure converged
+    to 1e-12 in every oracle step).  Agreement to 1e-3 relative."""
+    import os
+
+    import torch
+    from common import differentiable_plume, plume_directions
+    from diff_solver_b200.model import ExecutionMode, Model, fill_parameters
+    from diff_solver_b200.solver import TapeMode, simulate, vjp
+    path = os.path.join(ROOT, "tests", "golden", "fd_plume_128.npz")
+    if not os.path.exists(path):
+        pytest.skip("finite-difference fixture not generated (tests/golden/make_fd.py)")
+    z = np.load(path)
+    fd = np.asarray(z["finite_differences"], np.float64)
+    n, steps = int(z["grid"]), int(z["steps"])
+    assert fd.size >= 4, "the fixture holds fewer than 4 directions"
+    cfg, u0, target = differentiable_plume(n)
+    cfg.pressure_tolerance = 1e-10
+    cfg.pressure_max_iterations = 50000
+    model = Model(cfg)
+    ctx = model.allocate_context(ExecutionMode.differentiable)
+    params = fill_parameters(model.allocate_parameters(ctx), **PARAMS)
+    controls = [model.allocate_control(ctx) for _ in range(steps)]
+    s0 = model.allocate_state(ctx)
+    for t, v in zip(s0.velocity.components(), u0):
+        t.copy_(torch.from_numpy(v).float())
+    traj = simulate(model, ctx, s0, controls, params, TapeMode.checkpoint, 10)
+    final = traj.states[-1].density.values.double()
+    target_d = torch.from_numpy(target).cuda()
+    diff = final - target_d
+    loss = float(torch.sqrt((diff * diff).sum()))
+    assert abs(loss - float(z["loss"])) <= 1e-5 * float(z["loss"]), (loss, float(z["loss"]))
+    seed = model.allocate_state_adjoint(ctx)
+    seed.density.values.copy_(diff / loss)
+    grad = vjp(model, ctx, traj, controls, params, {steps: seed})
+    g = [t.cpu().numpy() for t in grad.initial_state.velocity.components()]
+    rels = []
+    for d, want in zip(plume_directions(n, fd.size), fd):
+        got = sum(float(gi @ di) for gi, di in zip(g, d))
+        rels.append(abs(got - want) / abs(want))
+    from common import report
+    report("fd_plume_128", loss=loss, finite_differences=fd.tolist(), relative_errors=rels)
+    assert max(rels) < 1e-3, rels

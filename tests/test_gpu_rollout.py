@@ -7,7 +7,7 @@
   converged to 1e-12) and by the reference's own kernels
   (solvers/smoke/operators.cu through oracle/_ref, model.cpp:341-349 order,
   red-black Gauss-Seidel iterated until the FP32 sweeps stop lowering the
-  residual: about 3e-6 relative on this plume).  Density, temperature and
+  residual: about 3e-6 relative at 64^3, 1e-5 at 128^3).  Density, temperature and
   velocity must agree to 1e-5 relative L2.
   Run with the plain zero start, the classical warm start (ring of previous
   solutions, coarse-grid step) and the benchmark's learned pipeline.
@@ -102,10 +102,11 @@ def test_plume_rollout_matches_oracle_and_reference_kernels(cuda, n, start, step
             report(f"rollout{n}_{start}", step=step + 1, oracle=e_oracle, reference=e_ref, reference_sweeps=sweeps,
                    reference_residual=residual, product_iterations=stats["iterations"], product_residual=stats["final_residual"],
                    warm_start_used=stats["warm_start_used"])
-            # the reference's FP32 sweeps stop at their rounding floor (~3e-6 on
-            # this plume: the stall test of the harness); that they got there
-            # and not stuck early is checked here, the fields below
-            assert residual < 1e-5, (step, sweeps, residual)
+            # the reference's FP32 sweeps stop at their rounding floor (the
+            # stall test of the harness: ~3e-6 relative at 64^3, ~1e-5 at
+            # 128^3); that they got there and not stuck early is checked here,
+            # the fields below
+            assert residual < 3e-5, (step, sweeps, residual)
             for name, e in (("oracle", e_oracle), ("reference", e_ref)):
                 for field, v in e.items():
                     assert v < 1e-5, (start, step + 1, name, field, v)

@@ -3,6 +3,8 @@ loss and parameter gradient against the CPU reference network (PyTorch FP32
 autograd with the GPU's BF16 storage points), restriction / prolongation,
 Adam training, the energy-scaled PCG start with its zero-guess fallback, and
 the network inside a model step."""
+import os
+
 import numpy as np
 import pytest
 
@@ -313,25 +315,52 @@ def test_galerkin_history_with_learned_guess(cuda):
 
 def test_trained_network_gain(cuda):
     """What the committed network (trained at 128^3 on 20k plume pairs) gains
-    on the held-out benchmark plume at 128^3: fewer PCG iterations than the
-    zero start on its own, and fewer than the Galerkin history alone when it
-    corrects the history's start."""
-    import os
-    from diff_solver_b200.warm_start import WarmStartNetwork, evaluate_arms
+    in the benchmark's own pipeline: the 256^3 plume from rest, each forward
+    solve started from the ring of the last 5 solutions and the coarse-grid
+    step, with and without the network's correction step on top (network
+    applied on the grid restricted x2).  The network's step removes fine PCG
+    iterations (measured in the benchmark window, steps 185-205: 26.9 -> 24.2
+    per step).  At this grid its inference and line step cost more time than
+    those iterations (bench.py's history+coarse and learned+history+coarse
+    arms report both); this test asserts the iteration gain, the part the
+    network is responsible for, on steps 20-60 of the plume."""
+    import torch
+    from diff_solver_b200.data import plume_configuration
+    from diff_solver_b200.model import ExecutionMode, Model, fill_parameters
+    from diff_solver_b200.warm_start import WarmStartNetwork
     weights = os.path.join(ROOT, "diff_solver_b200", "weights", "warm_start_128.npz")
-    net = WarmStartNetwork((128, 128, 128), factor=1)
+    res = (256, 256, 256)
+    net = WarmStartNetwork((128, 128, 128), factor=2)
     net.load(weights)
-    arms = evaluate_arms(net, (128, 128, 128), steps=60, history=5)
-    late = {k: float(np.mean(v[20:])) for k, v in arms.items()}
-    print(late)
-    # the network alone against the zero start it replaces (measured: 2.5 %
-    # fewer iterations)
-    assert late["learned"] < 0.99 * late["plain"], late
-    assert late["history"] < 0.5 * late["plain"], late
-    # on top of the residual-smoothed history start the correction is within
-    # the step-to-step scatter of warm-started iteration counts (measured
-    # -8 % to +8 %); it must not spoil that start
-    assert late["learned+history"] < 1.25 * late["history"], late
+    iterations = {}
+    for name in ("classical", "learned"):
+        cfg = plume_configuration(res)
+        cfg.pressure_max_iterations = 20000
+        cfg.warm_start_history = 5
+        cfg.warm_start_coarsening = 2
+        m = Model(cfg)
+        ctx = m.allocate_context(ExecutionMode.forward)
+        if name == "learned":
+            ctx.set_learned_warm_start(net)
+        s, n = m.allocate_state(ctx), m.allocate_state(ctx)
+        c, k = m.allocate_control(ctx), m.allocate_step_cache(ctx)
+        q = fill_parameters(m.allocate_parameters(ctx), 0.0, -0.1, 0.5)
+        g = torch.Generator(device="cuda").manual_seed(0)
+        for t in s.velocity.components():
+            t.uniform_(-0.01, 0.01, generator=g)
+        its = []
+        for _ in range(60):
+            m.forward_step(s, c, q, n, k, ctx)
+            s, n = n, s
+            st = ctx.read_solve_stats()
+            assert st["status"] == 0 and st["final_residual"] <= 1e-6, st
+            its.append(st["iterations"])
+        iterations[name] = float(np.mean(its[20:]))
+        del m, ctx, s, n, c, k
+        torch.cuda.empty_cache()
+    net.check()
+    print(iterations)
+    assert iterations["learned"] <= 0.95 * iterations["classical"], iterations
 
 
 def test_learned_warm_start_inside_a_model_step(cuda):
