@@ -83,32 +83,40 @@ __device__ __forceinline__ void cp_async4(float* dst, const float* src) {
 __device__ __forceinline__ void stage_wait() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // Stages face component A over the box: one warp per box row (x-contiguous,
-// coalesced), two passes for the row's SX nodes.  Nodes inside the array are
-// copied asynchronously; only nodes beyond the domain edge take the
-// boundary rules (a box that crosses the edge keeps the fast copy for the
-// rest of its nodes).  The caller runs stage_wait() and __syncthreads()
+// coalesced), two passes for the row's SX nodes.  A box inside the array is
+// copied asynchronously by a short unrolled loop; a box that crosses the
+// domain edge (rolled loop, one copy of the boundary logic) copies its
+// in-array nodes asynchronously and applies the boundary rules to the nodes
+// beyond the edge only.  The caller runs stage_wait() and __syncthreads()
 // before reading the box.
 template <class S, int A>
 __device__ __forceinline__ void stage_face(float* __restrict__ s, const float* __restrict__ v, const Origin& o, const Grid& g,
                                            const XsVelocityBoundary& b) {
     const int ex = extent(g, A, 0), ey = extent(g, A, 1), ez = extent(g, A, 2);
+    // nodes that are plain elements: inside the array, and inside the wrap
+    // period on a periodic axis (there the face at n is the face at 0)
+    const int lx = periodic(b, 0) ? g.nx : ex, ly = periodic(b, 1) ? g.ny : ey, lz = periodic(b, 2) ? g.nz : ez;
     const int lane = threadIdx.x, warp = threadIdx.y;
+    if (box_inside<S>(o, lx, ly, lz)) {
 #pragma unroll
-    for (int r = 0; r < S::kRows / S::TY; ++r) {
-        const int row = warp + r * S::TY;
-        const int y = o.y + row % S::SY, z = o.z + row / S::SY;
-        const bool row_in = static_cast<unsigned>(y) < static_cast<unsigned>(ey) && static_cast<unsigned>(z) < static_cast<unsigned>(ez);
-        float* dst = s + row * S::SX;
-#pragma unroll
-        for (int half = 0; half < 2; ++half) {
-            const int lx = lane + 32 * half;
-            if (half == 1 && lx >= S::SX) break;
-            const int x = o.x + lx;
-            if (row_in && static_cast<unsigned>(x) < static_cast<unsigned>(ex))
-                cp_async4(dst + lx, v + index32(x, y, z, ex, ey));
-            else
-                dst[lx] = load_face(v, A, x, y, z, g, b);
+        for (int r = 0; r < S::kRows / S::TY; ++r) {
+            const int row = warp + r * S::TY;
+            const float* src = v + index32(o.x, o.y + row % S::SY, o.z + row / S::SY, ex, ey);
+            float* dst = s + row * S::SX;
+            cp_async4(dst + lane, src + lane);
+            if (lane < S::SX - 32) cp_async4(dst + 32 + lane, src + 32 + lane);
         }
+        return;
+    }
+#pragma unroll 1
+    for (int k = lane + 32 * warp; k < S::kNodes; k += S::kThreads) {
+        const int bx = k % S::SX, row = k / S::SX;
+        const int x = o.x + bx, y = o.y + row % S::SY, z = o.z + row / S::SY;
+        if (static_cast<unsigned>(x) < static_cast<unsigned>(lx) && static_cast<unsigned>(y) < static_cast<unsigned>(ly) &&
+            static_cast<unsigned>(z) < static_cast<unsigned>(lz))
+            cp_async4(s + k, v + index32(x, y, z, ex, ey));
+        else
+            s[k] = load_face(v, A, x, y, z, g, b);
     }
 }
 
@@ -117,22 +125,26 @@ template <class S>
 __device__ __forceinline__ void stage_cells(float* __restrict__ s, const float* __restrict__ v, const Origin& o, const Grid& g,
                                             const XsScalarBoundary& b) {
     const int lane = threadIdx.x, warp = threadIdx.y;
+    if (box_inside<S>(o, g.nx, g.ny, g.nz)) {
 #pragma unroll
-    for (int r = 0; r < S::kRows / S::TY; ++r) {
-        const int row = warp + r * S::TY;
-        const int y = o.y + row % S::SY, z = o.z + row / S::SY;
-        const bool row_in = static_cast<unsigned>(y) < static_cast<unsigned>(g.ny) && static_cast<unsigned>(z) < static_cast<unsigned>(g.nz);
-        float* dst = s + row * S::SX;
-#pragma unroll
-        for (int half = 0; half < 2; ++half) {
-            const int lx = lane + 32 * half;
-            if (half == 1 && lx >= S::SX) break;
-            const int x = o.x + lx;
-            if (row_in && static_cast<unsigned>(x) < static_cast<unsigned>(g.nx))
-                cp_async4(dst + lx, v + index32(x, y, z, g.nx, g.ny));
-            else
-                dst[lx] = load_scalar(v, x, y, z, g, b);
+        for (int r = 0; r < S::kRows / S::TY; ++r) {
+            const int row = warp + r * S::TY;
+            const float* src = v + index32(o.x, o.y + row % S::SY, o.z + row / S::SY, g.nx, g.ny);
+            float* dst = s + row * S::SX;
+            cp_async4(dst + lane, src + lane);
+            if (lane < S::SX - 32) cp_async4(dst + 32 + lane, src + 32 + lane);
         }
+        return;
+    }
+#pragma unroll 1
+    for (int k = lane + 32 * warp; k < S::kNodes; k += S::kThreads) {
+        const int bx = k % S::SX, row = k / S::SX;
+        const int x = o.x + bx, y = o.y + row % S::SY, z = o.z + row / S::SY;
+        if (static_cast<unsigned>(x) < static_cast<unsigned>(g.nx) && static_cast<unsigned>(y) < static_cast<unsigned>(g.ny) &&
+            static_cast<unsigned>(z) < static_cast<unsigned>(g.nz))
+            cp_async4(s + k, v + index32(x, y, z, g.nx, g.ny));
+        else
+            s[k] = load_scalar(v, x, y, z, g, b);
     }
 }
 
@@ -397,7 +409,9 @@ template <class S, int A>
 __device__ __forceinline__ void flush_face(const double* __restrict__ acc, double* __restrict__ v, const Origin& o, const Grid& g,
                                            const XsVelocityBoundary& b) {
     const int ex = extent(g, A, 0), ey = extent(g, A, 1), ez = extent(g, A, 2);
-    const bool inside = box_inside<S>(o, ex, ey, ez);
+    // plain elements only inside the wrap period on a periodic axis (there the
+    // face at n is the face at 0)
+    const bool inside = box_inside<S>(o, periodic(b, 0) ? g.nx : ex, periodic(b, 1) ? g.ny : ey, periodic(b, 2) ? g.nz : ez);
     const int t = threadIdx.x + S::TX * threadIdx.y;
     for (int k = t; k < S::kNodes; k += S::kThreads) {
         const double s = acc[k];

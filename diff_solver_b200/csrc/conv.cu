@@ -50,15 +50,15 @@ CUtensorMapSwizzle swizzle_mode(uint32_t row_bytes) {
 
 }  // namespace
 
-// Activation map [B][Z][Y][X][C] with a (C, bx, by, 1, 1) box.
-bool make_activation_map(CUtensorMap* map, const void* base, const VolumeShape& s, uint32_t channels, uint32_t bx, uint32_t by) {
+// Activation map [B][Z][Y][X][C] with a (C, bx, by, bz, 1) box.
+bool make_activation_map(CUtensorMap* map, const void* base, const VolumeShape& s, uint32_t channels, uint32_t bx, uint32_t by, uint32_t bz) {
     auto fn = encode_fn();
     if (!fn) return false;
     const cuuint64_t dims[5] = {channels, s.x, s.y, s.z, s.batch};
     const cuuint64_t e = 2;
     const cuuint64_t strides[4] = {channels * e, s.x * channels * e, static_cast<cuuint64_t>(s.y) * s.x * channels * e,
                                    static_cast<cuuint64_t>(s.z) * s.y * s.x * channels * e};
-    const cuuint32_t box[5] = {channels, bx, by, 1, 1};
+    const cuuint32_t box[5] = {channels, bx, by, bz, 1};
     const cuuint32_t elem[5] = {1, 1, 1, 1, 1};
     return fn(map, CU_TENSOR_MAP_DATA_TYPE_BFLOAT16, 5, const_cast<void*>(base), dims, strides, box, elem, CU_TENSOR_MAP_INTERLEAVE_NONE,
               swizzle_mode(channels * 2), CU_TENSOR_MAP_L2_PROMOTION_L2_128B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
@@ -92,14 +92,14 @@ struct ConvSmem {
 
 struct ConvArgs {
     VolumeShape s;
-    uint32_t bx, by;  // output tile box
+    uint32_t bx, by, bz;  // output tile box
     const float* bias;
     __nv_bfloat16* out;
     int relu;
     int* error;
 };
 
-// One CTA = one tile of 128 output voxels (bx * by at one z of one batch).
+// One CTA = one tile of 128 output voxels (a bx * by * bz box of one batch).
 template <int CIN, int COUT>
 __global__ void __launch_bounds__(kConvThreads) conv3_forward_kernel(const __grid_constant__ CUtensorMap act_map,
                                                                      const __grid_constant__ CUtensorMap w_map, ConvArgs a) {
@@ -115,13 +115,13 @@ __global__ void __launch_bounds__(kConvThreads) conv3_forward_kernel(const __gri
 
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     // tile coordinates
-    const uint32_t tiles_x = a.s.x / a.bx, tiles_y = a.s.y / a.by;
+    const uint32_t tiles_x = a.s.x / a.bx, tiles_y = a.s.y / a.by, tiles_z = a.s.z / a.bz;
     uint32_t t = blockIdx.x;
     const uint32_t tx = t % tiles_x; t /= tiles_x;
     const uint32_t ty = t % tiles_y; t /= tiles_y;
-    const uint32_t z = t % a.s.z;
-    const uint32_t b = t / a.s.z;
-    const int x0 = static_cast<int>(tx * a.bx), y0 = static_cast<int>(ty * a.by);
+    const uint32_t tz = t % tiles_z;
+    const uint32_t b = t / tiles_z;
+    const int x0 = static_cast<int>(tx * a.bx), y0 = static_cast<int>(ty * a.by), z0 = static_cast<int>(tz * a.bz);
 
     if (threadIdx.x == 0) {
         for (int i = 0; i < kStages; ++i) {
@@ -150,7 +150,7 @@ __global__ void __launch_bounds__(kConvThreads) conv3_forward_kernel(const __gri
             if (tap >= kStages && !tc::mbar_wait(&empty[s], (round - 1) & 1)) { ok = false; break; }
             tc::mbar_expect_tx(&full[s], L::a_bytes + L::b_bytes_raw);
             const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
-            tc::tma_load_5d(a_tiles + s * L::a_bytes, &act_map, &full[s], 0, x0 + dx, y0 + dy, static_cast<int>(z) + dz, static_cast<int>(b));
+            tc::tma_load_5d(a_tiles + s * L::a_bytes, &act_map, &full[s], 0, x0 + dx, y0 + dy, z0 + dz, static_cast<int>(b));
             tc::tma_load_3d(b_tiles + s * L::b_bytes, &w_map, &full[s], 0, 0, tap);
         }
     } else if (warp == 1 && lane == 0) {
@@ -179,7 +179,8 @@ __global__ void __launch_bounds__(kConvThreads) conv3_forward_kernel(const __gri
     tc::tc_fence_after();
     if (got) {
         const int r = warp * 32 + lane;
-        const int x = x0 + r % static_cast<int>(a.bx), y = y0 + r / static_cast<int>(a.bx);
+        const int bxy = static_cast<int>(a.bx * a.by);
+        const int x = x0 + r % static_cast<int>(a.bx), y = y0 + (r % bxy) / static_cast<int>(a.bx), z = z0 + r / bxy;
         const uint64_t voxel = ((static_cast<uint64_t>(b) * a.s.z + z) * a.s.y + y) * a.s.x + x;
         __nv_bfloat16* dst = a.out + voxel * COUT;
 #pragma unroll
@@ -206,25 +207,29 @@ __global__ void __launch_bounds__(kConvThreads) conv3_forward_kernel(const __gri
 template <int CIN, int COUT>
 XsStatus launch_conv_forward(cudaStream_t st, const VolumeShape& s, const __nv_bfloat16* in, const __nv_bfloat16* w, const float* bias,
                              __nv_bfloat16* out, bool relu, int* error) {
-    uint32_t bx, by;
-    if (!conv_tile(s, bx, by)) return XS_INVALID_ARGUMENT;
+    uint32_t bx, by, bz;
+    if (!conv_tile(s, bx, by, bz)) return XS_INVALID_ARGUMENT;
     CUtensorMap am, wm;
-    if (!make_activation_map(&am, in, s, CIN, bx, by) || !make_weight_map(&wm, w, COUT, CIN)) return XS_CUDA_ERROR;
+    if (!make_activation_map(&am, in, s, CIN, bx, by, bz) || !make_weight_map(&wm, w, COUT, CIN)) return XS_CUDA_ERROR;
     using L = ConvSmem<CIN, COUT>;
     static DeviceOnce configured;
     if (!configured.run([] { return cudaFuncSetAttribute(conv3_forward_kernel<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::total); }))
         return XS_CUDA_ERROR;
-    ConvArgs args{s, bx, by, bias, out, relu ? 1 : 0, error};
-    const uint64_t tiles = static_cast<uint64_t>(s.batch) * s.z * (s.y / by) * (s.x / bx);
+    ConvArgs args{s, bx, by, bz, bias, out, relu ? 1 : 0, error};
+    const uint64_t tiles = static_cast<uint64_t>(s.batch) * (s.z / bz) * (s.y / by) * (s.x / bx);
     conv3_forward_kernel<CIN, COUT><<<static_cast<unsigned>(tiles), kConvThreads, L::total, st>>>(am, wm, args);
     return check_launch();
 }
 
-bool conv_tile(const VolumeShape& s, uint32_t& bx, uint32_t& by) {
+// The 128-voxel output tile: as wide in x as the volume allows (up to 128),
+// then in y, then in z (for small volumes, several z planes per tile).
+bool conv_tile(const VolumeShape& s, uint32_t& bx, uint32_t& by, uint32_t& bz) {
     bx = s.x < 128 ? s.x : 128;
     if (bx == 0 || 128 % bx != 0 || s.x % bx != 0) return false;
-    by = 128 / bx;
-    return by <= s.y && s.y % by == 0;
+    by = 128 / bx < s.y ? 128 / bx : s.y;
+    if (by == 0 || (128 / bx) % by != 0 || s.y % by != 0) return false;
+    bz = 128 / (bx * by);
+    return bz <= s.z && s.z % bz == 0;
 }
 
 XsStatus conv3_forward(cudaStream_t st, const VolumeShape& s, int cin, int cout, const __nv_bfloat16* in, const __nv_bfloat16* w,
@@ -260,7 +265,7 @@ struct WgradLayout {
 
 struct WgradArgs {
     VolumeShape s;
-    uint32_t bx, by;
+    uint32_t bx, by, bz;
     uint32_t tiles;
     float* partial;  // [gridDim.x][27][COUT][CIN]
     int* error;
@@ -304,7 +309,7 @@ __global__ void __launch_bounds__(kConvThreads) conv3_wgrad_kernel(const __grid_
     tc::tc_fence_after();
     const uint32_t tmem = *tmem_slot;
     bool ok = true;
-    const uint32_t tiles_x = a.s.x / a.bx, tiles_y = a.s.y / a.by;
+    const uint32_t tiles_x = a.s.x / a.bx, tiles_y = a.s.y / a.by, tiles_z = a.s.z / a.bz;
 
     if (warp == 0 && lane == 0) {
         for (uint32_t i = 0; i < items; ++i) {
@@ -315,7 +320,7 @@ __global__ void __launch_bounds__(kConvThreads) conv3_wgrad_kernel(const __grid_
             uint32_t t = tile;
             const uint32_t tx = t % tiles_x; t /= tiles_x;
             const uint32_t ty = t % tiles_y; t /= tiles_y;
-            const int z = static_cast<int>(t % a.s.z), b = static_cast<int>(t / a.s.z);
+            const int z = static_cast<int>((t % tiles_z) * a.bz), b = static_cast<int>(t / tiles_z);
             const int x0 = static_cast<int>(tx * a.bx), y0 = static_cast<int>(ty * a.by);
             unsigned char* st = smem + s * L::stage_bytes;
             tc::mbar_expect_tx(&full[s], L::G * L::x_tile + L::y_bytes);
@@ -325,7 +330,7 @@ __global__ void __launch_bounds__(kConvThreads) conv3_wgrad_kernel(const __grid_
                     const int dz = tap / 9 - 1, dy = (tap / 3) % 3 - 1, dx = tap % 3 - 1;
                     tc::tma_load_5d(st + j * L::x_tile, &x_map, &full[s], 0, x0 + dx, y0 + dy, z + dz, b);
                 } else {  // missing taps of the last group: a box far outside the volume reads zeros
-                    tc::tma_load_5d(st + j * L::x_tile, &x_map, &full[s], 0, 0, 0, -64, 0);
+                    tc::tma_load_5d(st + j * L::x_tile, &x_map, &full[s], 0, 0, 0, -static_cast<int>(2 * a.bz + 64), 0);
                 }
             }
             tc::tma_load_5d(st + L::G * L::x_tile, &dy_map, &full[s], 0, x0, y0, z, b);
@@ -387,9 +392,9 @@ __global__ void wgrad_reduce_kernel(const float* __restrict__ partial, uint32_t 
 }
 
 uint32_t wgrad_ctas(const VolumeShape& s) {
-    uint32_t bx, by;
-    if (!conv_tile(s, bx, by)) return 0;
-    const uint64_t tiles = static_cast<uint64_t>(s.batch) * s.z * (s.y / by) * (s.x / bx);
+    uint32_t bx, by, bz;
+    if (!conv_tile(s, bx, by, bz)) return 0;
+    const uint64_t tiles = static_cast<uint64_t>(s.batch) * (s.z / bz) * (s.y / by) * (s.x / bx);
     return static_cast<uint32_t>(tiles < 148 ? tiles : 148);
 }
 
@@ -401,16 +406,16 @@ template <int CIN, int COUT>
 XsStatus launch_wgrad(cudaStream_t st, const VolumeShape& s, const __nv_bfloat16* x, const __nv_bfloat16* dy, float* partial, float* dw,
                       bool accumulate, int* error) {
     using L = WgradLayout<CIN, COUT>;
-    uint32_t bx, by;
-    if (!conv_tile(s, bx, by)) return XS_INVALID_ARGUMENT;
+    uint32_t bx, by, bz;
+    if (!conv_tile(s, bx, by, bz)) return XS_INVALID_ARGUMENT;
     CUtensorMap xm, ym;
-    if (!make_activation_map(&xm, x, s, CIN, bx, by) || !make_activation_map(&ym, dy, s, COUT, bx, by)) return XS_CUDA_ERROR;
+    if (!make_activation_map(&xm, x, s, CIN, bx, by, bz) || !make_activation_map(&ym, dy, s, COUT, bx, by, bz)) return XS_CUDA_ERROR;
     static DeviceOnce configured;
     if (!configured.run([] { return cudaFuncSetAttribute(conv3_wgrad_kernel<CIN, COUT>, cudaFuncAttributeMaxDynamicSharedMemorySize, L::total); }))
         return XS_CUDA_ERROR;
-    const uint32_t tiles = static_cast<uint32_t>(static_cast<uint64_t>(s.batch) * s.z * (s.y / by) * (s.x / bx));
+    const uint32_t tiles = static_cast<uint32_t>(static_cast<uint64_t>(s.batch) * (s.z / bz) * (s.y / by) * (s.x / bx));
     const uint32_t ctas = wgrad_ctas(s);
-    WgradArgs args{s, bx, by, tiles, partial, error};
+    WgradArgs args{s, bx, by, bz, tiles, partial, error};
     conv3_wgrad_kernel<CIN, COUT><<<dim3(ctas, L::sets), kConvThreads, L::total, st>>>(xm, ym, args);
     if (check_launch() != XS_OK) return XS_CUDA_ERROR;
     const uint32_t count = 27u * CIN * COUT;

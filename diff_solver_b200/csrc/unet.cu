@@ -616,8 +616,8 @@ XsStatus refresh_weights(WarmStartNet& n, cudaStream_t st, bool update, float lr
 bool valid_net_shape(uint32_t nx, uint32_t ny, uint32_t nz) {
     if (nx % 8 || ny % 8 || nz % 8 || nx == 0 || ny == 0 || nz == 0) return false;
     for (int l = 0; l < 4; ++l) {
-        uint32_t bx, by;
-        if (!conv_tile(VolumeShape{nx >> l, ny >> l, nz >> l, 1}, bx, by)) return false;
+        uint32_t bx, by, bz;
+        if (!conv_tile(VolumeShape{nx >> l, ny >> l, nz >> l, 1}, bx, by, bz)) return false;
     }
     return true;
 }

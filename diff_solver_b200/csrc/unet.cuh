@@ -14,9 +14,10 @@ struct VolumeShape {
 };
 
 // Output tile of the convolutions: 128 voxels = bx * by of one x-y plane.
-bool conv_tile(const VolumeShape& s, uint32_t& bx, uint32_t& by);
+bool conv_tile(const VolumeShape& s, uint32_t& bx, uint32_t& by, uint32_t& bz);
 
-bool make_activation_map(CUtensorMap* map, const void* base, const VolumeShape& s, uint32_t channels, uint32_t bx, uint32_t by);
+bool make_activation_map(CUtensorMap* map, const void* base, const VolumeShape& s, uint32_t channels, uint32_t bx, uint32_t by,
+                         uint32_t bz);
 bool make_weight_map(CUtensorMap* map, const void* base, uint32_t rows, uint32_t cols);
 
 // out = act(conv3x3x3(in, w) + bias); w is [27][cout][cin] BF16.

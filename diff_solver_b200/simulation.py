@@ -25,6 +25,7 @@ import time
 from dataclasses import dataclass
 from typing import Optional, Tuple
 
+import numpy as np
 import torch
 
 from . import _native as N
@@ -105,7 +106,7 @@ def write_control(ctx, control, step: int, o: ForwardSimulationOptions) -> None:
         ctx.stream_handle, ctx.native.grid, int(step), float(o.pulse_period), _vec3(o.left_source_center), _vec3(o.right_source_center),
         float(o.source_radius), float(o.density_source_rate), float(o.temperature_source_rate), _vec3(o.left_acceleration),
         _vec3(o.right_acceleration), C.c_void_p(c.density_source.values.data_ptr()), C.c_void_p(c.temperature_source.values.data_ptr()),
-        N.vec(c.external_acceleration.components())))
+        N.vec([c.external_acceleration.x.values, c.external_acceleration.y.values, c.external_acceleration.z.values])))
 
 
 def reduce_metrics(ctx, state, step_cache, metrics: torch.Tensor) -> None:
@@ -185,18 +186,21 @@ class ForwardSimulation:
             ctx.synchronize()
         self.current_state, self._next_state = self._next_state, self.current_state
         m = self.metrics
+        # the reference's options are FP32 (simulation.ixx:11-12): the metrics
+        # use those values widened to FP64
+        dt, h = float(np.float32(o.time_step)), float(np.float32(o.cell_size))
         m.step += 1
-        m.physical_time = m.step * o.time_step
+        m.physical_time = m.step * dt
         if values is None:
             return
         ms = (time.perf_counter() - begin) * 1e3
         previous = m.step - 1
         cells = float(o.resolution[0] * o.resolution[1] * o.resolution[2])
-        m.density_mass = values[0] * o.cell_size * o.cell_size * o.cell_size
+        m.density_mass = values[0] * h * h * h
         m.density_maximum = values[1]
         m.temperature_maximum = values[2]
         m.maximum_velocity = values[3]
-        m.cfl = values[3] * o.time_step / o.cell_size
+        m.cfl = values[3] * dt / h
         m.pre_projection_divergence_rms = (values[4] / cells) ** 0.5
         m.post_projection_divergence_rms = (values[5] / cells) ** 0.5
         m.divergence_ratio = m.post_projection_divergence_rms / m.pre_projection_divergence_rms if m.pre_projection_divergence_rms else 0.0

@@ -142,10 +142,13 @@ def _seed(trajectory_adjoint, step):
 
 
 def vjp(model, context, trajectory: Trajectory, controls: Sequence, parameters,
-        trajectory_adjoint: Union[Sequence, Dict[int, object]]) -> GradientResult:
+        trajectory_adjoint: Union[Sequence, Dict[int, object]], after_step=None) -> GradientResult:
     """solver.ixx:115-150.  ``trajectory_adjoint`` holds one state adjoint per
     state (T+1 entries, as in the reference); it may also be a dict
-    {step: adjoint} or contain None for steps without a seed."""
+    {step: adjoint} or contain None for steps without a seed.  ``after_step``
+    (an addition, optional) is called with the step index right after that
+    step's vjp_step has been enqueued (for instance to copy the adjoint
+    solve's statistics without synchronising)."""
     T = len(controls)
     result = GradientResult(initial_state=model.allocate_state_adjoint(context),
                             controls=[model.allocate_control_adjoint(context) for _ in range(T)],
@@ -173,6 +176,8 @@ def vjp(model, context, trajectory: Trajectory, controls: Sequence, parameters,
             state, nxt, cache = seg_states[step - start], seg_states[step - start + 1], seg_caches[step - start]
         model.zero_state_adjoint(spare, context)
         model.vjp_step(state, controls[step], parameters, nxt, cache, running, spare, result.controls[step], result.parameters, context)
+        if after_step is not None:
+            after_step(step)
         seed = _seed(trajectory_adjoint, step)
         if seed is not None:
             model.accumulate_state_adjoint(seed, spare, context)

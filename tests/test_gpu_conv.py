@@ -18,7 +18,7 @@ def reference_conv(x, w, bias, relu):
 
 
 @pytest.mark.parametrize("cin,cout,shape", [(c, d, s) for (c, d), s in itertools.product(
-    [(16, 16), (16, 32), (32, 64), (64, 64), (64, 16), (32, 32)], [(16, 16, 6), (128, 2, 3)])])
+    [(16, 16), (16, 32), (32, 64), (64, 64), (64, 16), (32, 32)], [(16, 16, 6), (128, 2, 3), (8, 8, 6), (4, 8, 8)])])
 def test_conv_matches_torch(cuda, cin, cout, shape):
     import torch
     from diff_solver_b200 import _native as N
@@ -44,7 +44,9 @@ def test_conv_matches_torch(cuda, cin, cout, shape):
 
 @pytest.mark.parametrize("cin,cout,shape,batch", [
     (16, 16, (16, 16, 6), 2), (16, 32, (128, 2, 3), 1), (32, 64, (16, 16, 4), 2), (64, 64, (32, 8, 5), 1),
-    (64, 16, (16, 8, 7), 2), (32, 32, (64, 4, 3), 3), (64, 32, (16, 16, 16), 1)])
+    (64, 16, (16, 8, 7), 2), (32, 32, (64, 4, 3), 3), (64, 32, (16, 16, 16), 1),
+    # volumes whose x-y planes hold fewer than 128 voxels: tiles span several z planes
+    (16, 16, (8, 8, 6), 2), (32, 64, (4, 8, 8), 1), (64, 64, (8, 8, 4), 2)])
 def test_conv_gradients_match_torch(cuda, cin, cout, shape, batch):
     """Weight gradient (tcgen05, MN-major operands) and input gradient (the
     forward kernel with flipped, transposed weights) against autograd."""
