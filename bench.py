@@ -419,7 +419,7 @@ def load_network(args, shape):
     if not os.path.exists(args.weights):
         raise FileNotFoundError(f"{args.weights} is missing: train it with python -m diff_solver_b200.train_warm_start")
     # trained at 128^3, applied fully convolutionally on the grid restricted
-    # x network_factor (2 by default)
+    # x network_factor (4 by default)
     f = args.network_factor
     network = WarmStartNetwork(tuple(s // f for s in shape), factor=f)
     network.load(args.weights)
@@ -551,6 +551,7 @@ def adjoint_record(args, shape, network, start_state, window=40, checkpoint=8):
             "adjoint_iterations_per_step": [s.iterations for s in per_step],
             "adjoint_coarse_iterations_per_step": [s.coarse_iterations for s in per_step],
             "adjoint_start_used_per_step": [s.warm_start_used for s in per_step],
+            "adjoint_initial_residual_per_step": [s.initial_residual for s in per_step],
             "bytes_rule": "reverse_step_bytes(N, F, forward PCG iterations, adjoint PCG iterations)", "_n": n, "_f": faces}
 
 
@@ -738,7 +739,9 @@ def main():
     ap.add_argument("--cpu-budget", type=float, default=150.0, help="seconds after which the CPU legs stop adding steps")
     ap.add_argument("--weights", default=WEIGHTS, help="warm-start network parameters (.npz)")
     ap.add_argument("--coarsening", type=int, default=COARSENING, help="coarse-grid correction factor (0: off)")
-    ap.add_argument("--network-factor", type=int, default=2, help="restriction from the grid to the network's grid (1 or 2)")
+    # x4: the network runs on 64^3 for the 256^3 grid (8x cheaper than x2 for
+    # the same fine-iteration saving, measured: 141.9 against 119.4 steps/s)
+    ap.add_argument("--network-factor", type=int, default=4, help="restriction from the grid to the network's grid (1, 2 or 4)")
     ap.add_argument("--arms", default="", help="comma-separated subset of the arms, headline last (profiling; no roofline "
                                                "or CPU baseline without the plain arm)")
     args = ap.parse_args()

@@ -109,14 +109,21 @@ __device__ __forceinline__ void stage_face(float* __restrict__ s, const float* _
         return;
     }
 #pragma unroll 1
-    for (int k = lane + 32 * warp; k < S::kNodes; k += S::kThreads) {
-        const int bx = k % S::SX, row = k / S::SX;
-        const int x = o.x + bx, y = o.y + row % S::SY, z = o.z + row / S::SY;
-        if (static_cast<unsigned>(x) < static_cast<unsigned>(lx) && static_cast<unsigned>(y) < static_cast<unsigned>(ly) &&
-            static_cast<unsigned>(z) < static_cast<unsigned>(lz))
-            cp_async4(s + k, v + index32(x, y, z, ex, ey));
-        else
-            s[k] = load_face(v, A, x, y, z, g, b);
+    for (int r = 0; r < S::kRows / S::TY; ++r) {
+        const int row = warp + r * S::TY;
+        const int y = o.y + row % S::SY, z = o.z + row / S::SY;
+        const bool row_in = static_cast<unsigned>(y) < static_cast<unsigned>(ly) && static_cast<unsigned>(z) < static_cast<unsigned>(lz);
+        float* dst = s + row * S::SX;
+#pragma unroll
+        for (int half = 0; half < 2; ++half) {
+            const int bx = lane + 32 * half;
+            if (half == 1 && bx >= S::SX) break;
+            const int x = o.x + bx;
+            if (row_in && static_cast<unsigned>(x) < static_cast<unsigned>(lx))
+                cp_async4(dst + bx, v + index32(x, y, z, ex, ey));
+            else
+                dst[bx] = load_face(v, A, x, y, z, g, b);
+        }
     }
 }
 
@@ -137,14 +144,21 @@ __device__ __forceinline__ void stage_cells(float* __restrict__ s, const float* 
         return;
     }
 #pragma unroll 1
-    for (int k = lane + 32 * warp; k < S::kNodes; k += S::kThreads) {
-        const int bx = k % S::SX, row = k / S::SX;
-        const int x = o.x + bx, y = o.y + row % S::SY, z = o.z + row / S::SY;
-        if (static_cast<unsigned>(x) < static_cast<unsigned>(g.nx) && static_cast<unsigned>(y) < static_cast<unsigned>(g.ny) &&
-            static_cast<unsigned>(z) < static_cast<unsigned>(g.nz))
-            cp_async4(s + k, v + index32(x, y, z, g.nx, g.ny));
-        else
-            s[k] = load_scalar(v, x, y, z, g, b);
+    for (int r = 0; r < S::kRows / S::TY; ++r) {
+        const int row = warp + r * S::TY;
+        const int y = o.y + row % S::SY, z = o.z + row / S::SY;
+        const bool row_in = static_cast<unsigned>(y) < static_cast<unsigned>(g.ny) && static_cast<unsigned>(z) < static_cast<unsigned>(g.nz);
+        float* dst = s + row * S::SX;
+#pragma unroll
+        for (int half = 0; half < 2; ++half) {
+            const int bx = lane + 32 * half;
+            if (half == 1 && bx >= S::SX) break;
+            const int x = o.x + bx;
+            if (row_in && static_cast<unsigned>(x) < static_cast<unsigned>(g.nx))
+                cp_async4(dst + bx, v + index32(x, y, z, g.nx, g.ny));
+            else
+                dst[bx] = load_scalar(v, x, y, z, g, b);
+        }
     }
 }
 

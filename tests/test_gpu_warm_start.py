@@ -315,52 +315,66 @@ def test_galerkin_history_with_learned_guess(cuda):
 
 def test_trained_network_gain(cuda):
     """What the committed network (trained at 128^3 on 20k plume pairs) gains
-    in the benchmark's own pipeline: the 256^3 plume from rest, each forward
+    in the benchmark's own pipeline and window: the 256^3 plume spun up 180
+    steps from rest, then from that state 5 + 20 steps with each forward
     solve started from the ring of the last 5 solutions and the coarse-grid
-    step, with and without the network's correction step on top (network
-    applied on the grid restricted x2).  The network's step removes fine PCG
-    iterations (measured in the benchmark window, steps 185-205: 26.9 -> 24.2
-    per step).  At this grid its inference and line step cost more time than
-    those iterations (bench.py's history+coarse and learned+history+coarse
-    arms report both); this test asserts the iteration gain, the part the
-    network is responsible for, on steps 20-60 of the plume."""
+    step, with and without the network's correction step on top (network on
+    the grid restricted x4, as the benchmark runs it).  The network's step
+    removes fine PCG iterations there (measured: 8.6 -> 7.0 per step); on the
+    young plume (steps 20-60) the x4 network removes none.  Its restriction,
+    inference and line step cost more time than the iterations it saves
+    (bench.py's history+coarse and learned+history+coarse arms report both);
+    this test asserts the iteration gain, the part the network is
+    responsible for."""
     import torch
     from diff_solver_b200.data import plume_configuration
-    from diff_solver_b200.model import ExecutionMode, Model, fill_parameters
+    from diff_solver_b200.model import ExecutionMode, Model, fill_parameters, tensors_of
     from diff_solver_b200.warm_start import WarmStartNetwork
     weights = os.path.join(ROOT, "diff_solver_b200", "weights", "warm_start_128.npz")
     res = (256, 256, 256)
-    net = WarmStartNetwork((128, 128, 128), factor=2)
+    net = WarmStartNetwork((64, 64, 64), factor=4)
     net.load(weights)
-    iterations = {}
-    for name in ("classical", "learned"):
+
+    def model():
         cfg = plume_configuration(res)
         cfg.pressure_max_iterations = 20000
         cfg.warm_start_history = 5
         cfg.warm_start_coarsening = 2
         m = Model(cfg)
         ctx = m.allocate_context(ExecutionMode.forward)
+        return m, ctx, m.allocate_state(ctx), m.allocate_state(ctx), m.allocate_control(ctx), m.allocate_step_cache(ctx), \
+            fill_parameters(m.allocate_parameters(ctx), 0.0, -0.1, 0.5)
+
+    m, ctx, s, n, c, k, q = model()
+    g = torch.Generator(device="cuda").manual_seed(0)
+    for t in s.velocity.components():
+        t.uniform_(-0.01, 0.01, generator=g)
+    for _ in range(180):
+        m.forward_step(s, c, q, n, k, ctx)
+        s, n = n, s
+    spun = [t.clone() for t in tensors_of(s)]
+    del m, ctx, s, n, c, k, q
+    iterations = {}
+    for name in ("classical", "learned"):
+        m, ctx, s, n, c, k, q = model()
         if name == "learned":
             ctx.set_learned_warm_start(net)
-        s, n = m.allocate_state(ctx), m.allocate_state(ctx)
-        c, k = m.allocate_control(ctx), m.allocate_step_cache(ctx)
-        q = fill_parameters(m.allocate_parameters(ctx), 0.0, -0.1, 0.5)
-        g = torch.Generator(device="cuda").manual_seed(0)
-        for t in s.velocity.components():
-            t.uniform_(-0.01, 0.01, generator=g)
+        for d, src in zip(tensors_of(s), spun):
+            d.copy_(src)
         its = []
-        for _ in range(60):
+        for step in range(25):
             m.forward_step(s, c, q, n, k, ctx)
             s, n = n, s
             st = ctx.read_solve_stats()
             assert st["status"] == 0 and st["final_residual"] <= 1e-6, st
-            its.append(st["iterations"])
-        iterations[name] = float(np.mean(its[20:]))
-        del m, ctx, s, n, c, k
+            if step >= 5:
+                its.append(st["iterations"])
+        iterations[name] = float(np.mean(its))
+        del m, ctx, s, n, c, k, q
         torch.cuda.empty_cache()
     net.check()
     print(iterations)
-    assert iterations["learned"] <= 0.95 * iterations["classical"], iterations
+    assert iterations["learned"] <= 0.9 * iterations["classical"], iterations
 
 
 def test_learned_warm_start_inside_a_model_step(cuda):
