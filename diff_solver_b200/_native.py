@@ -137,6 +137,8 @@ SIGNATURES = {
     "xs_pressure_solve": (_S, [_V, _G, C.POINTER(XsPressureSolve), C.c_uint32, _V, XsScalarBoundary, _V, _V, _V]),
     "xs_read_solve_stats": (_S, [_V, _V, C.POINTER(XsSolveStats)]),
     "xs_solve_stats_offset": (C.c_size_t, []),
+    "xs_separable_solve_scratch_bytes": (C.c_size_t, []),
+    "xs_separable_solve": (_S, [_V, _G, XsScalarBoundary, C.c_uint32, _V, _V, _V]),
     "xs_pressure_solve_static": (_S, [_V, _G, C.POINTER(XsPressureSolve), C.c_uint32, _V, XsScalarBoundary, _V, _V,
                                       C.POINTER(XsSolveStats)]),
     "xs_smoke_build_domain": (_S, [_V, _G, XsScalarBoundary, _V, C.c_uint32, _V, XsVector, _V, _V, C.POINTER(C.c_uint32)]),

@@ -150,7 +150,10 @@ __global__ void advect_velocity_vjp_kernel(const __grid_constant__ Grid g, uint6
 // box node is added to global memory once at the end (instead of 56 global
 // atomics per face).  The same products as the general kernels; only the
 // order of the FP64 additions differs.
-using AdjointTile = tile::Shape<32, 4, 4>;
+// Halo 1: the box holds every stencil of traces shorter than half a cell per
+// step (longer ones scatter to global memory); the smaller boxes give four
+// CTAs per SM.
+using AdjointTile = tile::Shape<32, 4, 4, 1>;
 constexpr size_t kVelocityVjpSmem = 3 * AdjointTile::kNodes * (sizeof(double) + sizeof(float));
 constexpr size_t kScalarVjpSmem = 5 * AdjointTile::kNodes * (sizeof(double) + sizeof(float));
 
@@ -217,7 +220,7 @@ __device__ __forceinline__ void advect_velocity_vjp_tile_face(int x, int y, int 
     staged_trace_adjoint<A>(mid, m, der, src.gradient, o, li, acc, org, k, g, vb, ua, false);
 }
 
-__global__ void __launch_bounds__(AdjointTile::kThreads, 2) advect_velocity_vjp_tile_kernel(const __grid_constant__ Grid g, XsVector u, const __grid_constant__ XsVelocityBoundary vb,
+__global__ void __launch_bounds__(AdjointTile::kThreads, 4) advect_velocity_vjp_tile_kernel(const __grid_constant__ Grid g, XsVector u, const __grid_constant__ XsVelocityBoundary vb,
                                                                                           XsAdjointVector oa, XsAdjointVector ua) {
     using S = AdjointTile;
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -279,7 +282,7 @@ __global__ void advect_velocity_vjp_upper_kernel(const __grid_constant__ Grid g,
 // Density and temperature together (operators.cu:537-561 twice on one
 // trace): u and both sources staged, the velocity and both source adjoints
 // accumulated in the box.
-__global__ void __launch_bounds__(AdjointTile::kThreads, 1) advect_scalar_vjp_tile_kernel(const __grid_constant__ Grid g, const float* __restrict__ src,
+__global__ void __launch_bounds__(AdjointTile::kThreads, 3) advect_scalar_vjp_tile_kernel(const __grid_constant__ Grid g, const float* __restrict__ src,
                                                                                         const __grid_constant__ XsScalarBoundary sb, const double* __restrict__ oa,
                                                                                         double* __restrict__ sa, const float* __restrict__ src2,
                                                                                         const __grid_constant__ XsScalarBoundary sb2, const double* __restrict__ oa2,
@@ -554,19 +557,18 @@ XsStatus projection_vjp(cudaStream_t st, const Grid& g, const XsPressureSolve& s
         const bool ring = history && history->history > 0;
         const bool coarse = ring && history->coarsening != 0 && mask == nullptr;
         if (ring) {
-            // successive adjoint solves of a reverse pass are close: Galerkin
+            // successive adjoint solves of a reverse pass are related: Galerkin
             // start from the ring of previous adjoint solutions, then (with
-            // coarsening) one energy-optimal step along the coarse-grid
-            // correction of its residual, as in the forward solve
+            // coarsening) kAdjointStartCycles rounds of sweeps and an
+            // energy-optimal step along the coarse-grid correction of the
+            // residual (the forward solve takes one)
             const WarmHistory& h = *history;
             if ((s = galerkin_combine(st, g, anchor, mask, pb, h, true, nullptr, 0, nullptr, h.ring_start, pa)) != XS_OK) return s;
             adj.initial_guess = h.ring_start;
             if (coarse) {
-                if ((s = jacobi_sweeps(st, g, anchor, mask, pb, nullptr, pa, h.ring_start, h.extra_product, h.start)) != XS_OK) return s;
-                if ((s = start_residual(st, g, anchor, mask, pb, nullptr, h.start, h.residual, pa)) != XS_OK) return s;
-                if ((s = coarse_correction(st, g, anchor, pb, h, h.residual)) != XS_OK) return s;
-                if ((s = line_step(st, g, anchor, mask, pb, h, h.correction, h.start, h.residual, h.start)) != XS_OK) return s;
-                adj.initial_guess = h.start;
+                const float* x = nullptr;
+                if ((s = coarse_cycles(st, g, anchor, pb, h, nullptr, pa, kAdjointStartCycles, &x)) != XS_OK) return s;
+                adj.initial_guess = x;
             }
         }
         s = solve_pressure(st, g, adj, anchor, mask, pb, nullptr, pa, nullptr, ra, workspace, nullptr);

@@ -3,9 +3,10 @@
 //
 // A CTA owns a box of TX x TY x TZ output positions (faces or cells with the
 // same integer coordinates).  Every trilinear stencil those positions reach
-// lies, for traces shorter than about one cell per step, within the
-// positions' box widened by kHalo nodes on every side; each field the kernel
-// samples is copied once into shared memory over that box.  A staged node
+// lies within the positions' box widened by H nodes on every side when the
+// trace is shorter than H - 1/2 cells per step (a staggered component is
+// sampled half a cell off its nodes); each field the kernel samples is
+// copied once into shared memory over that box.  A staged node
 // holds exactly the value the boundary-aware loads of the reference return
 // for its integer coordinates (load_face / load_scalar: operators.cu:115-134):
 // a node beyond the domain takes the fixed boundary value or its clamped /
@@ -30,18 +31,16 @@
 namespace xs {
 namespace tile {
 
-constexpr int kHalo = 2;
-
-template <int TX_, int TY_, int TZ_>
+template <int TX_, int TY_, int TZ_, int H_>
 struct Shape {
-    static constexpr int TX = TX_, TY = TY_, TZ = TZ_;
+    static constexpr int TX = TX_, TY = TY_, TZ = TZ_, kHalo = H_;
     static constexpr int kThreads = TX * TY;  // one thread per (x, y), looping over z
     static constexpr int SX = TX + 2 * kHalo, SY = TY + 2 * kHalo, SZ = TZ + 2 * kHalo;
     static constexpr int kNodes = SX * SY * SZ;
     static constexpr int kRows = SY * SZ;
+    static constexpr int kRowPasses = (kRows + TY - 1) / TY;  // box rows per warp (the last pass partial)
     static constexpr int stride(int axis) { return axis == 0 ? 1 : (axis == 1 ? SX : SX * SY); }
     static_assert(TX == 32 && SX <= 64, "a box row is staged by one warp in two passes");
-    static_assert(kRows % TY == 0, "every warp stages the same number of box rows");
 };
 
 // Global coordinates of box node (0, 0, 0).
@@ -51,14 +50,14 @@ struct Origin {
 
 template <class S>
 __device__ __forceinline__ Origin tile_origin() {
-    return Origin{static_cast<int>(blockIdx.x) * S::TX - kHalo, static_cast<int>(blockIdx.y) * S::TY - kHalo,
-                  static_cast<int>(blockIdx.z) * S::TZ - kHalo};
+    return Origin{static_cast<int>(blockIdx.x) * S::TX - S::kHalo, static_cast<int>(blockIdx.y) * S::TY - S::kHalo,
+                  static_cast<int>(blockIdx.z) * S::TZ - S::kHalo};
 }
 
 // Box offset of the position handled by this thread at z step kz.
 template <class S>
 __device__ __forceinline__ int local_index(int kz) {
-    return (static_cast<int>(threadIdx.x) + kHalo) + S::SX * ((static_cast<int>(threadIdx.y) + kHalo) + S::SY * (kz + kHalo));
+    return (static_cast<int>(threadIdx.x) + S::kHalo) + S::SX * ((static_cast<int>(threadIdx.y) + S::kHalo) + S::SY * (kz + S::kHalo));
 }
 
 // Whether the box lies inside an array of the given extents (then every node
@@ -99,8 +98,9 @@ __device__ __forceinline__ void stage_face(float* __restrict__ s, const float* _
     const int lane = threadIdx.x, warp = threadIdx.y;
     if (box_inside<S>(o, lx, ly, lz)) {
 #pragma unroll
-        for (int r = 0; r < S::kRows / S::TY; ++r) {
+        for (int r = 0; r < S::kRowPasses; ++r) {
             const int row = warp + r * S::TY;
+            if (S::kRows % S::TY != 0 && row >= S::kRows) break;
             const float* src = v + index32(o.x, o.y + row % S::SY, o.z + row / S::SY, ex, ey);
             float* dst = s + row * S::SX;
             cp_async4(dst + lane, src + lane);
@@ -109,8 +109,7 @@ __device__ __forceinline__ void stage_face(float* __restrict__ s, const float* _
         return;
     }
 #pragma unroll 1
-    for (int r = 0; r < S::kRows / S::TY; ++r) {
-        const int row = warp + r * S::TY;
+    for (int row = warp; row < S::kRows; row += S::TY) {
         const int y = o.y + row % S::SY, z = o.z + row / S::SY;
         const bool row_in = static_cast<unsigned>(y) < static_cast<unsigned>(ly) && static_cast<unsigned>(z) < static_cast<unsigned>(lz);
         float* dst = s + row * S::SX;
@@ -134,8 +133,9 @@ __device__ __forceinline__ void stage_cells(float* __restrict__ s, const float* 
     const int lane = threadIdx.x, warp = threadIdx.y;
     if (box_inside<S>(o, g.nx, g.ny, g.nz)) {
 #pragma unroll
-        for (int r = 0; r < S::kRows / S::TY; ++r) {
+        for (int r = 0; r < S::kRowPasses; ++r) {
             const int row = warp + r * S::TY;
+            if (S::kRows % S::TY != 0 && row >= S::kRows) break;
             const float* src = v + index32(o.x, o.y + row % S::SY, o.z + row / S::SY, g.nx, g.ny);
             float* dst = s + row * S::SX;
             cp_async4(dst + lane, src + lane);
@@ -144,8 +144,7 @@ __device__ __forceinline__ void stage_cells(float* __restrict__ s, const float* 
         return;
     }
 #pragma unroll 1
-    for (int r = 0; r < S::kRows / S::TY; ++r) {
-        const int row = warp + r * S::TY;
+    for (int row = warp; row < S::kRows; row += S::TY) {
         const int y = o.y + row % S::SY, z = o.z + row / S::SY;
         const bool row_in = static_cast<unsigned>(y) < static_cast<unsigned>(g.ny) && static_cast<unsigned>(z) < static_cast<unsigned>(g.nz);
         float* dst = s + row * S::SX;
@@ -342,6 +341,12 @@ static __device__ __noinline__ void global_scalar_scatter(double* __restrict__ v
     scatter_scalar(v, p, adj, g, b);
 }
 
+// FP64 add to a shared-memory accumulator (a shared-window address: no
+// generic-address resolution per access).
+__device__ __forceinline__ void shared_add(double* p, double v) {
+    asm volatile("red.shared.add.f64 [%0], %1;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(p))), "d"(v) : "memory");
+}
+
 template <class S>
 __device__ __forceinline__ void box_scatter(double* __restrict__ acc, int c, double adj, float tx, float ty, float tz) {
     const double wx[2] = {1.0 - tx, static_cast<double>(tx)};
@@ -352,7 +357,7 @@ __device__ __forceinline__ void box_scatter(double* __restrict__ acc, int c, dou
 #pragma unroll
         for (int dy = 0; dy < 2; ++dy)
 #pragma unroll
-            for (int dx = 0; dx < 2; ++dx) atomicAdd(acc + c + dx + S::SX * (dy + S::SY * dz), adj * wx[dx] * wy[dy] * wz[dz]);
+            for (int dx = 0; dx < 2; ++dx) shared_add(acc + c + dx + S::SX * (dy + S::SY * dz), adj * wx[dx] * wy[dy] * wz[dz]);
 }
 
 template <class S, int B>
@@ -390,16 +395,16 @@ template <class S, int A, int B>
 __device__ __forceinline__ void face_start_scatter(double* __restrict__ acc, int li, double adj) {
     if (adj == 0.0) return;
     if (A == B) {
-        atomicAdd(acc + li, adj);
+        shared_add(acc + li, adj);
         return;
     }
     constexpr int lo = S::stride(A < B ? A : B), hi = S::stride(A < B ? B : A);
     double* c = acc + li - S::stride(A);
     const double w = adj * 0.5 * 0.5;
-    atomicAdd(c, w);
-    atomicAdd(c + lo, w);
-    atomicAdd(c + hi, w);
-    atomicAdd(c + lo + hi, w);
+    shared_add(c, w);
+    shared_add(c + lo, w);
+    shared_add(c + hi, w);
+    shared_add(c + lo + hi, w);
 }
 
 // Transpose of cell_start_component.
@@ -407,8 +412,8 @@ template <class S, int B>
 __device__ __forceinline__ void cell_start_scatter(double* __restrict__ acc, int li, double adj) {
     if (adj == 0.0) return;
     const double w = adj * 0.5;
-    atomicAdd(acc + li, w);
-    atomicAdd(acc + li + S::stride(B), w);
+    shared_add(acc + li, w);
+    shared_add(acc + li + S::stride(B), w);
 }
 
 template <class S>

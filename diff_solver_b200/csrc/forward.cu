@@ -235,13 +235,17 @@ __global__ void __launch_bounds__(kBlock, 4) advect_constrain_kernel(const __gri
 // coordinate along its own axis is below the grid size.  The faces at the
 // upper end of their axis (x = nx for u, ...) are left to the remainder
 // kernel below.  Bit-identical to advect_constrain_kernel.
-using ForwardTile = tile::Shape<32, 8, 4>;
+// Halo 1: every stencil of traces shorter than half a cell per step (the
+// plume benchmark's CFL number stays near 0.06); longer traces read the
+// stencils outside the box from global memory, same values.  Against halo 2
+// (traces up to 1.5 cells): 41 % fewer staged nodes, 3-4 % more steps/s at
+// 256^3.
+using ForwardTile = tile::Shape<32, 8, 4, 1>;
 
-template <int A, bool kConstrain>
+template <class S, int A, bool kConstrain>
 __device__ __forceinline__ void advect_constrain_tile_face(int x, int y, int z, int li, const tile::StagedVelocity& sv, const tile::Origin& o,
                                                            const tile::TileConsts& k, const Grid& g, const XsVelocityBoundary& b,
                                                            float* __restrict__ out) {
-    using S = ForwardTile;
     float v;
     if (!kConstrain || !constrained_boundary(A, x, y, z, g, b, v)) {
         const Vec3 s = face_position(A, x, y, z, g);
@@ -253,9 +257,8 @@ __device__ __forceinline__ void advect_constrain_tile_face(int x, int y, int z, 
 }
 
 // kConstrain = false: the raw advected field of advect_velocity_kernel.
-template <bool kConstrain>
-__global__ void __launch_bounds__(ForwardTile::kThreads, 4) advect_constrain_tile_kernel(const __grid_constant__ Grid g, XsVector u, const __grid_constant__ XsVelocityBoundary b, XsVector out) {
-    using S = ForwardTile;
+template <class S, bool kConstrain>
+__global__ void __launch_bounds__(S::kThreads, 4) advect_constrain_tile_kernel(const __grid_constant__ Grid g, XsVector u, const __grid_constant__ XsVelocityBoundary b, XsVector out) {
     __shared__ float box[3][S::kNodes];
     const tile::Origin o = tile::tile_origin<S>();
     tile::stage_face<S, 0>(box[0], u.x, o, g, b);
@@ -273,9 +276,9 @@ __global__ void __launch_bounds__(ForwardTile::kThreads, 4) advect_constrain_til
         const int z = static_cast<int>(blockIdx.z) * S::TZ + kz;
         if (z >= g.nz) break;
         const int li = tile::local_index<S>(kz);
-        advect_constrain_tile_face<0, kConstrain>(x, y, z, li, sv, o, k, g, b, out.x);
-        advect_constrain_tile_face<1, kConstrain>(x, y, z, li, sv, o, k, g, b, out.y);
-        advect_constrain_tile_face<2, kConstrain>(x, y, z, li, sv, o, k, g, b, out.z);
+        advect_constrain_tile_face<S, 0, kConstrain>(x, y, z, li, sv, o, k, g, b, out.x);
+        advect_constrain_tile_face<S, 1, kConstrain>(x, y, z, li, sv, o, k, g, b, out.y);
+        advect_constrain_tile_face<S, 2, kConstrain>(x, y, z, li, sv, o, k, g, b, out.z);
     }
 }
 
@@ -307,7 +310,7 @@ __global__ void advect_constrain_upper_kernel(const __grid_constant__ Grid g, co
 template <bool kConstrain>
 XsStatus launch_advect_tiled(cudaStream_t st, const Grid& g, const XsVector& col, const XsVector& u, const XsVelocityBoundary& b,
                              const XsVector& out) {
-    advect_constrain_tile_kernel<kConstrain><<<tile::tile_grid<ForwardTile>(g), tile::tile_block<ForwardTile>(), 0, st>>>(g, u, b, out);
+    advect_constrain_tile_kernel<ForwardTile, kConstrain><<<tile::tile_grid<ForwardTile>(g), tile::tile_block<ForwardTile>(), 0, st>>>(g, u, b, out);
     XsStatus s = check_launch();
     if (s != XS_OK) return s;
     const uint64_t upper = static_cast<uint64_t>(g.ny) * g.nz + static_cast<uint64_t>(g.nx) * g.nz + static_cast<uint64_t>(g.nx) * g.ny;
@@ -354,15 +357,15 @@ __global__ void __launch_bounds__(kBlock, 4) advect_scalar_pair_kernel(const __g
 // temperature are staged over the box (5 boxes, dynamic shared memory).
 // Bit-identical to advect_scalar_pair_kernel; kFields = 1 advects one field
 // (advect_scalar_kernel).
-constexpr size_t scalar_tile_smem(int fields) { return (3 + fields) * sizeof(float) * ForwardTile::kNodes; }
+template <class S>
+constexpr size_t scalar_tile_smem(int fields) { return (3 + fields) * sizeof(float) * S::kNodes; }
 
-template <int kFields>
-__global__ void __launch_bounds__(ForwardTile::kThreads, 3) advect_scalar_pair_tile_kernel(const __grid_constant__ Grid g, const float* __restrict__ src_rho,
+template <class S, int kFields>
+__global__ void __launch_bounds__(S::kThreads, 3) advect_scalar_pair_tile_kernel(const __grid_constant__ Grid g, const float* __restrict__ src_rho,
                                                                                       const float* __restrict__ src_temp, XsVector u,
                                                                                       const __grid_constant__ XsScalarBoundary rb, const __grid_constant__ XsScalarBoundary tb,
                                                                                       const __grid_constant__ XsVelocityBoundary vb, float* __restrict__ out_rho,
                                                                                       float* __restrict__ out_temp) {
-    using S = ForwardTile;
     extern __shared__ float smem[];
     float* box[5] = {smem, smem + S::kNodes, smem + 2 * S::kNodes, smem + 3 * S::kNodes, smem + 4 * S::kNodes};
     const tile::Origin o = tile::tile_origin<S>();
@@ -547,19 +550,26 @@ __global__ void __launch_bounds__(256) project64_faces_kernel(const __grid_const
 }
 
 // ------------------------------------------------------------ launchers
+template <class S, int kFields>
+XsStatus launch_scalar_tiled_shape(cudaStream_t st, const Grid& g, const float* src_rho, const float* src_temp, const XsVector& u,
+                                   const XsScalarBoundary& rb, const XsScalarBoundary& tb, const XsVelocityBoundary& vb, float* out_rho,
+                                   float* out_temp) {
+    static DeviceOnce configured;
+    if (!configured.run([] {
+            return cudaFuncSetAttribute(advect_scalar_pair_tile_kernel<S, kFields>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                        static_cast<int>(scalar_tile_smem<S>(kFields)));
+        }))
+        return XS_CUDA_ERROR;
+    advect_scalar_pair_tile_kernel<S, kFields><<<tile::tile_grid<S>(g), tile::tile_block<S>(), scalar_tile_smem<S>(kFields), st>>>(
+        g, src_rho, src_temp, u, rb, tb, vb, out_rho, out_temp);
+    return check_launch();
+}
+
 template <int kFields>
 XsStatus launch_scalar_tiled(cudaStream_t st, const Grid& g, const float* src_rho, const float* src_temp, const XsVector& u,
                              const XsScalarBoundary& rb, const XsScalarBoundary& tb, const XsVelocityBoundary& vb, float* out_rho,
                              float* out_temp) {
-    static DeviceOnce configured;
-    if (!configured.run([] {
-            return cudaFuncSetAttribute(advect_scalar_pair_tile_kernel<kFields>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                        static_cast<int>(scalar_tile_smem(kFields)));
-        }))
-        return XS_CUDA_ERROR;
-    advect_scalar_pair_tile_kernel<kFields><<<tile::tile_grid<ForwardTile>(g), tile::tile_block<ForwardTile>(), scalar_tile_smem(kFields), st>>>(
-        g, src_rho, src_temp, u, rb, tb, vb, out_rho, out_temp);
-    return check_launch();
+    return launch_scalar_tiled_shape<ForwardTile, kFields>(st, g, src_rho, src_temp, u, rb, tb, vb, out_rho, out_temp);
 }
 
 InflowSet make_inflows(const XsInflow* inflows, uint32_t count) {

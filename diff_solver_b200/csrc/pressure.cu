@@ -1497,6 +1497,8 @@ uint32_t second_coarsening(const Grid& coarse) {
     return 0;
 }
 
+static bool spectral_fits(const Grid& c) { return c.nx <= kSpectralMax && c.ny <= kSpectralMax && c.nz <= kSpectralMax; }
+
 size_t warm_history_bytes(const Grid& g, uint32_t history, uint32_t coarsening) {
     if (history == 0) return 0;
     const size_t n = cell_count(g);
@@ -1506,6 +1508,7 @@ size_t warm_history_bytes(const Grid& g, uint32_t history, uint32_t coarsening) 
     if (coarse_grid(g, coarsening, c)) {
         const size_t nc = cell_count(c);
         bytes += align_up(n * 4, 256) + align_up(nc * 8, 256) + align_up(nc * 4, 256) + align_up(pressure_workspace_bytes(c), 256);
+        if (spectral_fits(c)) bytes += align_up(4 * 3 * kSpectralMax * kSpectralMax, 256) + align_up(4 * 3 * kSpectralMax, 256);
         const uint32_t f2 = second_coarsening(c);
         if (f2 && coarse_grid(c, f2, c2)) {
             const size_t nc2 = cell_count(c2);
@@ -1545,6 +1548,10 @@ WarmHistory carve_warm_history(void* base, const Grid& g, uint32_t history, uint
         h.coarse_rhs = reinterpret_cast<double*>(take(nc * 8));
         h.coarse_solution = reinterpret_cast<float*>(take(nc * 4));
         h.coarse_solver = take(pressure_workspace_bytes(h.coarse));
+        if (spectral_fits(h.coarse)) {
+            h.spectral_basis = reinterpret_cast<float*>(take(4 * 3 * kSpectralMax * kSpectralMax));
+            h.spectral_eigen = reinterpret_cast<float*>(take(4 * 3 * kSpectralMax));
+        }
         const uint32_t f2 = second_coarsening(h.coarse);
         if (f2 && coarse_grid(h.coarse, f2, h.coarsest)) {
             const size_t nc2 = cell_count(h.coarsest);
@@ -1689,10 +1696,10 @@ uint32_t coarse_anchor(const Grid& g, uint32_t f, const Grid& c, uint32_t anchor
     return static_cast<uint32_t>(ax / f + static_cast<uint64_t>(c.nx) * (ay / f + static_cast<uint64_t>(c.ny) * (az / f)));
 }
 
-XsPressureSolve coarse_solve_settings(const float* guess) {
+XsPressureSolve coarse_solve_settings(const float* guess, uint32_t max_iterations = kCoarseMaxIterations) {
     XsPressureSolve cs{};
     cs.kind = XS_SOLVER_JACOBI_PCG;
-    cs.max_iterations = kCoarseMaxIterations;
+    cs.max_iterations = max_iterations;
     cs.tolerance = kCoarseTolerance;
     cs.initial_guess = guess;
     cs.scale_guess = 0u;
@@ -1701,13 +1708,22 @@ XsPressureSolve coarse_solve_settings(const float* guess) {
 
 }  // namespace
 
-XsStatus coarse_correction(cudaStream_t st, const Grid& g, uint32_t anchor, const XsScalarBoundary& pb, const WarmHistory& h, const float* r) {
+XsStatus coarse_correction(cudaStream_t st, const Grid& g, uint32_t anchor, const XsScalarBoundary& pb, const WarmHistory& h, const float* r,
+                           uint32_t max_iterations) {
     if (h.coarsening < 2 || !h.correction || !h.coarse_rhs || !h.coarse_solution || !h.coarse_solver || !r) return XS_INVALID_ARGUMENT;
     const Grid& c = h.coarse;
     const uint32_t f = h.coarsening;
     XsStatus s = restrict_to(st, g, c, f, r, h.coarse_rhs);
     if (s != XS_OK) return s;
     const uint32_t anchor_c = coarse_anchor(g, f, c, anchor);
+    SpectralAxes ax;
+    if (h.spectral_basis && spectral_axes(c, pb, anchor_c, ax)) {
+        // the separable coarse operator: solved exactly (no CG iterations to report)
+        if ((s = spectral_solve(st, c, ax, h.spectral_basis, h.spectral_eigen, h.coarse_rhs, h.coarse_solution)) != XS_OK) return s;
+        const PressureWorkspace cw = carve_pressure_workspace(h.coarse_solver, c);
+        if ((s = check_cuda(cudaMemsetAsync(&cw.state->stats.iterations, 0, sizeof(uint32_t), st))) != XS_OK) return s;
+        return prolong_from(st, g, c, f, h.coarse_solution, h.correction);
+    }
     const float* guess = nullptr;
     if (h.coarsening2) {
         // the coarse solve's own start, the same way one level down (from
@@ -1732,7 +1748,7 @@ XsStatus coarse_correction(cudaStream_t st, const Grid& g, uint32_t anchor, cons
             return s;
         guess = h.coarse_start;
     }
-    if ((s = solve_pressure(st, c, coarse_solve_settings(guess), anchor_c, nullptr, pb, nullptr, h.coarse_rhs, h.coarse_solution, nullptr,
+    if ((s = solve_pressure(st, c, coarse_solve_settings(guess, max_iterations), anchor_c, nullptr, pb, nullptr, h.coarse_rhs, h.coarse_solution, nullptr,
                             h.coarse_solver, nullptr)) != XS_OK)
         return s;
     return prolong_from(st, g, c, f, h.coarse_solution, h.correction);
@@ -1839,6 +1855,23 @@ XsStatus line_step(cudaStream_t st, const Grid& g, uint32_t anchor, const uint32
     if ((s = check_launch()) != XS_OK) return s;
     line_update_kernel<<<grid, 256, 0, st>>>(n, h.coef, d, h.extra_product, x, r, x_out);
     return check_launch();
+}
+
+XsStatus coarse_cycles(cudaStream_t st, const Grid& g, uint32_t anchor, const XsScalarBoundary& pb, const WarmHistory& h, const float* rhs,
+                       const double* rhs_d, int cycles, const float** out) {
+    if (cycles < 1 || !out) return XS_INVALID_ARGUMENT;
+    const float* x = h.ring_start;
+    for (int c = 0; c < cycles; ++c) {
+        float* dst = (c % 2 == 0) ? h.start : h.ring_start;  // never x
+        XsStatus s;
+        if ((s = jacobi_sweeps(st, g, anchor, nullptr, pb, rhs, rhs_d, x, h.extra_product, dst)) != XS_OK) return s;
+        if ((s = start_residual(st, g, anchor, nullptr, pb, rhs, dst, h.residual, rhs_d)) != XS_OK) return s;
+        if ((s = coarse_correction(st, g, anchor, pb, h, h.residual, c == 0 ? kCoarseMaxIterations : kLaterCoarseIterations)) != XS_OK) return s;
+        if ((s = line_step(st, g, anchor, nullptr, pb, h, h.correction, dst, h.residual, dst)) != XS_OK) return s;
+        x = dst;
+    }
+    *out = x;
+    return XS_OK;
 }
 
 XsStatus start_residual(cudaStream_t st, const Grid& g, uint32_t anchor, const uint32_t* mask, const XsScalarBoundary& pb, const float* rhs,

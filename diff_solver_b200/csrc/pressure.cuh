@@ -102,7 +102,23 @@ struct WarmHistory {
     double* coarsest_rhs;     // (coarsest cells)
     float* coarsest_solution; // (coarsest cells)
     void* coarsest_solver;    // pressure workspace of the coarsest grid
+    // eigenbases of the coarse grid's axes (coarse grids within kSpectralMax)
+    float* spectral_basis;    // 3 kSpectralMax^2
+    float* spectral_eigen;    // 3 kSpectralMax
 };
+// Exact coarse solve for operators that separate by axis (spectral.cu):
+// grids of at most kSpectralMax cells per axis, no anchor cell, no colliders.
+constexpr int kSpectralMax = 128;
+struct SpectralAxes {
+    int n[3];
+    int kind[3];  // per axis: zero-gradient / fixed-value ends, or periodic
+};
+// Whether the coarse operator of grid c (boundary modes of pb, anchor cell or
+// none) separates; fills the axis description.
+bool spectral_axes(const Grid& c, const XsScalarBoundary& pb, uint32_t anchor, SpectralAxes& out);
+// x = A^-1 rhs on grid c by the axes' eigenbases (built into basis /
+// eigen: 3 kSpectralMax^2 and 3 kSpectralMax floats).
+XsStatus spectral_solve(cudaStream_t st, const Grid& c, const SpectralAxes& ax, float* basis, float* eigen, const double* rhs, float* x);
 constexpr double kCoarseTolerance = 1e-2;
 constexpr uint32_t kCoarseMaxIterations = 1000;
 // Damped Jacobi sweeps (weight 2/3) on the start before its residual is
@@ -129,7 +145,8 @@ XsStatus galerkin_combine(cudaStream_t st, const Grid& g, uint32_t anchor, const
 // coarse grid (boundary modes kept, no fixed values), solved by Jacobi-PCG
 // to kCoarseTolerance; P is trilinear interpolation at the fine cell
 // centres, clamped at the domain edges.  Grids without colliders only.
-XsStatus coarse_correction(cudaStream_t st, const Grid& g, uint32_t anchor, const XsScalarBoundary& pb, const WarmHistory& h, const float* r);
+XsStatus coarse_correction(cudaStream_t st, const Grid& g, uint32_t anchor, const XsScalarBoundary& pb, const WarmHistory& h, const float* r,
+                           uint32_t max_iterations = kCoarseMaxIterations);
 // kCoarsePreSweeps damped Jacobi sweeps from x (FP32 rhs with fixed values,
 // or the FP64 adjoint rhs_d without), result in x_out; tmp is scratch (N).
 // x_out may not alias x or tmp.
@@ -143,6 +160,27 @@ XsStatus record_coarse_iterations(cudaStream_t st, const WarmHistory& h, void* f
 // of x on entry and of x_out on return.  A d goes to h.extra_product.
 XsStatus line_step(cudaStream_t st, const Grid& g, uint32_t anchor, const uint32_t* mask, const XsScalarBoundary& pb, const WarmHistory& h,
                    const float* d, const float* x, float* r, float* x_out);
+// Rounds of the start pipeline (sweeps + coarse-grid correction) before the
+// forward and the adjoint fine solves.  Measured at 256^3 (plume, steps
+// 180-204): the forward start leaves a relative residual of 2.8e-5 after one
+// round (7-9 fine iterations), and a second round saves 5 iterations for
+// about as much time as it costs; the adjoint start's ring predicts far
+// less (0.03-0.15 left, against 3e-3 forward), and each round takes a
+// further factor of about 7: 133 / 38 / 7 / 3 fine iterations after 1 / 2 /
+// 3 / 4 rounds.
+constexpr int kForwardStartCycles = 1;
+constexpr int kAdjointStartCycles = 3;
+// Iteration cap of the coarse Jacobi-PCG (grids without the exact coarse
+// solve) in rounds after the first: their residuals are rougher, and a
+// solve to kCoarseTolerance took 60-260 iterations for little gain.
+constexpr uint32_t kLaterCoarseIterations = 16;
+// `cycles` rounds of: kCoarsePreSweeps Jacobi sweeps, the residual, the
+// coarse-grid correction of it, one line step along that correction; from x
+// (h.ring_start on entry), the rounds alternating between h.start and
+// h.ring_start.  *out = the final start, h.residual = its residual.  Grids
+// without colliders only.
+XsStatus coarse_cycles(cudaStream_t st, const Grid& g, uint32_t anchor, const XsScalarBoundary& pb, const WarmHistory& h, const float* rhs,
+                       const double* rhs_d, int cycles, const float** out);
 // r = b + fixed boundary values - A x, or r = rhs_d - A x for the FP64
 // adjoint right-hand side (no fixed values) when rhs_d is given
 XsStatus start_residual(cudaStream_t st, const Grid& g, uint32_t anchor, const uint32_t* mask, const XsScalarBoundary& pb, const float* rhs,

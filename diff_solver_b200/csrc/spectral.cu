@@ -1,0 +1,287 @@
+// Exact solve of the coarse pressure system of the warm start when the
+// operator separates by axis.
+//
+// Without colliders and without an anchor cell, the pressure operator of
+// the reference (operators.cu:852-902: diagonal = connected neighbours +
+// fixed-value faces, off-diagonals -1, periodic axes wrapped) is the
+// Kronecker sum A = Tx (+) Ty (+) Tz of three 1D operators, each a
+// tridiagonal (-1, 2, -1) whose end rows depend on that axis' boundary modes:
+// a zero-gradient end drops its missing neighbour (diagonal 1), a
+// fixed-value end keeps it as a constant (diagonal 2), a periodic axis
+// wraps.  Their orthonormal eigenbases are closed-form cosine / sine
+// families (DCT-II, DST-I, the half-shifted cosines of a mixed axis, the
+// real Fourier basis), so
+//
+//     A^-1 b = (Qx (x) Qy (x) Qz) diag(1 / (lx_i + ly_j + lz_k)) (Qx (x) Qy (x) Qz)^T b,
+//
+// three forward line transforms, one scaling and three inverse transforms.
+// Each transform is a dense product with the n x n basis held in shared
+// memory (n <= 128 on the coarse grids this serves): O(n) flops per cell and
+// axis instead of the coarse Jacobi-PCG's dozens of latency-bound
+// iterations.  A mode whose eigenvalue sum vanishes (the constant of an
+// all-zero-gradient box) is dropped: the pseudo-inverse.
+#include <algorithm>
+
+#include "launch.cuh"
+#include "pressure.cuh"
+
+namespace xs {
+
+namespace {
+
+enum AxisKind : int { kZeroZero = 0, kFixedFixed = 1, kZeroFixed = 2, kFixedZero = 3, kPeriodicAxis = 4 };
+
+constexpr int kLines = 32;         // lines per tile (adjacent in memory for the strided axes)
+constexpr int kTransformThreads = 256;  // 8 warps x 4 lines
+
+// Basis entry Q[j][k] (spatial index j, mode k) and eigenvalue of mode k of
+// a 1D operator of length n, in FP64.
+__device__ double basis_entry(int kind, int n, int j, int k) {
+    const double dn = n;
+    switch (kind) {
+        case kZeroZero:  // cos(pi k (j + 1/2) / n): DCT-II
+            return (k == 0 ? sqrt(1.0 / dn) : sqrt(2.0 / dn)) * cospi(k * (j + 0.5) / dn);
+        case kFixedFixed:  // sin(pi (k + 1)(j + 1) / (n + 1)): DST-I
+            return sqrt(2.0 / (dn + 1.0)) * sinpi((k + 1.0) * (j + 1.0) / (dn + 1.0));
+        case kZeroFixed:  // v_{-1} = v_0, v_n = 0: cos(theta (j + 1/2)), theta (n + 1/2) = pi (k + 1/2)
+            return 2.0 / sqrt(2.0 * dn + 1.0) * cospi((k + 0.5) * (j + 0.5) / (dn + 0.5));
+        case kFixedZero:  // the mirror image
+            return 2.0 / sqrt(2.0 * dn + 1.0) * cospi((k + 0.5) * (n - 1 - j + 0.5) / (dn + 0.5));
+        default: {  // periodic: 1, then cos / sin pairs of frequency m, then (-1)^j for even n
+            if (k == 0) return sqrt(1.0 / dn);
+            const int m = (k + 1) / 2;
+            if (2 * m == n) return cospi(static_cast<double>(j)) * sqrt(1.0 / dn);
+            return sqrt(2.0 / dn) * ((k & 1) ? cospi(2.0 * m * j / dn) : sinpi(2.0 * m * j / dn));
+        }
+    }
+}
+
+__device__ double eigenvalue(int kind, int n, int k) {
+    const double dn = n;
+    switch (kind) {
+        case kZeroZero: return 2.0 - 2.0 * cospi(k / dn);
+        case kFixedFixed: return 2.0 - 2.0 * cospi((k + 1.0) / (dn + 1.0));
+        case kZeroFixed:
+        case kFixedZero: return 2.0 - 2.0 * cospi((k + 0.5) / (dn + 0.5));
+        default: return 2.0 - 2.0 * cospi(2.0 * ((k + 1) / 2) / dn);
+    }
+}
+
+// basis: 3 x kSpectralMax x kSpectralMax (row j, column k; zero beyond n),
+// eigen: 3 x kSpectralMax.
+__global__ void spectral_basis_kernel(SpectralAxes ax, float* __restrict__ basis, float* __restrict__ eigen) {
+    constexpr int P = kSpectralMax;
+    const int i = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
+    if (i >= 3 * P * P) return;
+    const int a = i / (P * P), j = (i / P) % P, k = i % P;
+    const int n = ax.n[a];
+    basis[i] = (j < n && k < n) ? static_cast<float>(basis_entry(ax.kind[a], n, j, k)) : 0.0f;
+    if (j == 0) eigen[a * P + k] = k < n ? static_cast<float>(eigenvalue(ax.kind[a], n, k)) : 0.0f;
+}
+
+// The lines of one axis: line L starts at (L % inner) * s_in + (L / inner) *
+// s_out, its elements `stride` apart.
+struct LineSet {
+    uint32_t lines;
+    uint32_t inner;
+    uint64_t s_in, s_out;
+    uint64_t stride;
+    int n;
+    __device__ __forceinline__ uint64_t base(uint32_t L) const { return static_cast<uint64_t>(L % inner) * s_in + static_cast<uint64_t>(L / inner) * s_out; }
+};
+
+// Eigenvalue sums of the last axis' lines for the scaling pass: line L holds
+// modes (L % inner, L / inner) of the two axes transformed before.
+struct LineScale {
+    const float* lam_a;  // indexed by L % inner
+    const float* lam_b;  // indexed by L / inner
+    const float* lam_line;
+    uint32_t inner;
+};
+
+constexpr size_t transform_smem(int np) { return sizeof(float) * static_cast<size_t>(np + kLines) * (np + 1); }
+
+// Tiles of 32 lines: loaded into shared memory (coalesced), transformed
+// against the basis in shared memory (row pitch np + 1: row and column
+// walks are both free of bank conflicts), written back in place.  kMode 0:
+// c_k = sum_j Q[j][k] v_j; 1: v_j = sum_k Q[j][k] c_k; 2: forward, divide by
+// the eigenvalue sum, inverse (the last axis).  Each warp owns four lines,
+// each lane the outputs lane, lane + 32, ... .
+template <int NP, int kMode, class Tin>
+__global__ void __launch_bounds__(kTransformThreads) line_transform_kernel(const Tin* in, float* out, LineSet ls, const float* __restrict__ q,
+                                                                         LineScale sc) {
+    constexpr int R = NP + 1;
+    constexpr int Q4 = NP / 32;
+    extern __shared__ float smem[];
+    float* ms = smem;           // NP x R
+    float* d = smem + NP * R;   // kLines x R
+    const int t = static_cast<int>(threadIdx.x), lane = t & 31, l0 = (t >> 5) * 4;
+    for (int i = t; i < NP * NP; i += kTransformThreads) ms[(i / NP) * R + i % NP] = q[(i / NP) * kSpectralMax + i % NP];
+    const bool contiguous = ls.stride == 1;
+    const uint32_t tiles = (ls.lines + kLines - 1) / kLines;
+    for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const uint32_t L0 = tile * kLines;
+        __syncthreads();  // the basis is in place; the previous tile is written out
+        for (int i = t; i < kLines * NP; i += kTransformThreads) {
+            const int l = contiguous ? i / NP : i % kLines, j = contiguous ? i % NP : i / kLines;
+            const uint32_t L = L0 + l;
+            d[l * R + j] = (L < ls.lines && j < ls.n) ? static_cast<float>(in[ls.base(L) + static_cast<uint64_t>(j) * ls.stride]) : 0.0f;
+        }
+        __syncthreads();
+        float acc[4][Q4];
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int c = 0; c < Q4; ++c) acc[i][c] = 0.0f;
+        if (kMode != 1) {
+#pragma unroll 4
+            for (int j = 0; j < NP; ++j) {
+                float v[4], m[Q4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) v[i] = d[(l0 + i) * R + j];
+#pragma unroll
+                for (int c = 0; c < Q4; ++c) m[c] = ms[j * R + lane + 32 * c];
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int c = 0; c < Q4; ++c) acc[i][c] = fmaf(v[i], m[c], acc[i][c]);
+            }
+        }
+        if (kMode == 2) {
+#pragma unroll
+            for (int i = 0; i < 4; ++i) {
+                const uint32_t L = L0 + l0 + i;
+                const float lam_ab = L < ls.lines ? sc.lam_a[L % sc.inner] + sc.lam_b[L / sc.inner] : 0.0f;
+#pragma unroll
+                for (int c = 0; c < Q4; ++c) {
+                    const int k = lane + 32 * c;
+                    const float lam = lam_ab + (k < ls.n ? sc.lam_line[k] : 0.0f);
+                    acc[i][c] = (L < ls.lines && k < ls.n && lam > 0.0f) ? acc[i][c] / lam : 0.0f;
+                }
+            }
+            __syncthreads();  // every warp has read its lines
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int c = 0; c < Q4; ++c) d[(l0 + i) * R + lane + 32 * c] = acc[i][c];
+            __syncthreads();
+        }
+        if (kMode != 0) {
+            float r[4][Q4];
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int c = 0; c < Q4; ++c) r[i][c] = 0.0f;
+#pragma unroll 4
+            for (int k = 0; k < NP; ++k) {
+                float v[4], m[Q4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) v[i] = d[(l0 + i) * R + k];
+#pragma unroll
+                for (int c = 0; c < Q4; ++c) m[c] = ms[(lane + 32 * c) * R + k];
+#pragma unroll
+                for (int i = 0; i < 4; ++i)
+#pragma unroll
+                    for (int c = 0; c < Q4; ++c) r[i][c] = fmaf(v[i], m[c], r[i][c]);
+            }
+#pragma unroll
+            for (int i = 0; i < 4; ++i)
+#pragma unroll
+                for (int c = 0; c < Q4; ++c) acc[i][c] = r[i][c];
+        }
+        __syncthreads();  // every warp has read its lines
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+#pragma unroll
+            for (int c = 0; c < Q4; ++c) d[(l0 + i) * R + lane + 32 * c] = acc[i][c];
+        __syncthreads();
+        for (int i = t; i < kLines * NP; i += kTransformThreads) {
+            const int l = contiguous ? i / NP : i % kLines, j = contiguous ? i % NP : i / kLines;
+            const uint32_t L = L0 + l;
+            if (L < ls.lines && j < ls.n) out[ls.base(L) + static_cast<uint64_t>(j) * ls.stride] = d[l * R + j];
+        }
+    }
+}
+
+template <int NP, int kMode, class Tin>
+XsStatus launch_transform(cudaStream_t st, const Tin* in, float* out, const LineSet& ls, const float* q, const LineScale& sc) {
+    static DeviceOnce configured;
+    const size_t smem = transform_smem(NP);
+    if (!configured.run([smem] {
+            return cudaFuncSetAttribute(line_transform_kernel<NP, kMode, Tin>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+        }))
+        return XS_CUDA_ERROR;
+    const uint32_t tiles = (ls.lines + kLines - 1) / kLines;
+    const unsigned blocks = std::min<uint32_t>(tiles, 2u * 148u);
+    line_transform_kernel<NP, kMode, Tin><<<blocks, kTransformThreads, smem, st>>>(in, out, ls, q, sc);
+    return check_launch();
+}
+
+template <int kMode, class Tin>
+XsStatus transform(cudaStream_t st, const Tin* in, float* out, const LineSet& ls, const float* q, const LineScale& sc) {
+    if (ls.n <= 32) return launch_transform<32, kMode, Tin>(st, in, out, ls, q, sc);
+    if (ls.n <= 64) return launch_transform<64, kMode, Tin>(st, in, out, ls, q, sc);
+    return launch_transform<128, kMode, Tin>(st, in, out, ls, q, sc);
+}
+
+}  // namespace
+
+bool spectral_axes(const Grid& c, const XsScalarBoundary& pb, uint32_t anchor, SpectralAxes& out) {
+    if (anchor < cell_count(c)) return false;  // the anchored operator is not a Kronecker sum
+    const int n[3] = {c.nx, c.ny, c.nz};
+    for (int a = 0; a < 3; ++a) {
+        if (n[a] < 4 || n[a] > kSpectralMax) return false;
+        const uint32_t lo = pb.modes[2 * a], hi = pb.modes[2 * a + 1];
+        out.n[a] = n[a];
+        if (lo == 2u && hi == 2u) {
+            out.kind[a] = kPeriodicAxis;
+        } else {
+            const bool flo = lo == 0u, fhi = hi == 0u;  // fixed value; anything else drops the missing neighbour
+            out.kind[a] = flo ? (fhi ? kFixedFixed : kFixedZero) : (fhi ? kZeroFixed : kZeroZero);
+        }
+    }
+    return true;
+}
+
+XsStatus spectral_solve(cudaStream_t st, const Grid& c, const SpectralAxes& ax, float* basis, float* eigen, const double* rhs, float* x) {
+    if (!basis || !eigen || !rhs || !x) return XS_INVALID_ARGUMENT;
+    constexpr int P = kSpectralMax;
+    spectral_basis_kernel<<<(3 * P * P + 255) / 256, 256, 0, st>>>(ax, basis, eigen);
+    XsStatus s = check_launch();
+    if (s != XS_OK) return s;
+    const uint64_t nx = c.nx, ny = c.ny, nz = c.nz;
+    // x lines: L = y + ny z, contiguous; y lines: L = x + nx z; z lines: L = x + nx y
+    const LineSet lx{static_cast<uint32_t>(ny * nz), 1u, 0u, nx, 1u, c.nx};
+    const LineSet ly{static_cast<uint32_t>(nx * nz), static_cast<uint32_t>(nx), 1u, nx * ny, nx, c.ny};
+    const LineSet lz{static_cast<uint32_t>(nx * ny), 1u, 0u, 1u, nx * ny, c.nz};
+    const float* qx = basis;
+    const float* qy = basis + P * P;
+    const float* qz = basis + 2 * P * P;
+    const LineScale none{nullptr, nullptr, nullptr, 1u};
+    const LineScale scale{eigen, eigen + P, eigen + 2 * P, static_cast<uint32_t>(nx)};
+    if ((s = transform<0, double>(st, rhs, x, lx, qx, none)) != XS_OK) return s;
+    if ((s = transform<0, float>(st, x, x, ly, qy, none)) != XS_OK) return s;
+    if ((s = transform<2, float>(st, x, x, lz, qz, scale)) != XS_OK) return s;
+    if ((s = transform<1, float>(st, x, x, ly, qy, none)) != XS_OK) return s;
+    return transform<1, float>(st, x, x, lx, qx, none);
+}
+
+}  // namespace xs
+
+using namespace xs;
+
+extern "C" {
+
+size_t xs_separable_solve_scratch_bytes(void) { return sizeof(float) * (3 * kSpectralMax * kSpectralMax + 3 * kSpectralMax); }
+
+XsStatus xs_separable_solve(cudaStream_t stream, XsGrid grid, XsScalarBoundary pressure_boundary, uint32_t pressure_anchor,
+                            const double* rhs, float* x, void* scratch) {
+    if (!valid_grid(grid) || !rhs || !x || !scratch) return XS_INVALID_ARGUMENT;
+    const Grid g = make_grid(grid);
+    SpectralAxes ax;
+    if (!spectral_axes(g, pressure_boundary, pressure_anchor, ax)) return XS_INVALID_ARGUMENT;
+    float* basis = static_cast<float*>(scratch);
+    return spectral_solve(stream, g, ax, basis, basis + 3 * kSpectralMax * kSpectralMax, rhs, x);
+}
+
+}  // extern "C"

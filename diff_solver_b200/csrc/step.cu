@@ -46,22 +46,21 @@ XsStatus projection_forward(cudaStream_t st, const Grid& g, const XsPressureSolv
         if ((s = galerkin_combine(st, g, anchor, mask, pb, h, true, nullptr, 0, rhs, h.ring_start)) != XS_OK) return s;
         used.initial_guess = h.ring_start;
         if (warm_start || coarse) {
+            // smooth the start before each coarse-grid step: the coarse grid
+            // then sees its smooth error alone
             const float* x = h.ring_start;
-            if (coarse) {  // smooth the start first: the coarse grid then sees its smooth error alone
-                if ((s = jacobi_sweeps(st, g, anchor, mask, pb, rhs, nullptr, h.ring_start, h.extra_product, h.start)) != XS_OK) return s;
-                x = h.start;
-            }
-            if ((s = start_residual(st, g, anchor, mask, pb, rhs, x, h.residual)) != XS_OK) return s;
             if (coarse) {
-                if ((s = coarse_correction(st, g, anchor, pb, h, h.residual)) != XS_OK) return s;
-                if ((s = line_step(st, g, anchor, mask, pb, h, h.correction, x, h.residual, h.start)) != XS_OK) return s;
-                x = h.start;
+                if ((s = coarse_cycles(st, g, anchor, pb, h, rhs, nullptr, kForwardStartCycles, &x)) != XS_OK) return s;
+            } else if ((s = start_residual(st, g, anchor, mask, pb, rhs, x, h.residual)) != XS_OK) {
+                return s;
             }
             if (warm_start) {
+                float* out = x == h.start ? h.ring_start : h.start;
                 if ((s = warm_start_guess(warm_start, st, g, h.residual, &guess)) != XS_OK) return s;
-                if ((s = line_step(st, g, anchor, mask, pb, h, guess, x, h.residual, h.start)) != XS_OK) return s;
+                if ((s = line_step(st, g, anchor, mask, pb, h, guess, x, h.residual, out)) != XS_OK) return s;
+                x = out;
             }
-            used.initial_guess = h.start;
+            used.initial_guess = x;
         }
         used.scale_guess = 0u;
     } else if (warm_start && pcg) {

@@ -248,6 +248,18 @@ XsStatus xs_pressure_solve_static(cudaStream_t stream, XsGrid grid, const XsPres
                                   const uint32_t* cell_mask, XsScalarBoundary pressure_boundary, const float* rhs, float* pressure,
                                   XsSolveStats* host_stats);
 
+/* No counterpart in the reference.  The exact solve the warm start's
+ * coarse-grid correction uses: A x = rhs (the pressure operator without
+ * fixed values) on a grid without colliders or anchor cell and with at most
+ * XS_SEPARABLE_SOLVE_MAX cells per axis, by the eigenbases of the three 1D
+ * operators the operator separates into.  XS_INVALID_ARGUMENT for other
+ * grids.  scratch: xs_separable_solve_scratch_bytes() bytes of device
+ * memory. */
+#define XS_SEPARABLE_SOLVE_MAX 128u
+size_t xs_separable_solve_scratch_bytes(void);
+XsStatus xs_separable_solve(cudaStream_t stream, XsGrid grid, XsScalarBoundary pressure_boundary, uint32_t pressure_anchor,
+                            const double* rhs, float* x, void* scratch);
+
 /* Byte offset of the XsSolveStats record inside a projection or step
  * workspace (device memory), for asynchronous copies that do not
  * synchronise. */
