@@ -757,7 +757,7 @@ def main():
               "spinup_steps": args.spinup,
               "warm_start": f"Galerkin start over the last {HISTORY} solutions"
                             + (f", 6 Jacobi sweeps and a step along the coarse-grid correction (grid coarsened x{args.coarsening}, "
-                               f"Jacobi-PCG to 1e-2 from its own two-level start)"
+                               f"solved exactly by the eigenbases of its separable operator; adjoint solves: three such rounds)"
                                if args.coarsening else "")
                             + ("" if args.no_learned else
                                f", step along the U-Net correction (network trained at 128^3, applied on the grid restricted "

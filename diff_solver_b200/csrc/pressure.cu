@@ -646,6 +646,35 @@ __device__ __forceinline__ Double4 apply4(const FastGeom& f, const float* __rest
     return q;
 }
 
+// apply4 in FP32: the start pipeline's smoothing, residual and line-step
+// passes (their results only shape the start; the solve's own residuals are
+// FP64), without the float-to-double conversions that bound the FP64 form.
+__device__ __forceinline__ float4 apply4f(const FastGeom& f, const float* __restrict__ x, uint32_t i, float4& c, float4& d) {
+    const uint32_t row = fastdiv(i, f.dnx);
+    const uint32_t x0 = i - row * f.nx;
+    const uint32_t z = fastdiv(row, f.dny);
+    const uint32_t y = row - z * f.ny;
+    const RowGeom rg = row_geom(f, y, z);
+    int32_t left, right;
+    x_geom(f, x0, rg.dyz, left, right, d);
+    c = ld4(x + i);
+    float4 q = make_float4(d.x * c.x, d.y * c.y, d.z * c.z, d.w * c.w);
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        if (rg.off[k] != 0) {
+            const float4 v = ld4(x + static_cast<uint32_t>(static_cast<int32_t>(i) + rg.off[k]));
+            q.x -= v.x; q.y -= v.y; q.z -= v.z; q.w -= v.w;
+        }
+    }
+    if (left != 0) q.x -= x[static_cast<uint32_t>(static_cast<int32_t>(i) + left)];
+    if (right != 0) q.w -= x[static_cast<uint32_t>(static_cast<int32_t>(i) + right)];
+    q.x -= c.y;
+    q.y -= c.x + c.z;
+    q.z -= c.y + c.w;
+    q.w -= c.z;
+    return q;
+}
+
 __device__ __forceinline__ float4 round4(const Double4& v) {
     return make_float4(static_cast<float>(v.x), static_cast<float>(v.y), static_cast<float>(v.z), static_cast<float>(v.w));
 }
@@ -658,26 +687,33 @@ __device__ __forceinline__ Double4 ld4_rhs(const double* p) {
     const double2 a = *reinterpret_cast<const double2*>(p), b = *reinterpret_cast<const double2*>(p + 2);
     return Double4{a.x, a.y, b.x, b.y};
 }
+__device__ __forceinline__ float4 ld4_rhs_f(const float* p) { return ld4(p); }
+__device__ __forceinline__ float4 ld4_rhs_f(const double* p) {
+    const double2 a = *reinterpret_cast<const double2*>(p), b = *reinterpret_cast<const double2*>(p + 2);
+    return make_float4(static_cast<float>(a.x), static_cast<float>(a.y), static_cast<float>(b.x), static_cast<float>(b.y));
+}
 
 enum FastPass { kPassJacobi = 0, kPassResidual = 1, kPassApply = 2 };
 
 // kPassJacobi: out = x + omega (b - A x) / diag; kPassResidual: out = b - A x;
-// kPassApply: out = A x.
+// kPassApply: out = A x.  FP32 arithmetic (apply4f): these passes build the
+// start of a solve.
 template <int kPass, class T>
 __global__ void fast_pass_kernel(FastGeom f, const float* __restrict__ x, const T* __restrict__ rhs, float* __restrict__ out, float omega) {
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < f.groups; t += gridDim.x * blockDim.x) {
         const uint32_t i = 4u * t;
         float4 c, d;
-        const Double4 q = apply4(f, x, i, c, d);
+        const float4 q = apply4f(f, x, i, c, d);
         if (kPass == kPassApply) {
-            st4(out + i, round4(q));
+            st4(out + i, q);
         } else {
-            const Double4 b = ld4_rhs(rhs + i);
-            const Double4 r{b.x - q.x, b.y - q.y, b.z - q.z, b.w - q.w};
+            const float4 b = ld4_rhs_f(rhs + i);
+            const float4 r = make_float4(b.x - q.x, b.y - q.y, b.z - q.z, b.w - q.w);
             if (kPass == kPassResidual)
-                st4(out + i, round4(r));
-            else
-                st4(out + i, round4(Double4{c.x + omega * r.x / d.x, c.y + omega * r.y / d.y, c.z + omega * r.z / d.z, c.w + omega * r.w / d.w}));
+                st4(out + i, r);
+            else  // damped Jacobi update
+                st4(out + i, make_float4(fmaf(r.x, omega / d.x, c.x), fmaf(r.y, omega / d.y, c.y), fmaf(r.z, omega / d.z, c.z),
+                                         fmaf(r.w, omega / d.w, c.w)));
         }
     }
 }
@@ -1318,6 +1354,63 @@ __global__ void __launch_bounds__(256, M > 5 ? 2 : 3) basis_gram_kernel(BasisArg
         for (int k = 0; k < K; ++k) a.partials[static_cast<size_t>(blockIdx.x) * K + k] = acc[k];
 }
 
+// basis_gram_kernel on 4-cell groups (n a multiple of 4, no fixed boundary
+// values in b): 16-byte loads, four times the bytes in flight per thread.
+template <int M>
+__global__ void __launch_bounds__(256, M > 3 ? 2 : 3) basis_gram4_kernel(BasisArgs<M> a, uint32_t groups) {
+    constexpr int K = M * (M + 1) / 2 + M;
+    __shared__ double red[K * 32];
+    const float* ptr[M];
+    const float* wptr[M];
+    uint32_t count;
+    basis_order(a, ptr, count, &wptr);
+    double acc[K];
+#pragma unroll
+    for (int k = 0; k < K; ++k) acc[k] = 0.0;
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < groups; t += gridDim.x * blockDim.x) {
+        const uint32_t i = 4u * t;
+        double b[4];
+        if (a.rhs_d) {
+            const double2 lo = *reinterpret_cast<const double2*>(a.rhs_d + i), hi = *reinterpret_cast<const double2*>(a.rhs_d + i + 2);
+            b[0] = lo.x; b[1] = lo.y; b[2] = hi.x; b[3] = hi.y;
+        } else {
+            const float4 v = ld4(a.rhs + i);
+            b[0] = v.x; b[1] = v.y; b[2] = v.z; b[3] = v.w;
+        }
+        float4 rv[M], ar[M];
+#pragma unroll
+        for (int j = 0; j < M; ++j) {
+            rv[j] = ptr[j] ? ld4(ptr[j] + i) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+            ar[j] = wptr[j] ? ld4(wptr[j] + i) : make_float4(0.0f, 0.0f, 0.0f, 0.0f);
+        }
+#pragma unroll
+        for (int e = 0; e < 4; ++e) {
+            double vi[M], av[M];
+#pragma unroll
+            for (int j = 0; j < M; ++j) {
+                const float* r0 = reinterpret_cast<const float*>(&rv[j]);
+                const float* a0 = reinterpret_cast<const float*>(&ar[j]);
+                const bool diff = j > 0 && j < static_cast<int>(a.history) && static_cast<uint32_t>(j) < count;
+                const float* r1 = reinterpret_cast<const float*>(&rv[j > 0 ? j - 1 : 0]);
+                const float* a1 = reinterpret_cast<const float*>(&ar[j > 0 ? j - 1 : 0]);
+                vi[j] = diff ? static_cast<double>(r1[e]) - static_cast<double>(r0[e]) : static_cast<double>(r0[e]);
+                av[j] = diff ? static_cast<double>(a1[e]) - static_cast<double>(a0[e]) : static_cast<double>(a0[e]);
+            }
+            int k = 0;
+#pragma unroll
+            for (int r = 0; r < M; ++r)
+#pragma unroll
+                for (int c = r; c < M; ++c) acc[k++] += vi[r] * av[c];
+#pragma unroll
+            for (int r = 0; r < M; ++r) acc[k++] += vi[r] * b[e];
+        }
+    }
+    block_sum<K>(acc, red);
+    if (threadIdx.x == 0)
+#pragma unroll
+        for (int k = 0; k < K; ++k) a.partials[static_cast<size_t>(blockIdx.x) * K + k] = acc[k];
+}
+
 // Sums the partials in block order and solves the scaled Gram system.
 template <int M>
 __global__ void basis_solve_kernel(const double* __restrict__ partials, uint32_t blocks, double* __restrict__ coef) {
@@ -1396,6 +1489,35 @@ __global__ void basis_combine_kernel(BasisArgs<M> a, const double* __restrict__ 
         for (int j = 0; j < M; ++j)
             if (w[j] != 0.0) acc += w[j] * static_cast<double>(ptr[j][i]);
         x0[i] = static_cast<float>(acc);
+    }
+}
+
+// basis_combine_kernel on 4-cell groups.
+template <int M>
+__global__ void __launch_bounds__(256) basis_combine4_kernel(BasisArgs<M> a, const double* __restrict__ coef, float* __restrict__ x0, uint32_t groups) {
+    const float* ptr[M];
+    uint32_t count;
+    basis_order(a, ptr, count);
+    double w[M];
+#pragma unroll
+    for (int j = 0; j < M; ++j) {
+        if (ptr[j] == nullptr) { w[j] = 0.0; continue; }
+        if (j >= static_cast<int>(a.history)) { w[j] = coef[j]; continue; }
+        w[j] = (j == 0 ? coef[0] : -coef[j]) + (static_cast<uint32_t>(j + 1) < count ? coef[j + 1] : 0.0);
+    }
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < groups; t += gridDim.x * blockDim.x) {
+        const uint32_t i = 4u * t;
+        double acc[4] = {0.0, 0.0, 0.0, 0.0};
+#pragma unroll
+        for (int j = 0; j < M; ++j)
+            if (w[j] != 0.0) {
+                const float4 v = ld4(ptr[j] + i);
+                acc[0] += w[j] * static_cast<double>(v.x);
+                acc[1] += w[j] * static_cast<double>(v.y);
+                acc[2] += w[j] * static_cast<double>(v.z);
+                acc[3] += w[j] * static_cast<double>(v.w);
+            }
+        st4(x0 + i, make_float4(static_cast<float>(acc[0]), static_cast<float>(acc[1]), static_cast<float>(acc[2]), static_cast<float>(acc[3])));
     }
 }
 
@@ -1508,7 +1630,7 @@ size_t warm_history_bytes(const Grid& g, uint32_t history, uint32_t coarsening) 
     if (coarse_grid(g, coarsening, c)) {
         const size_t nc = cell_count(c);
         bytes += align_up(n * 4, 256) + align_up(nc * 8, 256) + align_up(nc * 4, 256) + align_up(pressure_workspace_bytes(c), 256);
-        if (spectral_fits(c)) bytes += align_up(4 * 3 * kSpectralMax * kSpectralMax, 256) + align_up(4 * 3 * kSpectralMax, 256);
+        if (spectral_fits(c)) bytes += align_up(4 * 6 * kSpectralMax * kSpectralMax, 256) + align_up(4 * 3 * kSpectralMax, 256);
         const uint32_t f2 = second_coarsening(c);
         if (f2 && coarse_grid(c, f2, c2)) {
             const size_t nc2 = cell_count(c2);
@@ -1549,7 +1671,7 @@ WarmHistory carve_warm_history(void* base, const Grid& g, uint32_t history, uint
         h.coarse_solution = reinterpret_cast<float*>(take(nc * 4));
         h.coarse_solver = take(pressure_workspace_bytes(h.coarse));
         if (spectral_fits(h.coarse)) {
-            h.spectral_basis = reinterpret_cast<float*>(take(4 * 3 * kSpectralMax * kSpectralMax));
+            h.spectral_basis = reinterpret_cast<float*>(take(4 * 6 * kSpectralMax * kSpectralMax));
             h.spectral_eigen = reinterpret_cast<float*>(take(4 * 3 * kSpectralMax));
         }
         const uint32_t f2 = second_coarsening(h.coarse);
@@ -1596,12 +1718,23 @@ XsStatus galerkin_m(cudaStream_t st, const Operator& op, const WarmHistory& h, u
     if (!rhs_d)
         for (int f = 0; f < 6; ++f)
             if (op.pb.modes[f] == 0u && op.pb.values[f] != 0.0f) a.fixed_terms = 1u;
-    const unsigned blocks = static_cast<unsigned>(std::min<uint64_t>((n + 255) / 256, kGramBlocks));
-    basis_gram_kernel<M><<<blocks, 256, 0, st>>>(a);
+    // 4-cell groups when every group lies in the array and b has no fixed terms
+    const bool vec = n % 4 == 0 && n < (1ull << 31) && !a.fixed_terms;
+    const uint32_t groups = static_cast<uint32_t>(n / 4);
+    // (the 4-cell form of a basis of 4 or more vectors runs 2 blocks per SM)
+    const unsigned cap = vec && M > 3 ? 148u * 2u : static_cast<unsigned>(kGramBlocks);
+    const unsigned blocks = static_cast<unsigned>(std::min<uint64_t>(((vec ? groups : n) + 255) / 256, cap));
+    if (vec)
+        basis_gram4_kernel<M><<<blocks, 256, 0, st>>>(a, groups);
+    else
+        basis_gram_kernel<M><<<blocks, 256, 0, st>>>(a);
     if ((s = check_launch()) != XS_OK) return s;
     basis_solve_kernel<M><<<1, 64, 0, st>>>(h.partials, blocks, h.coef);
     if ((s = check_launch()) != XS_OK) return s;
-    basis_combine_kernel<M><<<static_cast<unsigned>(std::min<uint64_t>((n + 255) / 256, 148 * 16)), 256, 0, st>>>(a, h.coef, out);
+    if (vec)
+        basis_combine4_kernel<M><<<static_cast<unsigned>(std::min<uint64_t>((groups + 255) / 256, 148 * 16)), 256, 0, st>>>(a, h.coef, out, groups);
+    else
+        basis_combine_kernel<M><<<static_cast<unsigned>(std::min<uint64_t>((n + 255) / 256, 148 * 16)), 256, 0, st>>>(a, h.coef, out);
     return check_launch();
 }
 
@@ -1671,6 +1804,39 @@ __global__ void coarse_prolong_kernel(Grid g, Grid c, float inv_f, const float* 
     }
 }
 
+// coarse_prolong_kernel for 4 consecutive fine cells of a row per thread
+// (nx a multiple of 4), the row from the launch grid: no index division, one
+// 16-byte store.  The same arithmetic per cell.
+__global__ void __launch_bounds__(128) coarse_prolong4_kernel(Grid g, Grid c, float inv_f, const float* __restrict__ ec, float* __restrict__ out) {
+    const int x = 4 * static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
+    const int y = static_cast<int>(blockIdx.y), z = static_cast<int>(blockIdx.z);
+    if (x >= g.nx) return;
+    int y0, y1, z0, z1;
+    float wy, wz;
+    coarse_axis(y, c.ny, inv_f, y0, y1, wy);
+    coarse_axis(z, c.nz, inv_f, z0, z1, wz);
+    const uint64_t sy = static_cast<uint64_t>(c.nx), sz = static_cast<uint64_t>(c.nx) * static_cast<uint64_t>(c.ny);
+    const float* r00 = ec + static_cast<uint64_t>(z0) * sz + static_cast<uint64_t>(y0) * sy;
+    const float* r10 = ec + static_cast<uint64_t>(z0) * sz + static_cast<uint64_t>(y1) * sy;
+    const float* r01 = ec + static_cast<uint64_t>(z1) * sz + static_cast<uint64_t>(y0) * sy;
+    const float* r11 = ec + static_cast<uint64_t>(z1) * sz + static_cast<uint64_t>(y1) * sy;
+    float v[4];
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+        int x0, x1;
+        float wx;
+        coarse_axis(x + k, c.nx, inv_f, x0, x1, wx);
+        const float c00 = __ldg(r00 + x0) * (1.0f - wx) + __ldg(r00 + x1) * wx;
+        const float c10 = __ldg(r10 + x0) * (1.0f - wx) + __ldg(r10 + x1) * wx;
+        const float c01 = __ldg(r01 + x0) * (1.0f - wx) + __ldg(r01 + x1) * wx;
+        const float c11 = __ldg(r11 + x0) * (1.0f - wx) + __ldg(r11 + x1) * wx;
+        const float c0 = c00 * (1.0f - wy) + c10 * wy;
+        const float c1 = c01 * (1.0f - wy) + c11 * wy;
+        v[k] = c0 * (1.0f - wz) + c1 * wz;
+    }
+    st4(out + (static_cast<uint64_t>(z) * g.ny + y) * g.nx + x, make_float4(v[0], v[1], v[2], v[3]));
+}
+
 namespace {
 
 XsStatus restrict_to(cudaStream_t st, const Grid& fine, const Grid& coarse, uint32_t f, const float* r, double* rc) {
@@ -1681,6 +1847,11 @@ XsStatus restrict_to(cudaStream_t st, const Grid& fine, const Grid& coarse, uint
 }
 
 XsStatus prolong_from(cudaStream_t st, const Grid& fine, const Grid& coarse, uint32_t f, const float* ec, float* out) {
+    if (fine.nx % 4 == 0 && fine.ny <= 65535 && fine.nz <= 65535) {
+        const dim3 grid(static_cast<unsigned>((fine.nx / 4 + 127) / 128), static_cast<unsigned>(fine.ny), static_cast<unsigned>(fine.nz));
+        coarse_prolong4_kernel<<<grid, 128, 0, st>>>(fine, coarse, 1.0f / static_cast<float>(f), ec, out);
+        return check_launch();
+    }
     const uint64_t n = cell_count(fine);
     coarse_prolong_kernel<<<static_cast<unsigned>(std::min<uint64_t>((n + 255) / 256, 148 * 16)), 256, 0, st>>>(
         fine, coarse, 1.0f / static_cast<float>(f), ec, out);
@@ -1823,18 +1994,62 @@ __global__ void line_update_kernel(uint64_t n, const double* __restrict__ coef, 
     }
 }
 
+// The same on 4-cell groups (n a multiple of 4).
+__global__ void __launch_bounds__(256) line_update4_kernel(uint32_t groups, const double* __restrict__ coef, const float* __restrict__ d,
+                                                           const float* __restrict__ ad, const float* x, float* r, float* x_out) {
+    const float c = static_cast<float>(coef[0]);
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < groups; t += gridDim.x * blockDim.x) {
+        const uint32_t i = 4u * t;
+        st4(x_out + i, axpy4(ld4(x + i), c, ld4(d + i)));
+        st4(r + i, axpy4(ld4(r + i), -c, ld4(ad + i)));
+    }
+}
+
+// A d of a line step's direction and the two products of its coefficient,
+// d . A d and d . r, in one pass on the fast path's 4-cell groups: the same
+// per-block partials as basis_gram_kernel<1> ([block][2]); FP32 products and
+// per-thread sums (a few hundred terms), FP64 across the block.
+__global__ void __launch_bounds__(256) line_gram_fast_kernel(FastGeom f, const float* __restrict__ d, const float* __restrict__ r,
+                                                             float* __restrict__ ad, double* __restrict__ partials) {
+    __shared__ double red[2 * 32];
+    float s0 = 0.0f, s1 = 0.0f;  // a thread's own terms in FP32, the block's sums in FP64
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < f.groups; t += gridDim.x * blockDim.x) {
+        const uint32_t i = 4u * t;
+        float4 c, dg;
+        const float4 q = apply4f(f, d, i, c, dg);
+        st4(ad + i, q);
+        const float4 rv = ld4(r + i);
+        s0 = fmaf(c.x, q.x, fmaf(c.y, q.y, fmaf(c.z, q.z, fmaf(c.w, q.w, s0))));
+        s1 = fmaf(c.x, rv.x, fmaf(c.y, rv.y, fmaf(c.z, rv.z, fmaf(c.w, rv.w, s1))));
+    }
+    double acc[2] = {s0, s1};
+    block_sum<2>(acc, red);
+    if (threadIdx.x == 0) {
+        partials[2 * static_cast<size_t>(blockIdx.x)] = acc[0];
+        partials[2 * static_cast<size_t>(blockIdx.x) + 1] = acc[1];
+    }
+}
+
 XsStatus line_step(cudaStream_t st, const Grid& g, uint32_t anchor, const uint32_t* mask, const XsScalarBoundary& pb, const WarmHistory& h,
                    const float* d, const float* x, float* r, float* x_out) {
     if (!h.meta || !h.extra_product || !d || !x || !r || !x_out) return XS_INVALID_ARGUMENT;
     const Operator op{g, mask, anchor, pb, true};
     const uint64_t n = cell_count(g);
     const unsigned grid = static_cast<unsigned>(std::min<uint64_t>((n + 255) / 256, 148 * 16));
-    if (fast_pass_ok(g, mask, anchor, pb, false))
-        fast_pass_kernel<kPassApply, float><<<fast_pass_blocks(g), 256, 0, st>>>(fast_geom(g, anchor, pb), d, nullptr, h.extra_product, 0.0f);
-    else
-        apply_operator_kernel<<<grid, 256, 0, st>>>(op, d, h.extra_product);
-    XsStatus s = check_launch();
-    if (s != XS_OK) return s;
+    XsStatus s;
+    if (fast_pass_ok(g, mask, anchor, pb, false)) {
+        // A d with the coefficient's products in one pass, then the update
+        const FastGeom f = fast_geom(g, anchor, pb);
+        const unsigned blocks = static_cast<unsigned>(std::min<uint64_t>((f.groups + 255) / 256, kGramBlocks));
+        line_gram_fast_kernel<<<blocks, 256, 0, st>>>(f, d, r, h.extra_product, h.partials);
+        if ((s = check_launch()) != XS_OK) return s;
+        basis_solve_kernel<1><<<1, 64, 0, st>>>(h.partials, blocks, h.coef);
+        if ((s = check_launch()) != XS_OK) return s;
+        line_update4_kernel<<<fast_pass_blocks(g), 256, 0, st>>>(f.groups, h.coef, d, h.extra_product, x, r, x_out);
+        return check_launch();
+    }
+    apply_operator_kernel<<<grid, 256, 0, st>>>(op, d, h.extra_product);
+    if ((s = check_launch()) != XS_OK) return s;
     // the Galerkin machinery with the one vector d and b = r (r already holds
     // the fixed boundary values; r and A d vanish on inactive cells):
     // coef = (d . r) / (d . A d)

@@ -103,7 +103,7 @@ struct WarmHistory {
     float* coarsest_solution; // (coarsest cells)
     void* coarsest_solver;    // pressure workspace of the coarsest grid
     // eigenbases of the coarse grid's axes (coarse grids within kSpectralMax)
-    float* spectral_basis;    // 3 kSpectralMax^2
+    float* spectral_basis;    // 6 kSpectralMax^2 (each axis' basis and its transpose)
     float* spectral_eigen;    // 3 kSpectralMax
 };
 // Exact coarse solve for operators that separate by axis (spectral.cu):
@@ -117,7 +117,7 @@ struct SpectralAxes {
 // none) separates; fills the axis description.
 bool spectral_axes(const Grid& c, const XsScalarBoundary& pb, uint32_t anchor, SpectralAxes& out);
 // x = A^-1 rhs on grid c by the axes' eigenbases (built into basis /
-// eigen: 3 kSpectralMax^2 and 3 kSpectralMax floats).
+// eigen: 6 kSpectralMax^2 and 3 kSpectralMax floats).
 XsStatus spectral_solve(cudaStream_t st, const Grid& c, const SpectralAxes& ax, float* basis, float* eigen, const double* rhs, float* x);
 constexpr double kCoarseTolerance = 1e-2;
 constexpr uint32_t kCoarseMaxIterations = 1000;

@@ -31,8 +31,7 @@ namespace {
 
 enum AxisKind : int { kZeroZero = 0, kFixedFixed = 1, kZeroFixed = 2, kFixedZero = 3, kPeriodicAxis = 4 };
 
-constexpr int kLines = 32;         // lines per tile (adjacent in memory for the strided axes)
-constexpr int kTransformThreads = 256;  // 8 warps x 4 lines
+constexpr int kTransformThreads = 256;  // 8 warps
 
 // Basis entry Q[j][k] (spatial index j, mode k) and eigenvalue of mode k of
 // a 1D operator of length n, in FP64.
@@ -67,15 +66,17 @@ __device__ double eigenvalue(int kind, int n, int k) {
     }
 }
 
-// basis: 3 x kSpectralMax x kSpectralMax (row j, column k; zero beyond n),
-// eigen: 3 x kSpectralMax.
+// basis: per axis a, Q (row j, column k) at a * 2 P^2 and its transpose at
+// a * 2 P^2 + P^2 (P = kSpectralMax; zero beyond n); eigen: 3 x P.
 __global__ void spectral_basis_kernel(SpectralAxes ax, float* __restrict__ basis, float* __restrict__ eigen) {
     constexpr int P = kSpectralMax;
     const int i = static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
     if (i >= 3 * P * P) return;
     const int a = i / (P * P), j = (i / P) % P, k = i % P;
     const int n = ax.n[a];
-    basis[i] = (j < n && k < n) ? static_cast<float>(basis_entry(ax.kind[a], n, j, k)) : 0.0f;
+    const float q = (j < n && k < n) ? static_cast<float>(basis_entry(ax.kind[a], n, j, k)) : 0.0f;
+    basis[static_cast<size_t>(a) * 2 * P * P + j * P + k] = q;
+    basis[static_cast<size_t>(a) * 2 * P * P + P * P + k * P + j] = q;
     if (j == 0) eigen[a * P + k] = k < n ? static_cast<float>(eigenvalue(ax.kind[a], n, k)) : 0.0f;
 }
 
@@ -90,8 +91,8 @@ struct LineSet {
     __device__ __forceinline__ uint64_t base(uint32_t L) const { return static_cast<uint64_t>(L % inner) * s_in + static_cast<uint64_t>(L / inner) * s_out; }
 };
 
-// Eigenvalue sums of the last axis' lines for the scaling pass: line L holds
-// modes (L % inner, L / inner) of the two axes transformed before.
+// Eigenvalue sums for the scaling of the last axis: line L holds modes
+// (L % inner, L / inner) of the two axes transformed before.
 struct LineScale {
     const float* lam_a;  // indexed by L % inner
     const float* lam_b;  // indexed by L / inner
@@ -99,129 +100,134 @@ struct LineScale {
     uint32_t inner;
 };
 
-constexpr size_t transform_smem(int np) { return sizeof(float) * static_cast<size_t>(np + kLines) * (np + 1); }
+constexpr int kWarpLines = 8;                                  // lines per warp
+constexpr int kTileLines = kWarpLines * kTransformThreads / 32;  // 64 lines per tile
+constexpr int pitch(int np) { return np + 4; }                 // 16-byte rows
+constexpr size_t transform_smem(int np) { return sizeof(float) * static_cast<size_t>(np + kTileLines) * pitch(np); }
 
-// Tiles of 32 lines: loaded into shared memory (coalesced), transformed
-// against the basis in shared memory (row pitch np + 1: row and column
-// walks are both free of bank conflicts), written back in place.  kMode 0:
-// c_k = sum_j Q[j][k] v_j; 1: v_j = sum_k Q[j][k] c_k; 2: forward, divide by
-// the eigenvalue sum, inverse (the last axis).  Each warp owns four lines,
-// each lane the outputs lane, lane + 32, ... .
-template <int NP, int kMode, class Tin>
-__global__ void __launch_bounds__(kTransformThreads) line_transform_kernel(const Tin* in, float* out, LineSet ls, const float* __restrict__ q,
-                                                                         LineScale sc) {
-    constexpr int R = NP + 1;
-    constexpr int Q4 = NP / 32;
-    extern __shared__ float smem[];
-    float* ms = smem;           // NP x R
-    float* d = smem + NP * R;   // kLines x R
-    const int t = static_cast<int>(threadIdx.x), lane = t & 31, l0 = (t >> 5) * 4;
-    for (int i = t; i < NP * NP; i += kTransformThreads) ms[(i / NP) * R + i % NP] = q[(i / NP) * kSpectralMax + i % NP];
+// out_l[k] = sum_j M[j][k] in_l[j] for tiles of 64 lines: the tile and M in
+// shared memory (16-byte rows), each warp 8 lines, each lane NP / 32
+// consecutive outputs, both operands read as 16-byte vectors (the tile's
+// as broadcasts).  M = Q gives the coefficients, M = Q^T (stored) the
+// values back; with kScale the coefficients are divided by their
+// eigenvalue sums (the last axis' forward pass).  In place: a tile is read
+// completely before it is written.
+template <int NP, bool kScale, class Tin>
+__global__ void __launch_bounds__(kTransformThreads, 2) line_transform_kernel(const Tin* in, float* out, LineSet ls, const float* __restrict__ m,
+                                                                            LineScale sc) {
+    constexpr int R = pitch(NP);
+    constexpr int OL = NP / 32;  // outputs per lane
+    extern __shared__ __align__(16) float smem[];
+    float* ms = smem;          // NP x R
+    float* d = smem + NP * R;  // kTileLines x R
+    const int t = static_cast<int>(threadIdx.x), lane = t & 31, l0 = (t >> 5) * kWarpLines;
+    // the matrix: 16-byte asynchronous copies, all in flight at once
+    for (int i = t; i < NP * NP / 4; i += kTransformThreads) {
+        const int row = i / (NP / 4), col = 4 * (i % (NP / 4));
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(ms + row * R + col))),
+                     "l"(m + row * kSpectralMax + col)
+                     : "memory");
+    }
+    asm volatile("cp.async.wait_all;" ::: "memory");
     const bool contiguous = ls.stride == 1;
-    const uint32_t tiles = (ls.lines + kLines - 1) / kLines;
+    const uint32_t tiles = (ls.lines + kTileLines - 1) / kTileLines;
+    constexpr int kPer = kTileLines * NP / kTransformThreads;  // tile elements per thread
+    constexpr int kBatch = 8;                                  // loads in flight per thread
+    static_assert(kPer % kBatch == 0, "");
     for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
-        const uint32_t L0 = tile * kLines;
-        __syncthreads();  // the basis is in place; the previous tile is written out
-        for (int i = t; i < kLines * NP; i += kTransformThreads) {
-            const int l = contiguous ? i / NP : i % kLines, j = contiguous ? i % NP : i / kLines;
-            const uint32_t L = L0 + l;
-            d[l * R + j] = (L < ls.lines && j < ls.n) ? static_cast<float>(in[ls.base(L) + static_cast<uint64_t>(j) * ls.stride]) : 0.0f;
-        }
-        __syncthreads();
-        float acc[4][Q4];
+        const uint32_t L0 = tile * kTileLines;
+        __syncthreads();  // the matrix is in place; the previous tile is written out
+        for (int b0 = 0; b0 < kPer; b0 += kBatch) {
+            float v[kBatch];
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+            for (int u = 0; u < kBatch; ++u) {
+                const int i = t + (b0 + u) * kTransformThreads;
+                const int l = contiguous ? i / NP : i % kTileLines, j = contiguous ? i % NP : i / kTileLines;
+                const uint32_t L = L0 + l;
+                v[u] = (L < ls.lines && j < ls.n) ? static_cast<float>(in[ls.base(L) + static_cast<uint64_t>(j) * ls.stride]) : 0.0f;
+            }
 #pragma unroll
-            for (int c = 0; c < Q4; ++c) acc[i][c] = 0.0f;
-        if (kMode != 1) {
-#pragma unroll 4
-            for (int j = 0; j < NP; ++j) {
-                float v[4], m[Q4];
-#pragma unroll
-                for (int i = 0; i < 4; ++i) v[i] = d[(l0 + i) * R + j];
-#pragma unroll
-                for (int c = 0; c < Q4; ++c) m[c] = ms[j * R + lane + 32 * c];
-#pragma unroll
-                for (int i = 0; i < 4; ++i)
-#pragma unroll
-                    for (int c = 0; c < Q4; ++c) acc[i][c] = fmaf(v[i], m[c], acc[i][c]);
+            for (int u = 0; u < kBatch; ++u) {
+                const int i = t + (b0 + u) * kTransformThreads;
+                const int l = contiguous ? i / NP : i % kTileLines, j = contiguous ? i % NP : i / kTileLines;
+                d[l * R + j] = v[u];
             }
         }
-        if (kMode == 2) {
+        __syncthreads();
+        float acc[kWarpLines][OL];
 #pragma unroll
-            for (int i = 0; i < 4; ++i) {
+        for (int i = 0; i < kWarpLines; ++i)
+#pragma unroll
+            for (int c = 0; c < OL; ++c) acc[i][c] = 0.0f;
+#pragma unroll 2
+        for (int j = 0; j < NP; j += 4) {
+            float4 v[kWarpLines];
+#pragma unroll
+            for (int i = 0; i < kWarpLines; ++i) v[i] = *reinterpret_cast<const float4*>(d + (l0 + i) * R + j);
+#pragma unroll
+            for (int jj = 0; jj < 4; ++jj) {
+                float w[OL];
+                if (OL == 4) {
+                    const float4 q = *reinterpret_cast<const float4*>(ms + (j + jj) * R + 4 * lane);
+                    w[0] = q.x; w[OL > 1 ? 1 : 0] = q.y; w[OL > 2 ? 2 : 0] = q.z; w[OL > 3 ? 3 : 0] = q.w;
+                } else {
+#pragma unroll
+                    for (int c = 0; c < OL; ++c) w[c] = ms[(j + jj) * R + OL * lane + c];
+                }
+#pragma unroll
+                for (int i = 0; i < kWarpLines; ++i) {
+                    const float x = jj == 0 ? v[i].x : (jj == 1 ? v[i].y : (jj == 2 ? v[i].z : v[i].w));
+#pragma unroll
+                    for (int c = 0; c < OL; ++c) acc[i][c] = fmaf(x, w[c], acc[i][c]);
+                }
+            }
+        }
+        if (kScale) {
+#pragma unroll
+            for (int i = 0; i < kWarpLines; ++i) {
                 const uint32_t L = L0 + l0 + i;
                 const float lam_ab = L < ls.lines ? sc.lam_a[L % sc.inner] + sc.lam_b[L / sc.inner] : 0.0f;
 #pragma unroll
-                for (int c = 0; c < Q4; ++c) {
-                    const int k = lane + 32 * c;
+                for (int c = 0; c < OL; ++c) {
+                    const int k = OL * lane + c;
                     const float lam = lam_ab + (k < ls.n ? sc.lam_line[k] : 0.0f);
                     acc[i][c] = (L < ls.lines && k < ls.n && lam > 0.0f) ? acc[i][c] / lam : 0.0f;
                 }
             }
-            __syncthreads();  // every warp has read its lines
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int c = 0; c < Q4; ++c) d[(l0 + i) * R + lane + 32 * c] = acc[i][c];
-            __syncthreads();
-        }
-        if (kMode != 0) {
-            float r[4][Q4];
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int c = 0; c < Q4; ++c) r[i][c] = 0.0f;
-#pragma unroll 4
-            for (int k = 0; k < NP; ++k) {
-                float v[4], m[Q4];
-#pragma unroll
-                for (int i = 0; i < 4; ++i) v[i] = d[(l0 + i) * R + k];
-#pragma unroll
-                for (int c = 0; c < Q4; ++c) m[c] = ms[(lane + 32 * c) * R + k];
-#pragma unroll
-                for (int i = 0; i < 4; ++i)
-#pragma unroll
-                    for (int c = 0; c < Q4; ++c) r[i][c] = fmaf(v[i], m[c], r[i][c]);
-            }
-#pragma unroll
-            for (int i = 0; i < 4; ++i)
-#pragma unroll
-                for (int c = 0; c < Q4; ++c) acc[i][c] = r[i][c];
         }
         __syncthreads();  // every warp has read its lines
 #pragma unroll
-        for (int i = 0; i < 4; ++i)
+        for (int i = 0; i < kWarpLines; ++i)
 #pragma unroll
-            for (int c = 0; c < Q4; ++c) d[(l0 + i) * R + lane + 32 * c] = acc[i][c];
+            for (int c = 0; c < OL; ++c) d[(l0 + i) * R + OL * lane + c] = acc[i][c];
         __syncthreads();
-        for (int i = t; i < kLines * NP; i += kTransformThreads) {
-            const int l = contiguous ? i / NP : i % kLines, j = contiguous ? i % NP : i / kLines;
+        for (int i = t; i < kTileLines * NP; i += kTransformThreads) {
+            const int l = contiguous ? i / NP : i % kTileLines, j = contiguous ? i % NP : i / kTileLines;
             const uint32_t L = L0 + l;
             if (L < ls.lines && j < ls.n) out[ls.base(L) + static_cast<uint64_t>(j) * ls.stride] = d[l * R + j];
         }
     }
 }
 
-template <int NP, int kMode, class Tin>
-XsStatus launch_transform(cudaStream_t st, const Tin* in, float* out, const LineSet& ls, const float* q, const LineScale& sc) {
+template <int NP, bool kScale, class Tin>
+XsStatus launch_transform(cudaStream_t st, const Tin* in, float* out, const LineSet& ls, const float* m, const LineScale& sc) {
     static DeviceOnce configured;
     const size_t smem = transform_smem(NP);
     if (!configured.run([smem] {
-            return cudaFuncSetAttribute(line_transform_kernel<NP, kMode, Tin>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+            return cudaFuncSetAttribute(line_transform_kernel<NP, kScale, Tin>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
         }))
         return XS_CUDA_ERROR;
-    const uint32_t tiles = (ls.lines + kLines - 1) / kLines;
+    const uint32_t tiles = (ls.lines + kTileLines - 1) / kTileLines;
     const unsigned blocks = std::min<uint32_t>(tiles, 2u * 148u);
-    line_transform_kernel<NP, kMode, Tin><<<blocks, kTransformThreads, smem, st>>>(in, out, ls, q, sc);
+    line_transform_kernel<NP, kScale, Tin><<<blocks, kTransformThreads, smem, st>>>(in, out, ls, m, sc);
     return check_launch();
 }
 
-template <int kMode, class Tin>
-XsStatus transform(cudaStream_t st, const Tin* in, float* out, const LineSet& ls, const float* q, const LineScale& sc) {
-    if (ls.n <= 32) return launch_transform<32, kMode, Tin>(st, in, out, ls, q, sc);
-    if (ls.n <= 64) return launch_transform<64, kMode, Tin>(st, in, out, ls, q, sc);
-    return launch_transform<128, kMode, Tin>(st, in, out, ls, q, sc);
+template <bool kScale, class Tin>
+XsStatus transform(cudaStream_t st, const Tin* in, float* out, const LineSet& ls, const float* m, const LineScale& sc) {
+    if (ls.n <= 32) return launch_transform<32, kScale, Tin>(st, in, out, ls, m, sc);
+    if (ls.n <= 64) return launch_transform<64, kScale, Tin>(st, in, out, ls, m, sc);
+    return launch_transform<128, kScale, Tin>(st, in, out, ls, m, sc);
 }
 
 }  // namespace
@@ -254,16 +260,16 @@ XsStatus spectral_solve(cudaStream_t st, const Grid& c, const SpectralAxes& ax, 
     const LineSet lx{static_cast<uint32_t>(ny * nz), 1u, 0u, nx, 1u, c.nx};
     const LineSet ly{static_cast<uint32_t>(nx * nz), static_cast<uint32_t>(nx), 1u, nx * ny, nx, c.ny};
     const LineSet lz{static_cast<uint32_t>(nx * ny), 1u, 0u, 1u, nx * ny, c.nz};
-    const float* qx = basis;
-    const float* qy = basis + P * P;
-    const float* qz = basis + 2 * P * P;
+    auto q = [&](int a) { return basis + static_cast<size_t>(a) * 2 * P * P; };       // Q: forward
+    auto qt = [&](int a) { return basis + static_cast<size_t>(a) * 2 * P * P + P * P; };  // Q^T: inverse
     const LineScale none{nullptr, nullptr, nullptr, 1u};
     const LineScale scale{eigen, eigen + P, eigen + 2 * P, static_cast<uint32_t>(nx)};
-    if ((s = transform<0, double>(st, rhs, x, lx, qx, none)) != XS_OK) return s;
-    if ((s = transform<0, float>(st, x, x, ly, qy, none)) != XS_OK) return s;
-    if ((s = transform<2, float>(st, x, x, lz, qz, scale)) != XS_OK) return s;
-    if ((s = transform<1, float>(st, x, x, ly, qy, none)) != XS_OK) return s;
-    return transform<1, float>(st, x, x, lx, qx, none);
+    if ((s = transform<false, double>(st, rhs, x, lx, q(0), none)) != XS_OK) return s;
+    if ((s = transform<false, float>(st, x, x, ly, q(1), none)) != XS_OK) return s;
+    if ((s = transform<true, float>(st, x, x, lz, q(2), scale)) != XS_OK) return s;
+    if ((s = transform<false, float>(st, x, x, lz, qt(2), none)) != XS_OK) return s;
+    if ((s = transform<false, float>(st, x, x, ly, qt(1), none)) != XS_OK) return s;
+    return transform<false, float>(st, x, x, lx, qt(0), none);
 }
 
 }  // namespace xs
@@ -272,7 +278,7 @@ using namespace xs;
 
 extern "C" {
 
-size_t xs_separable_solve_scratch_bytes(void) { return sizeof(float) * (3 * kSpectralMax * kSpectralMax + 3 * kSpectralMax); }
+size_t xs_separable_solve_scratch_bytes(void) { return sizeof(float) * (6 * kSpectralMax * kSpectralMax + 3 * kSpectralMax); }
 
 XsStatus xs_separable_solve(cudaStream_t stream, XsGrid grid, XsScalarBoundary pressure_boundary, uint32_t pressure_anchor,
                             const double* rhs, float* x, void* scratch) {
@@ -281,7 +287,7 @@ XsStatus xs_separable_solve(cudaStream_t stream, XsGrid grid, XsScalarBoundary p
     SpectralAxes ax;
     if (!spectral_axes(g, pressure_boundary, pressure_anchor, ax)) return XS_INVALID_ARGUMENT;
     float* basis = static_cast<float*>(scratch);
-    return spectral_solve(stream, g, ax, basis, basis + 3 * kSpectralMax * kSpectralMax, rhs, x);
+    return spectral_solve(stream, g, ax, basis, basis + 6 * kSpectralMax * kSpectralMax, rhs, x);
 }
 
 }  // extern "C"

@@ -328,15 +328,18 @@ typedef struct XsSmokeModel {
      * emptied by xs_smoke_reset_warm_start, which must run once after the
      * workspace is allocated. */
     uint32_t warm_start_history;
-    /* coarse-grid correction of the forward start (0: off; otherwise the
-     * coarsening factor per axis, which must divide the grid; needs
-     * warm_start_history > 0 and no colliders).  The ring's start takes 6
-     * damped Jacobi sweeps; their residual is restricted to the coarse grid,
-     * solved there by Jacobi-PCG to 1e-2 relative residual (from the same
-     * kind of start one level further down, when the coarse grid divides
-     * again) and interpolated back; the start then takes one energy-optimal
-     * step along it (before the learned correction's step).  It removes the
-     * smooth error that fine-grid CG reduces slowest. */
+    /* coarse-grid correction of the forward and adjoint starts (0: off;
+     * otherwise the coarsening factor per axis, which must divide the grid;
+     * needs warm_start_history > 0 and no colliders).  The ring's start takes
+     * 6 damped Jacobi sweeps; their residual is restricted to the coarse
+     * grid and solved there: exactly when its operator separates (no anchor
+     * cell, at most XS_SEPARABLE_SOLVE_MAX cells per coarse axis), otherwise
+     * by Jacobi-PCG to 1e-2 relative residual (from the same kind of start
+     * one level further down, when the coarse grid divides again).  The
+     * solution is interpolated back and the start takes one energy-optimal
+     * step along it (before the learned correction's step).  Forward solves
+     * take one such round, adjoint solves three.  It removes the smooth
+     * error that fine-grid CG reduces slowest. */
     uint32_t warm_start_coarsening;
     /* optional per-stage timing of xs_smoke_forward_step (NULL: none): an
      * array of XS_STEP_STAGES + 1 events created by the caller with timing
