@@ -162,13 +162,16 @@ XsStatus line_step(cudaStream_t st, const Grid& g, uint32_t anchor, const uint32
                    const float* d, const float* x, float* r, float* x_out);
 // Rounds of the start pipeline (sweeps + coarse-grid correction) before the
 // forward and the adjoint fine solves.  Measured at 256^3 (plume, steps
-// 180-204): the forward start leaves a relative residual of 2.8e-5 after one
-// round (7-9 fine iterations), and a second round saves 5 iterations for
-// about as much time as it costs; the adjoint start's ring predicts far
-// less (0.03-0.15 left, against 3e-3 forward), and each round takes a
-// further factor of about 7: 133 / 38 / 7 / 3 fine iterations after 1 / 2 /
-// 3 / 4 rounds.
-constexpr int kForwardStartCycles = 1;
+// 185-205, exact coarse solve): the forward start leaves a relative residual
+// of 2.8e-5 after one round (9 fine iterations) and 6.2e-6 after two (4):
+// 203.5 against 211.0 steps/s.  With the learned correction after the
+// rounds, one round and the network's step give 7 iterations, two rounds
+// and the step 4: 193.1 against 185.8 steps/s.  The adjoint start's ring
+// predicts far less (0.03-0.15 left, against 3e-3 forward), and each round
+// takes a further factor of about 7: 133 / 38 / 7 / 3 fine iterations after
+// 1 / 2 / 3 / 4 rounds.
+constexpr int kForwardStartCycles = 2;
+constexpr int kForwardStartCyclesLearned = 1;
 constexpr int kAdjointStartCycles = 3;
 // Iteration cap of the coarse Jacobi-PCG (grids without the exact coarse
 // solve) in rounds after the first: their residuals are rougher, and a

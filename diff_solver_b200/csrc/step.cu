@@ -50,7 +50,8 @@ XsStatus projection_forward(cudaStream_t st, const Grid& g, const XsPressureSolv
             // then sees its smooth error alone
             const float* x = h.ring_start;
             if (coarse) {
-                if ((s = coarse_cycles(st, g, anchor, pb, h, rhs, nullptr, kForwardStartCycles, &x)) != XS_OK) return s;
+                const int cycles = warm_start ? kForwardStartCyclesLearned : kForwardStartCycles;
+                if ((s = coarse_cycles(st, g, anchor, pb, h, rhs, nullptr, cycles, &x)) != XS_OK) return s;
             } else if ((s = start_residual(st, g, anchor, mask, pb, rhs, x, h.residual)) != XS_OK) {
                 return s;
             }

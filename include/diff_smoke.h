@@ -338,8 +338,9 @@ typedef struct XsSmokeModel {
      * one level further down, when the coarse grid divides again).  The
      * solution is interpolated back and the start takes one energy-optimal
      * step along it (before the learned correction's step).  Forward solves
-     * take one such round, adjoint solves three.  It removes the smooth
-     * error that fine-grid CG reduces slowest. */
+     * take two such rounds (one when the learned step follows), adjoint
+     * solves three.  It removes the smooth error that fine-grid CG reduces
+     * slowest. */
     uint32_t warm_start_coarsening;
     /* optional per-stage timing of xs_smoke_forward_step (NULL: none): an
      * array of XS_STEP_STAGES + 1 events created by the caller with timing
