@@ -151,8 +151,9 @@ __global__ void advect_velocity_vjp_kernel(const __grid_constant__ Grid g, uint6
 // atomics per face).  The same products as the general kernels; only the
 // order of the FP64 additions differs.
 // Halo 1: the box holds every stencil of traces shorter than half a cell per
-// step (longer ones scatter to global memory); the smaller boxes give four
-// CTAs per SM.
+// step (longer ones scatter to global memory); the smaller boxes give five
+// velocity-adjoint CTAs per SM (96 registers: 6.49 against 6.88 ms at 256^3
+// with four; six spill) and three density-and-temperature ones.
 using AdjointTile = tile::Shape<32, 4, 4, 1>;
 constexpr size_t kVelocityVjpSmem = 3 * AdjointTile::kNodes * (sizeof(double) + sizeof(float));
 constexpr size_t kScalarVjpSmem = 5 * AdjointTile::kNodes * (sizeof(double) + sizeof(float));
@@ -220,7 +221,7 @@ __device__ __forceinline__ void advect_velocity_vjp_tile_face(int x, int y, int 
     staged_trace_adjoint<A>(mid, m, der, src.gradient, o, li, acc, org, k, g, vb, ua, false);
 }
 
-__global__ void __launch_bounds__(AdjointTile::kThreads, 4) advect_velocity_vjp_tile_kernel(const __grid_constant__ Grid g, XsVector u, const __grid_constant__ XsVelocityBoundary vb,
+__global__ void __launch_bounds__(AdjointTile::kThreads, 5) advect_velocity_vjp_tile_kernel(const __grid_constant__ Grid g, XsVector u, const __grid_constant__ XsVelocityBoundary vb,
                                                                                           XsAdjointVector oa, XsAdjointVector ua) {
     using S = AdjointTile;
     extern __shared__ __align__(16) unsigned char smem_raw[];

@@ -1589,6 +1589,23 @@ __global__ void fast_push_kernel(FastGeom f, const float* __restrict__ pressure,
     }
 }
 
+// history_push_kernel<double> on the fast path (the adjoint ring: FP64
+// solutions, their products by the operator applied in FP64)
+__global__ void fast_push64_kernel(FastGeom f, const double* __restrict__ pressure, HistorySlots slots, HistorySlots products, uint32_t history,
+                                   const uint32_t* meta) {
+    const uint32_t k = min(meta[1], history - 1);
+    float* dst = slots.s[k];
+    float* prod = products.s[k];
+    for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < f.groups; t += gridDim.x * blockDim.x) {
+        const uint32_t i = 4u * t;
+        double c[4], ax[4];
+        float4 d;
+        apply4_fp64(f, pressure, i, c, ax, d);
+        st4(dst + i, make_float4(static_cast<float>(c[0]), static_cast<float>(c[1]), static_cast<float>(c[2]), static_cast<float>(c[3])));
+        st4(prod + i, make_float4(static_cast<float>(ax[0]), static_cast<float>(ax[1]), static_cast<float>(ax[2]), static_cast<float>(ax[3])));
+    }
+}
+
 __global__ void apply_operator_kernel(Operator op, const float* __restrict__ u, float* __restrict__ out) {
     const uint64_t n = cell_count(op.g);
     for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
@@ -1805,12 +1822,13 @@ __global__ void coarse_prolong_kernel(Grid g, Grid c, float inv_f, const float* 
 }
 
 // coarse_prolong_kernel for 4 consecutive fine cells of a row per thread
-// (nx a multiple of 4), the row from the launch grid: no index division, one
-// 16-byte store.  The same arithmetic per cell.
-__global__ void __launch_bounds__(128) coarse_prolong4_kernel(Grid g, Grid c, float inv_f, const float* __restrict__ ec, float* __restrict__ out) {
+// (nx a multiple of 4), rows and planes from the launch grid (32 x 8 threads
+// per block: 8 rows): no index division, one 16-byte store.  The same
+// arithmetic per cell.
+__global__ void __launch_bounds__(256) coarse_prolong4_kernel(Grid g, Grid c, float inv_f, const float* __restrict__ ec, float* __restrict__ out) {
     const int x = 4 * static_cast<int>(blockIdx.x * blockDim.x + threadIdx.x);
-    const int y = static_cast<int>(blockIdx.y), z = static_cast<int>(blockIdx.z);
-    if (x >= g.nx) return;
+    const int y = static_cast<int>(blockIdx.y * blockDim.y + threadIdx.y), z = static_cast<int>(blockIdx.z);
+    if (x >= g.nx || y >= g.ny) return;
     int y0, y1, z0, z1;
     float wy, wz;
     coarse_axis(y, c.ny, inv_f, y0, y1, wy);
@@ -1847,9 +1865,9 @@ XsStatus restrict_to(cudaStream_t st, const Grid& fine, const Grid& coarse, uint
 }
 
 XsStatus prolong_from(cudaStream_t st, const Grid& fine, const Grid& coarse, uint32_t f, const float* ec, float* out) {
-    if (fine.nx % 4 == 0 && fine.ny <= 65535 && fine.nz <= 65535) {
-        const dim3 grid(static_cast<unsigned>((fine.nx / 4 + 127) / 128), static_cast<unsigned>(fine.ny), static_cast<unsigned>(fine.nz));
-        coarse_prolong4_kernel<<<grid, 128, 0, st>>>(fine, coarse, 1.0f / static_cast<float>(f), ec, out);
+    if (fine.nx % 4 == 0 && fine.nz <= 65535) {
+        const dim3 grid(static_cast<unsigned>((fine.nx / 4 + 31) / 32), static_cast<unsigned>((fine.ny + 7) / 8), static_cast<unsigned>(fine.nz));
+        coarse_prolong4_kernel<<<grid, dim3(32, 8), 0, st>>>(fine, coarse, 1.0f / static_cast<float>(f), ec, out);
         return check_launch();
     }
     const uint64_t n = cell_count(fine);
@@ -1857,6 +1875,14 @@ XsStatus prolong_from(cudaStream_t st, const Grid& fine, const Grid& coarse, uin
         fine, coarse, 1.0f / static_cast<float>(f), ec, out);
     return check_launch();
 }
+
+}  // namespace
+
+XsStatus prolong_cells(cudaStream_t st, const Grid& fine, const Grid& coarse, uint32_t f, const float* ec, float* out) {
+    return prolong_from(st, fine, coarse, f, ec, out);
+}
+
+namespace {
 
 // the anchor moves to the coarse cell that contains it (n: none, on both grids)
 uint32_t coarse_anchor(const Grid& g, uint32_t f, const Grid& c, uint32_t anchor) {
@@ -2119,7 +2145,9 @@ XsStatus history_push(cudaStream_t st, const Grid& g, uint32_t anchor, const uin
     const Operator op{g, mask, anchor, pb, pressure64 == nullptr};
     const uint64_t n = cell_count(g);
     const unsigned blocks = static_cast<unsigned>(std::min<uint64_t>((n + 255) / 256, 148 * 16));
-    if (pressure64)
+    if (pressure64 && fast_pass_ok(g, mask, anchor, pb, false))
+        fast_push64_kernel<<<fast_pass_blocks(g), 256, 0, st>>>(fast_geom(g, anchor, pb), pressure64, slots, products, h.history, h.meta);
+    else if (pressure64)
         history_push_kernel<double><<<blocks, 256, 0, st>>>(op, pressure64, slots, products, h.history, h.meta);
     else if (fast_pass_ok(g, mask, anchor, pb, false))
         fast_push_kernel<<<fast_pass_blocks(g), 256, 0, st>>>(fast_geom(g, anchor, pb), pressure, slots, products, h.history, h.meta);

@@ -184,6 +184,9 @@ constexpr uint32_t kLaterCoarseIterations = 16;
 // without colliders only.
 XsStatus coarse_cycles(cudaStream_t st, const Grid& g, uint32_t anchor, const XsScalarBoundary& pb, const WarmHistory& h, const float* rhs,
                        const double* rhs_d, int cycles, const float** out);
+// Trilinear interpolation of a cell-centred field on the grid coarsened f
+// times (coarse) at the cell centres of `fine`, clamped at the edges.
+XsStatus prolong_cells(cudaStream_t st, const Grid& fine, const Grid& coarse, uint32_t f, const float* ec, float* out);
 // r = b + fixed boundary values - A x, or r = rhs_d - A x for the FP64
 // adjoint right-hand side (no fixed values) when rhs_d is given
 XsStatus start_residual(cudaStream_t st, const Grid& g, uint32_t anchor, const uint32_t* mask, const XsScalarBoundary& pb, const float* rhs,

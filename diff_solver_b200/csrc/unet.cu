@@ -39,6 +39,7 @@
 
 #include "common.cuh"
 #include "launch.cuh"
+#include "pressure.cuh"
 #include "unet.cuh"
 
 namespace xs {
@@ -459,43 +460,6 @@ __global__ void prolong_kernel(const __nv_bfloat16* __restrict__ out, uint32_t X
     }
 }
 
-// prolong_kernel for 4 consecutive fine cells of a row per thread (X a
-// multiple of 4), the row from the launch grid: no index division, one
-// 16-byte store; the same arithmetic per cell.
-__global__ void __launch_bounds__(128) prolong4_kernel(const __nv_bfloat16* __restrict__ out, uint32_t X, uint32_t Y, uint32_t Z, uint32_t f,
-                                                       float* __restrict__ guess) {
-    const uint32_t x = 4u * (blockIdx.x * blockDim.x + threadIdx.x), y = blockIdx.y, z = blockIdx.z;
-    if (x >= X) return;
-    const uint32_t cx = X / f, cy = Y / f, cz = Z / f;
-    const float inv = 1.0f / static_cast<float>(f);
-    auto axis = [&](uint32_t c, uint32_t n, int& a0, int& a1, float& w) {
-        float u = (static_cast<float>(c) + 0.5f) * inv - 0.5f;
-        u = fminf(fmaxf(u, 0.0f), static_cast<float>(n - 1));
-        a0 = min(static_cast<int>(u), static_cast<int>(n) - 1);
-        a1 = min(a0 + 1, static_cast<int>(n) - 1);
-        w = u - static_cast<float>(a0);
-    };
-    int y0, y1, z0, z1;
-    float wy, wz;
-    axis(y, cy, y0, y1, wy);
-    axis(z, cz, z0, z1, wz);
-    auto at = [&](int xx, int yy, int zz) { return __bfloat162float(out[((static_cast<uint64_t>(zz) * cy + yy) * cx + xx) * 16]); };
-    float v[4];
-#pragma unroll
-    for (int k = 0; k < 4; ++k) {
-        int x0, x1;
-        float wx;
-        axis(x + k, cx, x0, x1, wx);
-        const float c00 = at(x0, y0, z0) * (1 - wx) + at(x1, y0, z0) * wx;
-        const float c10 = at(x0, y1, z0) * (1 - wx) + at(x1, y1, z0) * wx;
-        const float c01 = at(x0, y0, z1) * (1 - wx) + at(x1, y0, z1) * wx;
-        const float c11 = at(x0, y1, z1) * (1 - wx) + at(x1, y1, z1) * wx;
-        const float c0 = c00 * (1 - wy) + c10 * wy, c1 = c01 * (1 - wy) + c11 * wy;
-        v[k] = c0 * (1 - wz) + c1 * wz;
-    }
-    *reinterpret_cast<float4*>(guess + (static_cast<uint64_t>(z) * Y + y) * X + x) = make_float4(v[0], v[1], v[2], v[3]);
-}
-
 // guess[v] = out_0[v] (network grid, every sample)
 __global__ void extract_kernel(const __nv_bfloat16* __restrict__ out, uint64_t total, float* __restrict__ guess) {
     for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < total; i += static_cast<uint64_t>(gridDim.x) * blockDim.x)
@@ -676,11 +640,18 @@ XsStatus warm_start_guess(WarmStartNet* n, cudaStream_t st, const Grid& g, const
     }
     if ((s = prepare_input(*n, st, coarse, 1)) != XS_OK) return s;
     if ((s = forward(*n, st, 1)) != XS_OK) return s;
-    if (g.nx % 4 == 0 && g.ny <= 65535 && g.nz <= 65535)
-        prolong4_kernel<<<dim3((g.nx / 4 + 127) / 128, g.ny, g.nz), 128, 0, st>>>(n->act[A_OUT], g.nx, g.ny, g.nz, f, n->fine_guess);
-    else
+    if (f > 1 && g.nx % 4 == 0) {
+        // the output channel into a compact FP32 array (the restricted
+        // right-hand side is no longer needed), then the 4-wide trilinear
+        // prolongation of the coarse-grid correction: the same arithmetic
+        extract_kernel<<<grid_for(voxels(l0)), 256, 0, st>>>(n->act[A_OUT], voxels(l0), n->coarse_rhs);
+        if ((s = check_launch()) != XS_OK) return s;
+        const Grid c{static_cast<int>(l0.x), static_cast<int>(l0.y), static_cast<int>(l0.z), g.h * static_cast<float>(f), g.dt};
+        if ((s = prolong_cells(st, g, c, f, n->coarse_rhs, n->fine_guess)) != XS_OK) return s;
+    } else {
         prolong_kernel<<<grid_for(voxels(l0) * f * f * f), 256, 0, st>>>(n->act[A_OUT], g.nx, g.ny, g.nz, f, n->fine_guess);
-    if ((s = check_launch()) != XS_OK) return s;
+        if ((s = check_launch()) != XS_OK) return s;
+    }
     *guess = n->fine_guess;
     return XS_OK;
 }

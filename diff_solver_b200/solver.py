@@ -91,15 +91,17 @@ def simulate(model, context, initial_state, controls: Sequence, parameters, tape
     return traj
 
 
-def _segment(model, context, traj: Trajectory, controls, parameters, start: int):
+def _segment(model, context, traj: Trajectory, controls, parameters, start: int, pool=None):
     """Recompute the checkpoint segment beginning at ``start``: returns the
-    states start..end and the caches of steps start..end-1."""
+    states start..end and the caches of steps start..end-1.  ``pool`` (states,
+    caches; at least one segment's worth) supplies the buffers, reused from
+    segment to segment: every step overwrites its state and cache."""
     end = min(start + traj.checkpoint_interval, traj.steps)
     states = [traj.state_at(start)]
     caches = []
-    for step in range(start, end):
-        nxt = model.allocate_state(context)
-        cache = model.allocate_step_cache(context)
+    for i, step in enumerate(range(start, end)):
+        nxt = pool[0][i] if pool else model.allocate_state(context)
+        cache = pool[1][i] if pool else model.allocate_step_cache(context)
         model.forward_step(states[-1], controls[step], parameters, nxt, cache, context)
         states.append(nxt)
         caches.append(cache)
@@ -162,6 +164,10 @@ def vjp(model, context, trajectory: Trajectory, controls: Sequence, parameters,
     rcache = model.allocate_step_cache(context) if (mode == TapeMode.recompute_step_cache and controls) else None
     spare = model.allocate_state_adjoint(context)
     seg_states, seg_caches, seg_start = None, None, -1
+    pool = None
+    if mode == TapeMode.checkpoint and controls:
+        k = min(trajectory.checkpoint_interval, T)
+        pool = ([model.allocate_state(context) for _ in range(k)], [model.allocate_step_cache(context) for _ in range(k)])
     for step in range(T - 1, -1, -1):
         if mode == TapeMode.store_all:
             state, nxt, cache = trajectory.states[step], trajectory.states[step + 1], trajectory.step_caches[step]
@@ -171,7 +177,7 @@ def vjp(model, context, trajectory: Trajectory, controls: Sequence, parameters,
         else:
             start = step - step % trajectory.checkpoint_interval
             if start != seg_start:
-                seg_states, seg_caches = _segment(model, context, trajectory, controls, parameters, start)
+                seg_states, seg_caches = _segment(model, context, trajectory, controls, parameters, start, pool)
                 seg_start = start
             state, nxt, cache = seg_states[step - start], seg_states[step - start + 1], seg_caches[step - start]
         model.zero_state_adjoint(spare, context)
