@@ -536,9 +536,11 @@ def adjoint_record(args, shape, network, start_state, window=40, checkpoint=8):
     off = N.lib().xs_solve_stats_offset()
     stats_dev = ctx.workspace[off:off + C.sizeof(N.XsSolveStats)]
     stats_host = torch.zeros((window, C.sizeof(N.XsSolveStats)), dtype=torch.uint8).pin_memory()
+    torch.cuda.nvtx.range_push("reverse")  # the reverse pass, for profilers
     grad = vjp(model, ctx, traj, controls, params, {window: seed},
                after_step=lambda step: stats_host[step].copy_(stats_dev, non_blocking=True))
     ev[2].record()
+    torch.cuda.nvtx.range_pop()
     torch.cuda.synchronize()
     per_step = [N.XsSolveStats.from_buffer_copy(bytes(stats_host[i].numpy())) for i in range(window)]
     stats = ctx.read_solve_stats()

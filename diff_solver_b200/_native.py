@@ -71,7 +71,7 @@ class XsSmokeModel(C.Structure):
                 ("inflows", C.c_void_p), ("inflow_count", C.c_uint32), ("cell_mask", C.c_void_p), ("collider_velocity", XsVector),
                 ("collider_density", C.c_void_p), ("collider_temperature", C.c_void_p), ("solve_begin", C.c_void_p),
                 ("solve_end", C.c_void_p), ("warm_start", C.c_void_p), ("warm_start_history", C.c_uint32),
-                ("warm_start_coarsening", C.c_uint32), ("stage_events", C.c_void_p)]
+                ("warm_start_coarsening", C.c_uint32), ("warm_start_rounds", C.c_uint32), ("stage_events", C.c_void_p)]
 
 
 XS_STEP_STAGES = 9

@@ -74,6 +74,7 @@ struct WarmHistory {
     float* slots[kMaxBasis];
     float* products[kMaxBasis];  // A slot, computed when the slot is written
     uint32_t history;   // ring slots (0: off)
+    uint32_t forward_rounds;  // start rounds before a forward solve (0: defaults)
     uint32_t* meta;     // device: [0] valid slots, [1] next slot
     float* start;       // the start vector of the last forward solve (N)
     float* ring_start;  // the Galerkin start from the ring alone (N)
@@ -173,6 +174,7 @@ XsStatus line_step(cudaStream_t st, const Grid& g, uint32_t anchor, const uint32
 constexpr int kForwardStartCycles = 2;
 constexpr int kForwardStartCyclesLearned = 1;
 constexpr int kAdjointStartCycles = 3;
+constexpr uint32_t kMaxStartRounds = 8;
 // Iteration cap of the coarse Jacobi-PCG (grids without the exact coarse
 // solve) in rounds after the first: their residuals are rougher, and a
 // solve to kCoarseTolerance took 60-260 iterations for little gain.

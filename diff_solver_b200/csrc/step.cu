@@ -50,7 +50,8 @@ XsStatus projection_forward(cudaStream_t st, const Grid& g, const XsPressureSolv
             // then sees its smooth error alone
             const float* x = h.ring_start;
             if (coarse) {
-                const int cycles = warm_start ? kForwardStartCyclesLearned : kForwardStartCycles;
+                const int cycles = h.forward_rounds ? static_cast<int>(h.forward_rounds)
+                                                    : (warm_start ? kForwardStartCyclesLearned : kForwardStartCycles);
                 if ((s = coarse_cycles(st, g, anchor, pb, h, rhs, nullptr, cycles, &x)) != XS_OK) return s;
             } else if ((s = start_residual(st, g, anchor, mask, pb, rhs, x, h.residual)) != XS_OK) {
                 return s;
@@ -161,7 +162,7 @@ StepWorkspace carve_step(void* base, const Grid& g, uint32_t mode, uint32_t hist
 
 bool valid_model(const XsSmokeModel* m) {
     if (m == nullptr || !valid_grid(m->grid) || m->inflow_count > XS_MAX_INFLOWS || (m->inflow_count != 0 && m->inflows == nullptr) ||
-        m->warm_start_history > static_cast<uint32_t>(kMaxHistory))
+        m->warm_start_history > static_cast<uint32_t>(kMaxHistory) || m->warm_start_rounds > kMaxStartRounds)
         return false;
     if (m->warm_start_coarsening != 0) {  // a divisible grid, a ring, no colliders
         Grid c;
@@ -311,9 +312,11 @@ XsStatus xs_smoke_forward_step(cudaStream_t stream, const XsSmokeModel* m, XsSta
     if (s != XS_OK) return s;
     if ((s = mark_stage(stream, ev, 3)) != XS_OK) return s;
     // projection
+    WarmHistory history = w.history;
+    history.forward_rounds = m->warm_start_rounds;
     s = projection_forward(stream, g, m->pressure, m->pressure_anchor, m->cell_mask, cache.advected_velocity, m->pressure_boundary,
                            w.pressure, w.rhs, next_state.velocity, w.solver, m->solve_begin, m->solve_end,
-                           reinterpret_cast<WarmStartNet*>(m->warm_start), &w.history, ev ? ev + 4 : nullptr);
+                           reinterpret_cast<WarmStartNet*>(m->warm_start), &history, ev ? ev + 4 : nullptr);
     if (s != XS_OK) return s;
     // scalar advection of the sourced fields through the projected velocity
     s = launch_advect_scalar_pair(stream, g, m->cell_mask, m->collider_density, m->collider_temperature, cache.sourced_density,

@@ -156,6 +156,8 @@ class Configuration:
     # coarse-grid correction of that start (0: off; else the coarsening
     # factor per axis, dividing the grid; needs a ring and no colliders)
     warm_start_coarsening: int = 0
+    # rounds of sweeps and coarse-grid correction before a forward solve (0: defaults)
+    warm_start_rounds: int = 0
 
 
 def plume_configuration(n=(64, 64, 64), cell_size=None, inflow_center=(0.5, 0.1, 0.5), inflow_radius=0.08,

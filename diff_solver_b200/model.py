@@ -291,6 +291,7 @@ class Model:
         m.collider_temperature = ct.data_ptr() if has_colliders else None
         m.warm_start_history = int(cfg.warm_start_history)
         m.warm_start_coarsening = int(cfg.warm_start_coarsening)
+        m.warm_start_rounds = int(cfg.warm_start_rounds)
         ctx.native = m
         nbytes = L.xs_smoke_workspace_bytes(C.byref(m), int(mode))
         if nbytes == 0:

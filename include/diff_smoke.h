@@ -337,11 +337,14 @@ typedef struct XsSmokeModel {
      * by Jacobi-PCG to 1e-2 relative residual (from the same kind of start
      * one level further down, when the coarse grid divides again).  The
      * solution is interpolated back and the start takes one energy-optimal
-     * step along it (before the learned correction's step).  Forward solves
-     * take two such rounds (one when the learned step follows), adjoint
-     * solves three.  It removes the smooth error that fine-grid CG reduces
-     * slowest. */
+     * step along it (before the learned correction's step), in rounds
+     * (warm_start_rounds).  It removes the smooth error that fine-grid CG
+     * reduces slowest. */
     uint32_t warm_start_coarsening;
+    /* rounds of sweeps and coarse-grid correction before a forward solve
+     * (0: the defaults, two without a learned warm start and one before its
+     * step; at most 8).  Adjoint solves always take three. */
+    uint32_t warm_start_rounds;
     /* optional per-stage timing of xs_smoke_forward_step (NULL: none): an
      * array of XS_STEP_STAGES + 1 events created by the caller with timing
      * enabled, recorded on the step's stream at the stage boundaries:

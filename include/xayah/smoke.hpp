@@ -96,6 +96,8 @@ struct Configuration {
     // coarse-grid correction of that start (0: off; else the coarsening factor
     // per axis, dividing the grid; needs a ring and no colliders)
     std::uint32_t warm_start_coarsening{0u};
+    // rounds of sweeps and coarse-grid correction before a forward solve (0: defaults)
+    std::uint32_t warm_start_rounds{0u};
 };
 
 // ------------------------------------------------------------- data.ixx:85-204
@@ -266,6 +268,7 @@ public:
         m.collider_temperature = colliders ? ctx.domain.collider_temperature.values.data : nullptr;
         m.warm_start_history = configuration.warm_start_history;
         m.warm_start_coarsening = configuration.warm_start_coarsening;
+        m.warm_start_rounds = configuration.warm_start_rounds;
         const std::size_t bytes = xs_smoke_workspace_bytes(&m, static_cast<std::uint32_t>(mode));
         if (bytes == 0) throw std::invalid_argument("invalid smoke configuration");
         ctx.workspace_ = cuda::Buffer<unsigned char>(ctx.resource, bytes);
