@@ -77,6 +77,9 @@ __global__ void integrate_vjp_faces_kernel(uint64_t n, const double* __restrict_
 
 // operators.cu:366-379, force part gathered per fluid cell: each of the cell's
 // two faces along axis a hands dt * oa / (fluid cells beside that face).
+// kAssign: the force adjoint is written instead of accumulated (a caller
+// whose force adjoint starts at zero skips clearing it).
+template <bool kAssign>
 __global__ void integrate_vjp_cells_kernel(Grid g, const uint32_t* __restrict__ mask, XsAdjointVector oa, XsAdjointVector fa) {
     const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i >= cell_count(g) || is_solid(mask, i)) return;
@@ -90,7 +93,32 @@ __global__ void integrate_vjp_cells_kernel(Grid g, const uint32_t* __restrict__ 
         const double lo = o[idx3(x, y, z, ex, ey)] / fluid_neighbours_of_face(g, mask, a, x, y, z);
         const double hi = o[idx3(ux, uy, uz, ex, ey)] / fluid_neighbours_of_face(g, mask, a, ux, uy, uz);
         double* f = component<double>(fa.x, fa.y, fa.z, a);
-        f[i] += static_cast<double>(g.dt) * lo + static_cast<double>(g.dt) * hi;
+        const double v = static_cast<double>(g.dt) * lo + static_cast<double>(g.dt) * hi;
+        if (kAssign) f[i] = v; else f[i] += v;
+    }
+}
+
+// The same without colliders: a face has two fluid cells beside it unless it
+// lies on the domain boundary (one), so the division by the count is an exact
+// halving or nothing; bit-identical to integrate_vjp_cells_kernel.
+template <bool kAssign>
+__global__ void integrate_vjp_open_cells_kernel(Grid g, XsAdjointVector oa, XsAdjointVector fa) {
+    const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
+    if (i >= cell_count(g)) return;
+    int x, y, z;
+    decode(i, g.nx, g.ny, x, y, z);
+#pragma unroll
+    for (int a = 0; a < 3; ++a) {
+        const int ex = extent(g, a, 0), ey = extent(g, a, 1);
+        const double* o = component<double>(oa.x, oa.y, oa.z, a);
+        const int ux = x + (a == 0), uy = y + (a == 1), uz = z + (a == 2);
+        const int c = a == 0 ? x : (a == 1 ? y : z), n = a == 0 ? g.nx : (a == 1 ? g.ny : g.nz);
+        double lo = o[idx3(x, y, z, ex, ey)], hi = o[idx3(ux, uy, uz, ex, ey)];
+        if (c > 0) lo *= 0.5;
+        if (c + 1 < n) hi *= 0.5;
+        double* f = component<double>(fa.x, fa.y, fa.z, a);
+        const double v = static_cast<double>(g.dt) * lo + static_cast<double>(g.dt) * hi;
+        if (kAssign) f[i] = v; else f[i] += v;
     }
 }
 
@@ -388,6 +416,7 @@ __device__ __forceinline__ bool constrained_or_solid(int a, int x, int y, int z,
     return false;
 }
 
+template <bool kAssign>
 __global__ void constrain_vjp_kernel(Grid g, uint64_t f0, uint64_t f1, uint64_t f2, const uint32_t* __restrict__ mask, XsAdjointVector oa,
                                      XsVelocityBoundary b, XsAdjointVector ua) {
     const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -408,7 +437,8 @@ __global__ void constrain_vjp_kernel(Grid g, uint64_t f0, uint64_t f1, uint64_t 
         const int px = a == 0 ? mx : x, py = a == 1 ? mx : y, pz = a == 2 ? mx : z;
         if (!constrained_or_solid(a, px, py, pz, g, mask, b)) acc += o[idx3(px, py, pz, ex, ey)];
     }
-    if (acc != 0.0) component<double>(ua.x, ua.y, ua.z, a)[local] += acc;
+    if (kAssign) component<double>(ua.x, ua.y, ua.z, a)[local] = acc;
+    else if (acc != 0.0) component<double>(ua.x, ua.y, ua.z, a)[local] += acc;
 }
 
 // ---------------------------------------------------------------- projection
@@ -442,6 +472,7 @@ __global__ void project_reverse_cells_kernel(Grid g, const uint32_t* __restrict_
 // operators.cu:957-969 gathered per face, plus the face part of :922-933
 // (velocity adjoint += output adjoint).  scale(c) = -h * rhs_adj(c) / dt for
 // fluid, non-anchor cells; the face gets scale(lower) - scale(upper).
+template <bool kAssign>
 __global__ void pressure_rhs_reverse_kernel(Grid g, uint64_t f0, uint64_t f1, uint64_t f2, uint32_t anchor, const uint32_t* __restrict__ mask,
                                             const double* __restrict__ rhs_adj, XsAdjointVector oa, XsAdjointVector ua) {
     const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
@@ -462,7 +493,8 @@ __global__ void pressure_rhs_reverse_kernel(Grid g, uint64_t f0, uint64_t f1, ui
         const uint64_t c = idx3(x, y, z, g.nx, g.ny);
         if (!is_solid(mask, c) && c != anchor) acc -= k * rhs_adj[c];
     }
-    component<double>(ua.x, ua.y, ua.z, a)[local] += acc;
+    if (kAssign) component<double>(ua.x, ua.y, ua.z, a)[local] = acc;
+    else component<double>(ua.x, ua.y, ua.z, a)[local] += acc;
 }
 
 // ---------------------------------------------------------------- launchers
@@ -481,14 +513,22 @@ XsStatus launch_buoyancy_vjp(cudaStream_t st, const Grid& g, const uint32_t* mas
 }
 
 XsStatus launch_integrate_vjp(cudaStream_t st, const Grid& g, const uint32_t* mask, const XsAdjointVector& oa, const XsAdjointVector& ua,
-                              const XsAdjointVector& fa) {
+                              const XsAdjointVector& fa, bool assign_force) {
     for (int a = 0; a < 3; ++a) {
         const uint64_t n = face_count(g, a);
         integrate_vjp_faces_kernel<<<blocks_for(n), kBlock, 0, st>>>(n, component<double>(oa.x, oa.y, oa.z, a),
                                                                      component<double>(ua.x, ua.y, ua.z, a));
         if (check_launch() != XS_OK) return XS_CUDA_ERROR;
     }
-    integrate_vjp_cells_kernel<<<blocks_for(cell_count(g)), kBlock, 0, st>>>(g, mask, oa, fa);
+    const unsigned blocks = blocks_for(cell_count(g));
+    if (mask == nullptr && assign_force)
+        integrate_vjp_open_cells_kernel<true><<<blocks, kBlock, 0, st>>>(g, oa, fa);
+    else if (mask == nullptr)
+        integrate_vjp_open_cells_kernel<false><<<blocks, kBlock, 0, st>>>(g, oa, fa);
+    else if (assign_force)
+        integrate_vjp_cells_kernel<true><<<blocks, kBlock, 0, st>>>(g, mask, oa, fa);
+    else
+        integrate_vjp_cells_kernel<false><<<blocks, kBlock, 0, st>>>(g, mask, oa, fa);
     return check_launch();
 }
 
@@ -533,9 +573,12 @@ XsStatus launch_advect_scalar_vjp(cudaStream_t st, const Grid& g, const uint32_t
 }
 
 XsStatus launch_constrain_vjp(cudaStream_t st, const Grid& g, const uint32_t* mask, const XsAdjointVector& oa, const XsVelocityBoundary& b,
-                              const XsAdjointVector& ua) {
+                              const XsAdjointVector& ua, bool assign) {
     const uint64_t f0 = face_count(g, 0), f1 = face_count(g, 1), f2 = face_count(g, 2);
-    constrain_vjp_kernel<<<blocks_for(f0 + f1 + f2), kBlock, 0, st>>>(g, f0, f1, f2, mask, oa, b, ua);
+    if (assign)
+        constrain_vjp_kernel<true><<<blocks_for(f0 + f1 + f2), kBlock, 0, st>>>(g, f0, f1, f2, mask, oa, b, ua);
+    else
+        constrain_vjp_kernel<false><<<blocks_for(f0 + f1 + f2), kBlock, 0, st>>>(g, f0, f1, f2, mask, oa, b, ua);
     return check_launch();
 }
 
@@ -544,7 +587,7 @@ XsStatus launch_constrain_vjp(cudaStream_t st, const Grid& g, const uint32_t* ma
 // or reverse-swept (RBGS kind), and the divergence transpose is added.
 XsStatus projection_vjp(cudaStream_t st, const Grid& g, const XsPressureSolve& solve, uint32_t anchor, const uint32_t* mask,
                         const XsAdjointVector& oa, const XsScalarBoundary& pb, double* pa, double* ra, const XsAdjointVector& ua,
-                        void* workspace, const WarmHistory* history) {
+                        void* workspace, const WarmHistory* history, bool assign) {
     project_reverse_cells_kernel<<<blocks_for(cell_count(g)), kBlock, 0, st>>>(g, mask, oa, pa);
     if (check_launch() != XS_OK) return XS_CUDA_ERROR;
     XsStatus s;
@@ -578,7 +621,10 @@ XsStatus projection_vjp(cudaStream_t st, const Grid& g, const XsPressureSolve& s
     }
     if (s != XS_OK) return s;
     const uint64_t f0 = face_count(g, 0), f1 = face_count(g, 1), f2 = face_count(g, 2);
-    pressure_rhs_reverse_kernel<<<blocks_for(f0 + f1 + f2), kBlock, 0, st>>>(g, f0, f1, f2, anchor, mask, ra, oa, ua);
+    if (assign)
+        pressure_rhs_reverse_kernel<true><<<blocks_for(f0 + f1 + f2), kBlock, 0, st>>>(g, f0, f1, f2, anchor, mask, ra, oa, ua);
+    else
+        pressure_rhs_reverse_kernel<false><<<blocks_for(f0 + f1 + f2), kBlock, 0, st>>>(g, f0, f1, f2, anchor, mask, ra, oa, ua);
     return check_launch();
 }
 

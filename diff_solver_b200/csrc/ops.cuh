@@ -38,18 +38,20 @@ XsStatus launch_source_vjp(cudaStream_t st, const Grid& g, const uint32_t* mask,
 XsStatus launch_buoyancy_vjp(cudaStream_t st, const Grid& g, const uint32_t* mask, const float* rho, const float* temp, const float* ambient,
                              const float* beta_rho, const float* beta_temp, const XsAdjointVector& fa, double* rho_a, double* temp_a,
                              const XsAdjointVector& ea, double* amb_a, double* br_a, double* bt_a);
+// assign_force / assign: the force / velocity adjoint is written instead of
+// accumulated (the step's scratch adjoints, which start at zero)
 XsStatus launch_integrate_vjp(cudaStream_t st, const Grid& g, const uint32_t* mask, const XsAdjointVector& oa, const XsAdjointVector& ua,
-                              const XsAdjointVector& fa);
+                              const XsAdjointVector& fa, bool assign_force = false);
 XsStatus launch_advect_velocity_vjp(cudaStream_t st, const Grid& g, const uint32_t* mask, const XsVector& u, const XsVelocityBoundary& vb,
                                     const XsAdjointVector& oa, const XsAdjointVector& ua);
 XsStatus launch_advect_scalar_vjp(cudaStream_t st, const Grid& g, const uint32_t* mask, const float* src, const XsScalarBoundary& sb,
                                   const double* oa, double* sa, const float* src2, const XsScalarBoundary& sb2, const double* oa2,
                                   double* sa2, const XsVector& u, const XsVelocityBoundary& vb, const XsAdjointVector& ua);
 XsStatus launch_constrain_vjp(cudaStream_t st, const Grid& g, const uint32_t* mask, const XsAdjointVector& oa, const XsVelocityBoundary& b,
-                              const XsAdjointVector& ua);
+                              const XsAdjointVector& ua, bool assign = false);
 XsStatus projection_vjp(cudaStream_t st, const Grid& g, const XsPressureSolve& solve, uint32_t anchor, const uint32_t* mask,
                         const XsAdjointVector& oa, const XsScalarBoundary& pb, double* pa, double* ra, const XsAdjointVector& ua,
-                        void* workspace, const WarmHistory* history = nullptr);
+                        void* workspace, const WarmHistory* history = nullptr, bool assign = false);
 
 // tangent.cu
 XsStatus launch_source_jvp_pair(cudaStream_t st, const Grid& g, const uint32_t* mask, const float* rho_t, const float* temp_t,

@@ -389,17 +389,15 @@ XsStatus xs_smoke_vjp_step(cudaStream_t stream, const XsSmokeModel* m, XsState s
     const InflowSet inflows = make_inflows(m->inflows, m->inflow_count);
     const uint64_t n = cell_count(g), f0 = face_count(g, 0), f1 = face_count(g, 1), f2 = face_count(g, 2);
     XsStatus s;
-    // scratch adjoints start at zero (model.cpp:362-378)
+    // scratch adjoints start at zero (model.cpp:362-378): those accumulated
+    // by scatters are cleared; the advected, raw and force adjoints are
+    // written whole by the first operator that produces them instead
     if ((s = zero(stream, w.sourced_rho_a, 8 * n)) != XS_OK) return s;
     if ((s = zero(stream, w.sourced_temp_a, 8 * n)) != XS_OK) return s;
-    for (double* p : {w.force_a.x, w.force_a.y, w.force_a.z})
-        if ((s = zero(stream, p, 8 * n)) != XS_OK) return s;
     const size_t fb[3] = {8 * f0, 8 * f1, 8 * f2};
-    for (const XsAdjointVector* v : {&w.advected_a, &w.raw_a, &w.forced_a}) {
-        if ((s = zero(stream, v->x, fb[0])) != XS_OK) return s;
-        if ((s = zero(stream, v->y, fb[1])) != XS_OK) return s;
-        if ((s = zero(stream, v->z, fb[2])) != XS_OK) return s;
-    }
+    if ((s = zero(stream, w.forced_a.x, fb[0])) != XS_OK) return s;
+    if ((s = zero(stream, w.forced_a.y, fb[1])) != XS_OK) return s;
+    if ((s = zero(stream, w.forced_a.z, fb[2])) != XS_OK) return s;
     // lambda of the projected velocity starts as the incoming adjoint (model.cpp:379-381)
     if ((s = check_cuda(cudaMemcpyAsync(w.projected_a.x, na.velocity.x, fb[0], cudaMemcpyDeviceToDevice, stream))) != XS_OK) return s;
     if ((s = check_cuda(cudaMemcpyAsync(w.projected_a.y, na.velocity.y, fb[1], cudaMemcpyDeviceToDevice, stream))) != XS_OK) return s;
@@ -411,14 +409,14 @@ XsStatus xs_smoke_vjp_step(cudaStream_t stream, const XsSmokeModel* m, XsState s
     if (s != XS_OK) return s;
     // projection
     s = projection_vjp(stream, g, m->pressure, m->pressure_anchor, m->cell_mask, w.projected_a, m->pressure_boundary, w.pressure_a, w.rhs_a,
-                       w.advected_a, w.solver, &w.adjoint_history);
+                       w.advected_a, w.solver, &w.adjoint_history, true);
     if (s != XS_OK) return s;
     // velocity evolution: constrain, advect, integrate (operators.cpp:152-156)
-    s = launch_constrain_vjp(stream, g, m->cell_mask, w.advected_a, m->velocity_boundary, w.raw_a);
+    s = launch_constrain_vjp(stream, g, m->cell_mask, w.advected_a, m->velocity_boundary, w.raw_a, true);
     if (s != XS_OK) return s;
     s = launch_advect_velocity_vjp(stream, g, m->cell_mask, cache.forced_velocity, m->velocity_boundary, w.raw_a, w.forced_a);
     if (s != XS_OK) return s;
-    s = launch_integrate_vjp(stream, g, m->cell_mask, w.forced_a, pa.velocity, w.force_a);
+    s = launch_integrate_vjp(stream, g, m->cell_mask, w.forced_a, pa.velocity, w.force_a, true);
     if (s != XS_OK) return s;
     // forces: buoyancy then vorticity (operators.cpp:135-138)
     s = launch_buoyancy_vjp(stream, g, m->cell_mask, cache.sourced_density, cache.sourced_temperature, parameters.ambient_temperature,
