@@ -13,12 +13,14 @@ The plume first spins up from rest (seeded uniform velocity noise in
 
   plain                   zero start (the reference's zero-initialised solve)
   history                 Galerkin start from the last 5 forward solutions
-  history+coarse          ... then a step along the coarse-grid correction
+  history+coarse          ... then two rounds of Jacobi sweeps and a step along
+                          the coarse-grid correction (coarse grid solved exactly
+                          when its operator separates)
   learned                 the warm-start network's guess alone, energy-scaled
   learned+history         the ring start, then a step along the network's
                           correction of its residual
-  learned+history+coarse  the ring start, the coarse-grid step, then the
-                          network's step (headline)
+  learned+history+coarse  the ring start, one round of sweeps and coarse-grid
+                          step, then the network's step (headline)
 
 Each arm runs W warm-up steps (which also refill its ring) and K timed steps,
 every timed step with per-stage CUDA events (XsSmokeModel.stage_events).

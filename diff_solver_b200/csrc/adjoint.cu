@@ -188,9 +188,9 @@ constexpr size_t kScalarVjpSmem = 5 * AdjointTile::kNodes * (sizeof(double) + si
 
 // The trace adjoint of one sample at the trace end (operators.cu:426-438):
 // through the end position to the midpoint samples (their gradients m), and
-// through the midpoint to the start (exact start weights).
-template <int A>
-__device__ __forceinline__ void staged_trace_adjoint(const Vec3& mid, const Sample (&m)[3], const Vec3& der, const Vec3& src_gradient,
+// through the midpoint to the start (exact start weights).  A is the face
+// component at run time (a cell centre for the scalar adjoints: cell).
+__device__ __forceinline__ void staged_trace_adjoint(int A, const Vec3& mid, const Sample (&m)[3], const Vec3& der, const Vec3& src_gradient,
                                                      double o, int li, double* const (&acc)[3], const tile::Origin& org,
                                                      const tile::TileConsts& k, const Grid& g, const XsVelocityBoundary& vb,
                                                      const XsAdjointVector& ua, bool cell) {
@@ -210,9 +210,9 @@ __device__ __forceinline__ void staged_trace_adjoint(const Vec3& mid, const Samp
         tile::cell_start_scatter<S, 1>(acc[1], li, h * my);
         tile::cell_start_scatter<S, 2>(acc[2], li, h * mz);
     } else {
-        tile::face_start_scatter<S, A, 0>(acc[0], li, h * mx);
-        tile::face_start_scatter<S, A, 1>(acc[1], li, h * my);
-        tile::face_start_scatter<S, A, 2>(acc[2], li, h * mz);
+        tile::face_start_scatter_rt<S, 0>(acc[0], li, A, h * mx);
+        tile::face_start_scatter_rt<S, 1>(acc[1], li, A, h * my);
+        tile::face_start_scatter_rt<S, 2>(acc[2], li, A, h * mz);
     }
 }
 
@@ -232,8 +232,9 @@ __device__ __forceinline__ Vec3 staged_trace_with_samples(const tile::StagedVelo
     return raw;
 }
 
-template <int A>
-__device__ __forceinline__ void advect_velocity_vjp_tile_face(int x, int y, int z, int li, const tile::StagedVelocity& sv,
+// One face of component A (run time: the kernel loops over the components
+// with one copy of this body).
+__device__ __forceinline__ void advect_velocity_vjp_tile_face(int A, int x, int y, int z, int li, const tile::StagedVelocity& sv,
                                                               double* const (&acc)[3], const tile::Origin& org, const tile::TileConsts& k,
                                                               const Grid& g, const XsVelocityBoundary& vb, const XsAdjointVector& oa,
                                                               const XsAdjointVector& ua) {
@@ -243,10 +244,10 @@ __device__ __forceinline__ void advect_velocity_vjp_tile_face(int x, int y, int 
     const Vec3 s = face_position(A, x, y, z, g);
     Vec3 mid, der;
     Sample m[3];
-    const Vec3 end = staged_trace_with_samples(sv, s, tile::face_start_velocity<S, A>(sv, li), org, k, g, vb, mid, m, der);
-    const Sample src = tile::staged_face<S, A, true>(sv.s[A], component<const float>(sv.u.x, sv.u.y, sv.u.z, A), end, org, k, g, vb);
-    tile::staged_face_scatter<S, A>(acc[A], component<double>(ua.x, ua.y, ua.z, A), end, o, org, k, g, vb);
-    staged_trace_adjoint<A>(mid, m, der, src.gradient, o, li, acc, org, k, g, vb, ua, false);
+    const Vec3 end = staged_trace_with_samples(sv, s, tile::face_start_velocity_rt<S>(sv, li, A), org, k, g, vb, mid, m, der);
+    const Sample src = tile::staged_face_rt<S>(sv.s[A], component<const float>(sv.u.x, sv.u.y, sv.u.z, A), A, end, org, k, g, vb);
+    tile::staged_face_scatter_rt<S>(acc[A], component<double>(ua.x, ua.y, ua.z, A), A, end, o, org, k, g, vb);
+    staged_trace_adjoint(A, mid, m, der, src.gradient, o, li, acc, org, k, g, vb, ua, false);
 }
 
 __global__ void __launch_bounds__(AdjointTile::kThreads, 5) advect_velocity_vjp_tile_kernel(const __grid_constant__ Grid g, XsVector u, const __grid_constant__ XsVelocityBoundary vb,
@@ -275,9 +276,8 @@ __global__ void __launch_bounds__(AdjointTile::kThreads, 5) advect_velocity_vjp_
             const int z = static_cast<int>(blockIdx.z) * S::TZ + kz;
             if (z >= g.nz) break;
             const int li = tile::local_index<S>(kz);
-            advect_velocity_vjp_tile_face<0>(x, y, z, li, sv, acc, org, k, g, vb, oa, ua);
-            advect_velocity_vjp_tile_face<1>(x, y, z, li, sv, acc, org, k, g, vb, oa, ua);
-            advect_velocity_vjp_tile_face<2>(x, y, z, li, sv, acc, org, k, g, vb, oa, ua);
+#pragma unroll 1
+            for (int A = 0; A < 3; ++A) advect_velocity_vjp_tile_face(A, x, y, z, li, sv, acc, org, k, g, vb, oa, ua);
         }
     }
     __syncthreads();
@@ -353,11 +353,11 @@ __global__ void __launch_bounds__(AdjointTile::kThreads, 3) advect_scalar_vjp_ti
             const Vec3 end = staged_trace_with_samples(sv, s, tile::cell_start_velocity<S>(sv, li), org, k, g, vb, mid, m, der);
             const Sample smp = tile::staged_scalar<S, true>(box + 3 * S::kNodes, src, end, org, k, g, sb);
             tile::staged_scalar_scatter<S>(sacc[0], sa, end, o1, org, k, g, sb);
-            if (o1 != 0.0) staged_trace_adjoint<0>(mid, m, der, smp.gradient, o1, li, acc, org, k, g, vb, ua, true);
+            if (o1 != 0.0) staged_trace_adjoint(0, mid, m, der, smp.gradient, o1, li, acc, org, k, g, vb, ua, true);
             if (two && o2 != 0.0) {
                 const Sample smp2 = tile::staged_scalar<S, true>(box + 4 * S::kNodes, src2, end, org, k, g, sb2);
                 tile::staged_scalar_scatter<S>(sacc[1], sa2, end, o2, org, k, g, sb2);
-                staged_trace_adjoint<0>(mid, m, der, smp2.gradient, o2, li, acc, org, k, g, vb, ua, true);
+                staged_trace_adjoint(0, mid, m, der, smp2.gradient, o2, li, acc, org, k, g, vb, ua, true);
             }
         }
     }

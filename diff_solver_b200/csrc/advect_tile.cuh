@@ -467,6 +467,79 @@ __device__ __forceinline__ void flush_cells(const double* __restrict__ acc, doub
     }
 }
 
+// ------------------------------------------------ runtime face component
+// The face component as a runtime value: the adjoint kernel loops over the
+// three components with one copy of its per-face body (three unrolled
+// copies of a body that large stall on instruction fetch).  The same
+// arithmetic as the compile-time forms above.
+template <class S>
+__device__ __forceinline__ int stride_rt(int a) { return a == 0 ? 1 : (a == 1 ? S::SX : S::SX * S::SY); }
+
+template <class S, int B>
+__device__ __forceinline__ float face_start_component_rt(const float* __restrict__ s, int li, int A) {
+    if (A == B) return s[li];
+    const int lo = stride_rt<S>(A < B ? A : B), hi = stride_rt<S>(A < B ? B : A);
+    const float* c = s + li - stride_rt<S>(A);
+    float r = 0.25f * c[0];
+    r = fmaf(0.25f, c[lo], r);
+    r = fmaf(0.25f, c[hi], r);
+    r = fmaf(0.25f, c[lo + hi], r);
+    return r;
+}
+
+template <class S>
+__device__ __forceinline__ Vec3 face_start_velocity_rt(const StagedVelocity& sv, int li, int A) {
+    return Vec3{face_start_component_rt<S, 0>(sv.s[0], li, A), face_start_component_rt<S, 1>(sv.s[1], li, A),
+                face_start_component_rt<S, 2>(sv.s[2], li, A)};
+}
+
+template <class S, int B>
+__device__ __forceinline__ void face_start_scatter_rt(double* __restrict__ acc, int li, int A, double adj) {
+    if (adj == 0.0) return;
+    if (A == B) {
+        shared_add(acc + li, adj);
+        return;
+    }
+    const int lo = stride_rt<S>(A < B ? A : B), hi = stride_rt<S>(A < B ? B : A);
+    double* c = acc + li - stride_rt<S>(A);
+    const double w = adj * 0.5 * 0.5;
+    shared_add(c, w);
+    shared_add(c + lo, w);
+    shared_add(c + hi, w);
+    shared_add(c + lo + hi, w);
+}
+
+// staged_face<S, A, true> with A at run time
+template <class S>
+__device__ __forceinline__ Sample staged_face_rt(const float* __restrict__ s, const float* __restrict__ v, int A, const Vec3& p, const Origin& o,
+                                                 const TileConsts& k, const Grid& g, const XsVelocityBoundary& b) {
+    float gx, gy, gz;
+    grid_coordinates_pow2(p, k.r, A, gx, gy, gz);
+    const int x0 = static_cast<int>(floorf(gx)), y0 = static_cast<int>(floorf(gy)), z0 = static_cast<int>(floorf(gz));
+    const int c = box_corner<S>(x0, y0, z0, o);
+    if (c >= 0) {
+        float v8[2][2][2];
+        box_stencil<S>(s, c, v8);
+        return trilinear(v8, gx - x0, gy - y0, gz - z0, g.h);
+    }
+    return global_face_sample(v, A, p, g, b);
+}
+
+// staged_face_scatter<S, B> with B at run time
+template <class S>
+__device__ __forceinline__ void staged_face_scatter_rt(double* __restrict__ acc, double* __restrict__ v, int B, const Vec3& p, double adj,
+                                                       const Origin& o, const TileConsts& k, const Grid& g, const XsVelocityBoundary& b) {
+    if (adj == 0.0) return;
+    float gx, gy, gz;
+    grid_coordinates_pow2(p, k.r, B, gx, gy, gz);
+    const int x0 = static_cast<int>(floorf(gx)), y0 = static_cast<int>(floorf(gy)), z0 = static_cast<int>(floorf(gz));
+    const int c = box_corner<S>(x0, y0, z0, o);
+    if (c >= 0)
+        box_scatter<S>(acc, c, adj, gx - x0, gy - y0, gz - z0);
+    else
+        global_face_scatter(v, B, p, adj, g, b);
+}
+
 // ------------------------------------------------------------ dispatch
 // Whether the tile kernels apply: no collider mask (no bisection, no solid
 // faces) and a power-of-two spacing (exact start weights).
