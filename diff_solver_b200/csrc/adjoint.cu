@@ -184,20 +184,17 @@ __global__ void advect_velocity_vjp_kernel(const __grid_constant__ Grid g, uint6
 // with four; six spill) and three density-and-temperature ones.
 using AdjointTile = tile::Shape<32, 4, 4, 1>;
 constexpr size_t kVelocityVjpSmem = 3 * AdjointTile::kNodes * (sizeof(double) + sizeof(float));
-// The density-and-temperature adjoint keeps five FP64 and five FP32 boxes:
-// tiles two positions deep in z (49 KB) give it four CTAs per SM.
-using ScalarAdjointTile = tile::Shape<32, 4, 2, 1>;
-constexpr size_t kScalarVjpSmem = 5 * ScalarAdjointTile::kNodes * (sizeof(double) + sizeof(float));
+constexpr size_t kScalarVjpSmem = 5 * AdjointTile::kNodes * (sizeof(double) + sizeof(float));
 
 // The trace adjoint of one sample at the trace end (operators.cu:426-438):
 // through the end position to the midpoint samples (their gradients m), and
 // through the midpoint to the start (exact start weights).  A is the face
 // component at run time (a cell centre for the scalar adjoints: cell).
-template <class S>
 __device__ __forceinline__ void staged_trace_adjoint(int A, const Vec3& mid, const Sample (&m)[3], const Vec3& der, const Vec3& src_gradient,
                                                      double o, int li, double* const (&acc)[3], const tile::Origin& org,
                                                      const tile::TileConsts& k, const Grid& g, const XsVelocityBoundary& vb,
                                                      const XsAdjointVector& ua, bool cell) {
+    using S = AdjointTile;
     const double v1x = -static_cast<double>(der.x * g.dt * src_gradient.x) * o;
     const double v1y = -static_cast<double>(der.y * g.dt * src_gradient.y) * o;
     const double v1z = -static_cast<double>(der.z * g.dt * src_gradient.z) * o;
@@ -221,10 +218,10 @@ __device__ __forceinline__ void staged_trace_adjoint(int A, const Vec3& mid, con
 
 // Midpoint samples (values and gradients) and the clamped end of the trace
 // from a start with known velocity.
-template <class S>
 __device__ __forceinline__ Vec3 staged_trace_with_samples(const tile::StagedVelocity& sv, const Vec3& s, const Vec3& v0, const tile::Origin& org,
                                                           const tile::TileConsts& k, const Grid& g, const XsVelocityBoundary& vb, Vec3& mid,
                                                           Sample (&m)[3], Vec3& der) {
+    using S = AdjointTile;
     mid = Vec3{s.x - 0.5f * g.dt * v0.x, s.y - 0.5f * g.dt * v0.y, s.z - 0.5f * g.dt * v0.z};
     m[0] = tile::staged_face<S, 0, true>(sv.s[0], sv.u.x, mid, org, k, g, vb);
     m[1] = tile::staged_face<S, 1, true>(sv.s[1], sv.u.y, mid, org, k, g, vb);
@@ -247,10 +244,10 @@ __device__ __forceinline__ void advect_velocity_vjp_tile_face(int A, int x, int 
     const Vec3 s = face_position(A, x, y, z, g);
     Vec3 mid, der;
     Sample m[3];
-    const Vec3 end = staged_trace_with_samples<S>(sv, s, tile::face_start_velocity_rt<S>(sv, li, A), org, k, g, vb, mid, m, der);
+    const Vec3 end = staged_trace_with_samples(sv, s, tile::face_start_velocity_rt<S>(sv, li, A), org, k, g, vb, mid, m, der);
     const Sample src = tile::staged_face_rt<S>(sv.s[A], component<const float>(sv.u.x, sv.u.y, sv.u.z, A), A, end, org, k, g, vb);
     tile::staged_face_scatter_rt<S>(acc[A], component<double>(ua.x, ua.y, ua.z, A), A, end, o, org, k, g, vb);
-    staged_trace_adjoint<S>(A, mid, m, der, src.gradient, o, li, acc, org, k, g, vb, ua, false);
+    staged_trace_adjoint(A, mid, m, der, src.gradient, o, li, acc, org, k, g, vb, ua, false);
 }
 
 __global__ void __launch_bounds__(AdjointTile::kThreads, 5) advect_velocity_vjp_tile_kernel(const __grid_constant__ Grid g, XsVector u, const __grid_constant__ XsVelocityBoundary vb,
@@ -314,13 +311,13 @@ __global__ void advect_velocity_vjp_upper_kernel(const __grid_constant__ Grid g,
 // Density and temperature together (operators.cu:537-561 twice on one
 // trace): u and both sources staged, the velocity and both source adjoints
 // accumulated in the box.
-__global__ void __launch_bounds__(ScalarAdjointTile::kThreads, 4) advect_scalar_vjp_tile_kernel(const __grid_constant__ Grid g, const float* __restrict__ src,
+__global__ void __launch_bounds__(AdjointTile::kThreads, 3) advect_scalar_vjp_tile_kernel(const __grid_constant__ Grid g, const float* __restrict__ src,
                                                                                         const __grid_constant__ XsScalarBoundary sb, const double* __restrict__ oa,
                                                                                         double* __restrict__ sa, const float* __restrict__ src2,
                                                                                         const __grid_constant__ XsScalarBoundary sb2, const double* __restrict__ oa2,
                                                                                         double* __restrict__ sa2, XsVector u,
                                                                                         const __grid_constant__ XsVelocityBoundary vb, XsAdjointVector ua) {
-    using S = ScalarAdjointTile;
+    using S = AdjointTile;
     extern __shared__ __align__(16) unsigned char smem_raw[];
     double* const acc[3] = {reinterpret_cast<double*>(smem_raw), reinterpret_cast<double*>(smem_raw) + S::kNodes,
                             reinterpret_cast<double*>(smem_raw) + 2 * S::kNodes};
@@ -353,14 +350,14 @@ __global__ void __launch_bounds__(ScalarAdjointTile::kThreads, 4) advect_scalar_
             const Vec3 s = cell_position(x, y, z, g);
             Vec3 mid, der;
             Sample m[3];
-            const Vec3 end = staged_trace_with_samples<S>(sv, s, tile::cell_start_velocity<S>(sv, li), org, k, g, vb, mid, m, der);
+            const Vec3 end = staged_trace_with_samples(sv, s, tile::cell_start_velocity<S>(sv, li), org, k, g, vb, mid, m, der);
             const Sample smp = tile::staged_scalar<S, true>(box + 3 * S::kNodes, src, end, org, k, g, sb);
             tile::staged_scalar_scatter<S>(sacc[0], sa, end, o1, org, k, g, sb);
-            if (o1 != 0.0) staged_trace_adjoint<S>(0, mid, m, der, smp.gradient, o1, li, acc, org, k, g, vb, ua, true);
+            if (o1 != 0.0) staged_trace_adjoint(0, mid, m, der, smp.gradient, o1, li, acc, org, k, g, vb, ua, true);
             if (two && o2 != 0.0) {
                 const Sample smp2 = tile::staged_scalar<S, true>(box + 4 * S::kNodes, src2, end, org, k, g, sb2);
                 tile::staged_scalar_scatter<S>(sacc[1], sa2, end, o2, org, k, g, sb2);
-                staged_trace_adjoint<S>(0, mid, m, der, smp2.gradient, o2, li, acc, org, k, g, vb, ua, true);
+                staged_trace_adjoint(0, mid, m, der, smp2.gradient, o2, li, acc, org, k, g, vb, ua, true);
             }
         }
     }
@@ -567,7 +564,7 @@ XsStatus launch_advect_scalar_vjp(cudaStream_t st, const Grid& g, const uint32_t
                                             static_cast<int>(kScalarVjpSmem));
             }))
             return XS_CUDA_ERROR;
-        advect_scalar_vjp_tile_kernel<<<tile::tile_grid<ScalarAdjointTile>(g), tile::tile_block<ScalarAdjointTile>(), kScalarVjpSmem, st>>>(
+        advect_scalar_vjp_tile_kernel<<<tile::tile_grid<AdjointTile>(g), tile::tile_block<AdjointTile>(), kScalarVjpSmem, st>>>(
             g, src, sb, oa, sa, src2, sb2, oa2, sa2, u, vb, ua);
         return check_launch();
     }

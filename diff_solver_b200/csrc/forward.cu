@@ -453,6 +453,36 @@ __global__ void pressure_rhs_kernel(Grid g, uint32_t anchor, const uint32_t* __r
     rhs[i] = -g.h * g.h * div / g.dt;
 }
 
+// pressure_rhs_kernel without colliders, 3D-indexed: a thread takes kFaceZ
+// cells of one (x, y) column, loading all their face velocities before the
+// first store; the same arithmetic per cell.
+template <int kZ>
+__global__ void __launch_bounds__(256) pressure_rhs_cells_kernel(const __grid_constant__ Grid g, uint32_t anchor, XsVector u, float* __restrict__ rhs) {
+    const int x = static_cast<int>(blockIdx.x * 32 + threadIdx.x), y = static_cast<int>(blockIdx.y * 8 + threadIdx.y);
+    const int z0 = static_cast<int>(blockIdx.z) * kZ;
+    if (x >= g.nx || y >= g.ny) return;
+    float d[kZ][6];
+#pragma unroll
+    for (int k = 0; k < kZ; ++k) {
+        const int z = z0 + k;
+        if (z >= g.nz) continue;
+        d[k][0] = __ldg(u.x + tile::index32(x + 1, y, z, g.nx + 1, g.ny));
+        d[k][1] = __ldg(u.x + tile::index32(x, y, z, g.nx + 1, g.ny));
+        d[k][2] = __ldg(u.y + tile::index32(x, y + 1, z, g.nx, g.ny + 1));
+        d[k][3] = __ldg(u.y + tile::index32(x, y, z, g.nx, g.ny + 1));
+        d[k][4] = __ldg(u.z + tile::index32(x, y, z + 1, g.nx, g.ny));
+        d[k][5] = __ldg(u.z + tile::index32(x, y, z, g.nx, g.ny));
+    }
+#pragma unroll
+    for (int k = 0; k < kZ; ++k) {
+        const int z = z0 + k;
+        if (z >= g.nz) continue;
+        const uint32_t i = tile::index32(x, y, z, g.nx, g.ny);
+        const float div = (d[k][0] - d[k][1] + d[k][2] - d[k][3] + d[k][4] - d[k][5]) / g.h;
+        rhs[i] = i == anchor ? 0.0f : -g.h * g.h * div / g.dt;
+    }
+}
+
 __global__ void accumulate_kernel(const double* __restrict__ src, double* __restrict__ dst, uint64_t n) {
     const uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x;
     if (i < n) dst[i] += src[i];
@@ -463,80 +493,125 @@ __global__ void accumulate_kernel(const double* __restrict__ src, double* __rest
 // z-slices of u, then v, then w (each component's own z extent); threads
 // cover (x, y) with x fastest, so loads and stores are coalesced and no index
 // is decoded.  The arithmetic is the general kernels' (bit-identical).
+// Each thread handles kFaceZ consecutive z-slices of its component: all of
+// their loads are issued before the first store (four times the bytes in
+// flight of one face per thread).
+constexpr int kFaceZ = 4;
+
 struct FaceSlice {
-    int a, z;
+    int a, z;  // component and first z-slice of the block
 };
+
+__host__ __device__ __forceinline__ int face_blocks_z(int extent_z) { return (extent_z + kFaceZ - 1) / kFaceZ; }
 
 __device__ __forceinline__ FaceSlice face_slice(const Grid& g) {
     const int zi = static_cast<int>(blockIdx.z);
-    const int z0 = g.nz, z1 = 2 * g.nz;  // u and v have nz slices, w has nz + 1
-    if (zi < z0) return FaceSlice{0, zi};
-    if (zi < z1) return FaceSlice{1, zi - z0};
-    return FaceSlice{2, zi - z1};
+    const int z0 = face_blocks_z(g.nz), z1 = 2 * z0;  // u and v have nz slices, w has nz + 1
+    if (zi < z0) return FaceSlice{0, kFaceZ * zi};
+    if (zi < z1) return FaceSlice{1, kFaceZ * (zi - z0)};
+    return FaceSlice{2, kFaceZ * (zi - z1)};
 }
 
 inline dim3 face_pass_grid(const Grid& g) {
-    return dim3(static_cast<unsigned>((g.nx + 1 + 31) / 32), static_cast<unsigned>((g.ny + 1 + 7) / 8), static_cast<unsigned>(3 * g.nz + 1));
+    return dim3(static_cast<unsigned>((g.nx + 1 + 31) / 32), static_cast<unsigned>((g.ny + 1 + 7) / 8),
+                static_cast<unsigned>(2 * face_blocks_z(g.nz) + face_blocks_z(g.nz + 1)));
 }
 
-// operators.cu:358-364 without colliders, for face component A: the mean of
+// operators.cu:358-364 without colliders, for kFaceZ z-slices of face
+// component A: the mean of
 // the one or two in-grid cell forces beside the face (division by a count
 // of 2 is the exact product with 0.5).
 template <int A>
-__device__ __forceinline__ void integrate_face(const Grid& g, int x, int y, int z, const XsVector& u, const XsVector& f, const XsVector& out) {
-    const int ex = extent(g, A, 0), ey = extent(g, A, 1);
+__device__ __forceinline__ void integrate_faces(const Grid& g, int x, int y, int z0, const XsVector& u, const XsVector& f, const XsVector& out) {
+    const int ex = extent(g, A, 0), ey = extent(g, A, 1), ez = extent(g, A, 2);
     if (x >= ex || y >= ey) return;
-    const uint32_t i = tile::index32(x, y, z, ex, ey);
     const float* fa = component<const float>(f.x, f.y, f.z, A);
-    const int c = A == 0 ? x : (A == 1 ? y : z);
+    const float* ua = component<const float>(u.x, u.y, u.z, A);
     const int n = A == 0 ? g.nx : (A == 1 ? g.ny : g.nz);
-    const uint32_t upper = tile::index32(x, y, z, g.nx, g.ny);
-    const uint32_t lower = upper - static_cast<uint32_t>(A == 0 ? 1 : (A == 1 ? g.nx : g.nx * g.ny));
-    float sum = 0.0f, mean;
-    if (c == 0) {
-        sum += __ldg(fa + upper);
-        mean = sum;
-    } else if (c == n) {
-        sum += __ldg(fa + lower);
-        mean = sum;
-    } else {
-        sum += __ldg(fa + lower);
-        sum += __ldg(fa + upper);
-        mean = sum * 0.5f;
+    const uint32_t step = static_cast<uint32_t>(A == 0 ? 1 : (A == 1 ? g.nx : g.nx * g.ny));
+    float uv[kFaceZ], lo[kFaceZ], hi[kFaceZ];
+#pragma unroll
+    for (int k = 0; k < kFaceZ; ++k) {
+        const int z = z0 + k;
+        uv[k] = lo[k] = hi[k] = 0.0f;
+        if (z >= ez) continue;
+        const int c = A == 0 ? x : (A == 1 ? y : z);
+        const uint32_t upper = tile::index32(x, y, z, g.nx, g.ny);
+        uv[k] = __ldg(ua + tile::index32(x, y, z, ex, ey));
+        if (c != n) hi[k] = __ldg(fa + upper);
+        if (c != 0) lo[k] = __ldg(fa + upper - step);
     }
-    component(out.x, out.y, out.z, A)[i] = component<const float>(u.x, u.y, u.z, A)[i] + g.dt * mean;
+    float* oa = component(out.x, out.y, out.z, A);
+#pragma unroll
+    for (int k = 0; k < kFaceZ; ++k) {
+        const int z = z0 + k;
+        if (z >= ez) continue;
+        const int c = A == 0 ? x : (A == 1 ? y : z);
+        float sum = 0.0f, mean;
+        if (c == 0) {
+            sum += hi[k];
+            mean = sum;
+        } else if (c == n) {
+            sum += lo[k];
+            mean = sum;
+        } else {
+            sum += lo[k];
+            sum += hi[k];
+            mean = sum * 0.5f;
+        }
+        oa[tile::index32(x, y, z, ex, ey)] = uv[k] + g.dt * mean;
+    }
 }
 
 __global__ void __launch_bounds__(256) integrate_faces_kernel(const __grid_constant__ Grid g, XsVector u, XsVector f, XsVector out) {
     const FaceSlice fsl = face_slice(g);
     const int x = static_cast<int>(blockIdx.x * 32 + threadIdx.x), y = static_cast<int>(blockIdx.y * 8 + threadIdx.y);
-    if (fsl.a == 0) integrate_face<0>(g, x, y, fsl.z, u, f, out);
-    else if (fsl.a == 1) integrate_face<1>(g, x, y, fsl.z, u, f, out);
-    else integrate_face<2>(g, x, y, fsl.z, u, f, out);
+    if (fsl.a == 0) integrate_faces<0>(g, x, y, fsl.z, u, f, out);
+    else if (fsl.a == 1) integrate_faces<1>(g, x, y, fsl.z, u, f, out);
+    else integrate_faces<2>(g, x, y, fsl.z, u, f, out);
 }
 
 // operators.cu:912-920 with the FP64 pressure iterate, without colliders, for
-// face component A.  For a power-of-two spacing the FP64 division by h is the
+// kFaceZ z-slices of face component A.  For a power-of-two spacing the FP64 division by h is the
 // exact product with inv_h = 1/h (computed on the host; the same IEEE result).
 template <int A, bool kPow2>
-__device__ __forceinline__ void project64_face(const Grid& g, double inv_h, int x, int y, int z, const XsVector& u, const double* __restrict__ p,
-                                               const XsVector& out) {
-    const int ex = extent(g, A, 0), ey = extent(g, A, 1);
+__device__ __forceinline__ void project64_faces(const Grid& g, double inv_h, int x, int y, int z0, const XsVector& u, const double* __restrict__ p,
+                                                const XsVector& out) {
+    const int ex = extent(g, A, 0), ey = extent(g, A, 1), ez = extent(g, A, 2);
     if (x >= ex || y >= ey) return;
-    const uint32_t i = tile::index32(x, y, z, ex, ey);
     const float* ua = component<const float>(u.x, u.y, u.z, A);
-    float* oa = component(out.x, out.y, out.z, A);
-    const int c = A == 0 ? x : (A == 1 ? y : z);
     const int n = A == 0 ? g.nx : (A == 1 ? g.ny : g.nz);
-    if (c == 0 || c == n) {  // projectable_face: both cells in the grid
-        oa[i] = ua[i];
-        return;
+    const uint32_t step = static_cast<uint32_t>(A == 0 ? 1 : (A == 1 ? g.nx : g.nx * g.ny));
+    float uv[kFaceZ];
+    double p0[kFaceZ], p1[kFaceZ];
+#pragma unroll
+    for (int k = 0; k < kFaceZ; ++k) {
+        const int z = z0 + k;
+        uv[k] = 0.0f;
+        p0[k] = p1[k] = 0.0;
+        if (z >= ez) continue;
+        const int c = A == 0 ? x : (A == 1 ? y : z);
+        uv[k] = __ldg(ua + tile::index32(x, y, z, ex, ey));
+        if (c == 0 || c == n) continue;  // projectable_face: both cells in the grid
+        const uint32_t second = tile::index32(x, y, z, g.nx, g.ny);
+        p1[k] = __ldg(p + second);
+        p0[k] = __ldg(p + second - step);
     }
-    const uint32_t second = tile::index32(x, y, z, g.nx, g.ny);
-    const uint32_t first = second - static_cast<uint32_t>(A == 0 ? 1 : (A == 1 ? g.nx : g.nx * g.ny));
-    const double dp = __ldg(p + second) - __ldg(p + first);
-    const double scaled = static_cast<double>(g.dt) * dp;
-    oa[i] = static_cast<float>(static_cast<double>(ua[i]) - (kPow2 ? scaled * inv_h : scaled / static_cast<double>(g.h)));
+    float* oa = component(out.x, out.y, out.z, A);
+#pragma unroll
+    for (int k = 0; k < kFaceZ; ++k) {
+        const int z = z0 + k;
+        if (z >= ez) continue;
+        const int c = A == 0 ? x : (A == 1 ? y : z);
+        const uint32_t i = tile::index32(x, y, z, ex, ey);
+        if (c == 0 || c == n) {
+            oa[i] = uv[k];
+            continue;
+        }
+        const double dp = p1[k] - p0[k];
+        const double scaled = static_cast<double>(g.dt) * dp;
+        oa[i] = static_cast<float>(static_cast<double>(uv[k]) - (kPow2 ? scaled * inv_h : scaled / static_cast<double>(g.h)));
+    }
 }
 
 template <bool kPow2>
@@ -544,9 +619,9 @@ __global__ void __launch_bounds__(256) project64_faces_kernel(const __grid_const
                                                               XsVector out) {
     const FaceSlice fsl = face_slice(g);
     const int x = static_cast<int>(blockIdx.x * 32 + threadIdx.x), y = static_cast<int>(blockIdx.y * 8 + threadIdx.y);
-    if (fsl.a == 0) project64_face<0, kPow2>(g, inv_h, x, y, fsl.z, u, p, out);
-    else if (fsl.a == 1) project64_face<1, kPow2>(g, inv_h, x, y, fsl.z, u, p, out);
-    else project64_face<2, kPow2>(g, inv_h, x, y, fsl.z, u, p, out);
+    if (fsl.a == 0) project64_faces<0, kPow2>(g, inv_h, x, y, fsl.z, u, p, out);
+    else if (fsl.a == 1) project64_faces<1, kPow2>(g, inv_h, x, y, fsl.z, u, p, out);
+    else project64_faces<2, kPow2>(g, inv_h, x, y, fsl.z, u, p, out);
 }
 
 // ------------------------------------------------------------ launchers
@@ -624,6 +699,11 @@ XsStatus launch_advect_scalar_pair(cudaStream_t st, const Grid& g, const uint32_
 }
 
 XsStatus launch_pressure_rhs(cudaStream_t st, const Grid& g, uint32_t anchor, const uint32_t* mask, const XsVector& u, float* rhs) {
+    if (mask == nullptr && g.nz <= 4 * 65535) {
+        const dim3 grid(static_cast<unsigned>((g.nx + 31) / 32), static_cast<unsigned>((g.ny + 7) / 8), static_cast<unsigned>((g.nz + kFaceZ - 1) / kFaceZ));
+        pressure_rhs_cells_kernel<kFaceZ><<<grid, dim3(32, 8), 0, st>>>(g, anchor, u, rhs);
+        return check_launch();
+    }
     pressure_rhs_kernel<<<blocks_for(cell_count(g)), kBlock, 0, st>>>(g, anchor, mask, u, rhs);
     return check_launch();
 }
