@@ -421,8 +421,13 @@ def load_network(args, shape):
     if not os.path.exists(args.weights):
         raise FileNotFoundError(f"{args.weights} is missing: train it with python -m diff_solver_b200.train_warm_start")
     # trained at 128^3, applied fully convolutionally on the grid restricted
-    # x network_factor (4 by default)
+    # x network_factor (4 by default; halved while that grid would be
+    # smaller than 64 cells on an axis, the smallest the U-Net's four levels
+    # are run on here)
     f = args.network_factor
+    while f > 1 and min(shape) // f < 64:
+        f //= 2
+    args.network_factor = f
     network = WarmStartNetwork(tuple(s // f for s in shape), factor=f)
     network.load(args.weights)
     return network
