@@ -159,6 +159,11 @@ def counts(shape):
 # workload's plain solve at 256^3: 800.5 GB for 1323 CG iterations and 2
 # refinement passes, whose algorithmic count below is 801.7 GB.
 PCG_TRAFFIC_PER_ALGORITHMIC_BYTE_256 = 800.5 / 801.7
+# The same for the warm-started solve with minimal-residual smoothing
+# (pcg_kernel<1, 1>) in the benchmark window: 7.223 GB per launch over three
+# captured launches of 7 CG iterations (5 smoothed) and 1 refinement pass,
+# whose algorithmic count below is 7.181 GB.
+PCG_SMOOTH_TRAFFIC_PER_ALGORITHMIC_BYTE_256 = 7.223 / 7.181
 
 
 def pcg_algorithmic_bytes(n_cells, iterations, refinements, smoothed=0):
@@ -791,17 +796,19 @@ def main():
     arms, pcg_roofline = summarize(results, args, args.shape, world, headline)
     h = results[headline]
     value = arms[headline]["steps_per_s"]
-    roofline = pcg_roofline(headline)
-    traffic = None
-    if tuple(args.shape) == (GRID,) * 3:  # the captured workload: its measured traffic per algorithmic byte
-        traffic = PCG_TRAFFIC_PER_ALGORITHMIC_BYTE_256 * roofline["algorithmic_bytes_per_launch"]
-    roofline["traffic"] = traffic
-    roofline["traffic_unit"] = "bytes per launch (the plain-launch ratio of dram bytes to algorithmic bytes, measured by ncu)"
+    def with_traffic(rf):
+        # the captured workload: each kernel's measured dram bytes per algorithmic byte
+        ratio = PCG_TRAFFIC_PER_ALGORITHMIC_BYTE_256 if rf["arm"] == "plain" else PCG_SMOOTH_TRAFFIC_PER_ALGORITHMIC_BYTE_256
+        rf["traffic"] = ratio * rf["algorithmic_bytes_per_launch"] if tuple(args.shape) == (GRID,) * 3 else None
+        rf["traffic_unit"] = "bytes per launch (the kernel's ncu-measured ratio of dram bytes to algorithmic bytes at 256^3)"
+        return rf
+
+    roofline = with_traffic(pcg_roofline(headline))
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps, "warmup": args.warmup,
             "ms_per_step": h["elapsed_ms"] / args.steps, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32 (FP64 CG reductions and iterate)", "data": "synthetic", "config": config,
             "method": headline, "speedup_vs_plain": value / arms["plain"]["steps_per_s"] if "plain" in arms else None, "arms": arms,
-            "roofline": roofline, "roofline_plain": pcg_roofline("plain") if "plain" in results else None,
+            "roofline": roofline, "roofline_plain": with_traffic(pcg_roofline("plain")) if "plain" in results else None,
             "gpu_launches": h["launches"], "clocks": clocks,
             "e2e": {"value": steps_total / (h["e2e_ms"] / 1e3), "unit": UNIT, "h2d_bytes_per_step": h["h2d"],
                     "d2h_bytes_per_step": h["d2h"]},
