@@ -109,7 +109,7 @@ struct WarmHistory {
 };
 // Exact coarse solve for operators that separate by axis (spectral.cu):
 // grids of at most kSpectralMax cells per axis, no anchor cell, no colliders.
-constexpr int kSpectralMax = 128;
+constexpr int kSpectralMax = 256;
 struct SpectralAxes {
     int n[3];
     int kind[3];  // per axis: zero-gradient / fixed-value ends, or periodic

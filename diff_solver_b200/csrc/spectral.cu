@@ -16,9 +16,9 @@
 //
 // three forward line transforms, one scaling and three inverse transforms.
 // Each transform is a dense product with the n x n basis held in shared
-// memory (n <= 128 on the coarse grids this serves): O(n) flops per cell and
-// axis instead of the coarse Jacobi-PCG's dozens of latency-bound
-// iterations.  A mode whose eigenvalue sum vanishes (the constant of an
+// memory (n <= 256 on the coarse grids this serves; above 128 in two column
+// halves): O(n) flops per cell and axis instead of the coarse Jacobi-PCG's
+// dozens of latency-bound iterations.  A mode whose eigenvalue sum vanishes (the constant of an
 // all-zero-gradient box) is dropped: the pseudo-inverse.
 #include <algorithm>
 
@@ -105,6 +105,80 @@ constexpr int kTileLines = kWarpLines * kTransformThreads / 32;  // 64 lines per
 constexpr int pitch(int np) { return np + 4; }                 // 16-byte rows
 constexpr size_t transform_smem(int np) { return sizeof(float) * static_cast<size_t>(np + kTileLines) * pitch(np); }
 
+// Copies the tile of lines L0.. into d (row pitch R, zero beyond n and past
+// the last line): kBatch loads in flight per thread; contiguous lines are
+// read along the line, strided ones across lines (consecutive threads take
+// consecutive lines, which are adjacent in memory).
+template <int NP, class Tin>
+__device__ __forceinline__ void load_tile(const Tin* in, const LineSet& ls, uint32_t L0, float* d, int t) {
+    constexpr int R = pitch(NP);
+    constexpr int kPer = kTileLines * NP / kTransformThreads;  // tile elements per thread
+    constexpr int kBatch = 8;
+    static_assert(kPer % kBatch == 0, "");
+    const bool contiguous = ls.stride == 1;
+    for (int b0 = 0; b0 < kPer; b0 += kBatch) {
+        float v[kBatch];
+#pragma unroll
+        for (int u = 0; u < kBatch; ++u) {
+            const int i = t + (b0 + u) * kTransformThreads;
+            const int l = contiguous ? i / NP : i % kTileLines, j = contiguous ? i % NP : i / kTileLines;
+            const uint32_t L = L0 + l;
+            v[u] = (L < ls.lines && j < ls.n) ? static_cast<float>(in[ls.base(L) + static_cast<uint64_t>(j) * ls.stride]) : 0.0f;
+        }
+#pragma unroll
+        for (int u = 0; u < kBatch; ++u) {
+            const int i = t + (b0 + u) * kTransformThreads;
+            const int l = contiguous ? i / NP : i % kTileLines, j = contiguous ? i % NP : i / kTileLines;
+            d[l * R + j] = v[u];
+        }
+    }
+}
+
+template <int NP>
+__device__ __forceinline__ void store_tile(float* out, const LineSet& ls, uint32_t L0, const float* d, int t) {
+    constexpr int R = pitch(NP);
+    const bool contiguous = ls.stride == 1;
+    for (int i = t; i < kTileLines * NP; i += kTransformThreads) {
+        const int l = contiguous ? i / NP : i % kTileLines, j = contiguous ? i % NP : i / kTileLines;
+        const uint32_t L = L0 + l;
+        if (L < ls.lines && j < ls.n) out[ls.base(L) + static_cast<uint64_t>(j) * ls.stride] = d[l * R + j];
+    }
+}
+
+// acc[i][c] += sum_j d[l0 + i][j] * M[j][4 lane + c] over j < NP: the warp's
+// kWarpLines lines (16-byte broadcasts of the tile) against the lane's four
+// consecutive columns of M (row pitch RM).
+template <int NP, int RM>
+__device__ __forceinline__ void accumulate_modes(const float* d, const float* ms, int l0, int lane, float (&acc)[kWarpLines][4]) {
+    constexpr int R = pitch(NP);
+#pragma unroll 2
+    for (int j = 0; j < NP; j += 4) {
+        float4 v[kWarpLines];
+#pragma unroll
+        for (int i = 0; i < kWarpLines; ++i) v[i] = *reinterpret_cast<const float4*>(d + (l0 + i) * R + j);
+#pragma unroll
+        for (int jj = 0; jj < 4; ++jj) {
+            const float4 q = *reinterpret_cast<const float4*>(ms + (j + jj) * RM + 4 * lane);
+#pragma unroll
+            for (int i = 0; i < kWarpLines; ++i) {
+                const float x = jj == 0 ? v[i].x : (jj == 1 ? v[i].y : (jj == 2 ? v[i].z : v[i].w));
+                acc[i][0] = fmaf(x, q.x, acc[i][0]);
+                acc[i][1] = fmaf(x, q.y, acc[i][1]);
+                acc[i][2] = fmaf(x, q.z, acc[i][2]);
+                acc[i][3] = fmaf(x, q.w, acc[i][3]);
+            }
+        }
+    }
+}
+
+// Divides coefficient k of line L by its eigenvalue sum (zero for a
+// vanishing sum: the pseudo-inverse; zero past n and past the last line).
+__device__ __forceinline__ float scaled_mode(float v, const LineSet& ls, const LineScale& sc, uint32_t L, int k) {
+    if (!(L < ls.lines && k < ls.n)) return 0.0f;
+    const float lam = sc.lam_a[L % sc.inner] + sc.lam_b[L / sc.inner] + sc.lam_line[k];
+    return lam > 0.0f ? v / lam : 0.0f;
+}
+
 // out_l[k] = sum_j M[j][k] in_l[j] for tiles of 64 lines: the tile and M in
 // shared memory (16-byte rows), each warp 8 lines, each lane NP / 32
 // consecutive outputs, both operands read as 16-byte vectors (the tile's
@@ -129,30 +203,11 @@ __global__ void __launch_bounds__(kTransformThreads, 2) line_transform_kernel(co
                      : "memory");
     }
     asm volatile("cp.async.wait_all;" ::: "memory");
-    const bool contiguous = ls.stride == 1;
     const uint32_t tiles = (ls.lines + kTileLines - 1) / kTileLines;
-    constexpr int kPer = kTileLines * NP / kTransformThreads;  // tile elements per thread
-    constexpr int kBatch = 8;                                  // loads in flight per thread
-    static_assert(kPer % kBatch == 0, "");
     for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
         const uint32_t L0 = tile * kTileLines;
         __syncthreads();  // the matrix is in place; the previous tile is written out
-        for (int b0 = 0; b0 < kPer; b0 += kBatch) {
-            float v[kBatch];
-#pragma unroll
-            for (int u = 0; u < kBatch; ++u) {
-                const int i = t + (b0 + u) * kTransformThreads;
-                const int l = contiguous ? i / NP : i % kTileLines, j = contiguous ? i % NP : i / kTileLines;
-                const uint32_t L = L0 + l;
-                v[u] = (L < ls.lines && j < ls.n) ? static_cast<float>(in[ls.base(L) + static_cast<uint64_t>(j) * ls.stride]) : 0.0f;
-            }
-#pragma unroll
-            for (int u = 0; u < kBatch; ++u) {
-                const int i = t + (b0 + u) * kTransformThreads;
-                const int l = contiguous ? i / NP : i % kTileLines, j = contiguous ? i % NP : i / kTileLines;
-                d[l * R + j] = v[u];
-            }
-        }
+        load_tile<NP>(in, ls, L0, d, t);
         __syncthreads();
         float acc[kWarpLines][OL];
 #pragma unroll
@@ -201,11 +256,7 @@ __global__ void __launch_bounds__(kTransformThreads, 2) line_transform_kernel(co
 #pragma unroll
             for (int c = 0; c < OL; ++c) d[(l0 + i) * R + OL * lane + c] = acc[i][c];
         __syncthreads();
-        for (int i = t; i < kTileLines * NP; i += kTransformThreads) {
-            const int l = contiguous ? i / NP : i % kTileLines, j = contiguous ? i % NP : i / kTileLines;
-            const uint32_t L = L0 + l;
-            if (L < ls.lines && j < ls.n) out[ls.base(L) + static_cast<uint64_t>(j) * ls.stride] = d[l * R + j];
-        }
+        store_tile<NP>(out, ls, L0, d, t);
     }
 }
 
@@ -223,11 +274,104 @@ XsStatus launch_transform(cudaStream_t st, const Tin* in, float* out, const Line
     return check_launch();
 }
 
+// Lines of 129-256 values.  A 256 x 256 basis (256 KB) does not fit in shared
+// memory beside a tile, so each tile is multiplied by the basis' two column
+// halves in turn (modes 0-127, then 128-255), each half copied in once the
+// previous one is no longer read; every lane keeps both halves' sums in
+// registers until the tile is written back, in place as above.  The halves
+// come from L2 (the basis stays resident): 256 KB per tile of 64 lines,
+// against 2 x 64 x 256 x 256 flop of products.  One CTA per SM.
+constexpr int kWideLines = 256;
+constexpr int kHalfModes = kWideLines / 2;
+constexpr int kHalfPitch = kHalfModes + 4;  // 16-byte rows
+constexpr size_t wide_transform_smem() {
+    return sizeof(float) * (static_cast<size_t>(kTileLines) * pitch(kWideLines) + static_cast<size_t>(kWideLines) * kHalfPitch);
+}
+
+// Columns [h 128, h 128 + 128) of the basis into mh (row pitch kHalfPitch),
+// 16-byte asynchronous copies; the caller waits.
+__device__ __forceinline__ void copy_half(float* mh, const float* __restrict__ m, int h, int t) {
+    constexpr int kChunks = kHalfModes / 4;  // per row
+    for (int i = t; i < kWideLines * kChunks; i += kTransformThreads) {
+        const int row = i / kChunks, col = 4 * (i % kChunks);
+        asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(static_cast<uint32_t>(__cvta_generic_to_shared(mh + row * kHalfPitch + col))),
+                     "l"(m + row * kSpectralMax + h * kHalfModes + col)
+                     : "memory");
+    }
+}
+
+template <bool kScale, class Tin>
+__global__ void __launch_bounds__(kTransformThreads, 1) line_transform_wide_kernel(const Tin* in, float* out, LineSet ls, const float* __restrict__ m,
+                                                                                 LineScale sc) {
+    constexpr int NP = kWideLines;
+    constexpr int R = pitch(NP);
+    extern __shared__ __align__(16) float smem[];
+    float* d = smem;                    // kTileLines x R
+    float* mh = smem + kTileLines * R;  // NP x kHalfPitch: one column half of the basis
+    const int t = static_cast<int>(threadIdx.x), lane = t & 31, l0 = (t >> 5) * kWarpLines;
+    const uint32_t tiles = (ls.lines + kTileLines - 1) / kTileLines;
+    for (uint32_t tile = blockIdx.x; tile < tiles; tile += gridDim.x) {
+        const uint32_t L0 = tile * kTileLines;
+        __syncthreads();  // the previous tile is written out and its second half no longer read
+        copy_half(mh, m, 0, t);
+        load_tile<NP>(in, ls, L0, d, t);
+        asm volatile("cp.async.wait_all;" ::: "memory");
+        __syncthreads();
+        float acc[2][kWarpLines][4];
+#pragma unroll
+        for (int h = 0; h < 2; ++h) {
+            if (h == 1) {
+                __syncthreads();  // every warp is done with the first half
+                copy_half(mh, m, 1, t);
+                asm volatile("cp.async.wait_all;" ::: "memory");
+                __syncthreads();
+            }
+#pragma unroll
+            for (int i = 0; i < kWarpLines; ++i)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) acc[h][i][c] = 0.0f;
+            accumulate_modes<NP, kHalfPitch>(d, mh, l0, lane, acc[h]);
+        }
+        if (kScale) {
+#pragma unroll
+            for (int h = 0; h < 2; ++h)
+#pragma unroll
+                for (int i = 0; i < kWarpLines; ++i)
+#pragma unroll
+                    for (int c = 0; c < 4; ++c) acc[h][i][c] = scaled_mode(acc[h][i][c], ls, sc, L0 + l0 + i, h * kHalfModes + 4 * lane + c);
+        }
+        __syncthreads();  // every warp has read its lines
+#pragma unroll
+        for (int h = 0; h < 2; ++h)
+#pragma unroll
+            for (int i = 0; i < kWarpLines; ++i)
+                *reinterpret_cast<float4*>(d + (l0 + i) * R + h * kHalfModes + 4 * lane) =
+                    make_float4(acc[h][i][0], acc[h][i][1], acc[h][i][2], acc[h][i][3]);
+        __syncthreads();
+        store_tile<NP>(out, ls, L0, d, t);
+    }
+}
+
+template <bool kScale, class Tin>
+XsStatus launch_wide_transform(cudaStream_t st, const Tin* in, float* out, const LineSet& ls, const float* m, const LineScale& sc) {
+    static DeviceOnce configured;
+    constexpr size_t smem = wide_transform_smem();
+    if (!configured.run([] {
+            return cudaFuncSetAttribute(line_transform_wide_kernel<kScale, Tin>, cudaFuncAttributeMaxDynamicSharedMemorySize, static_cast<int>(smem));
+        }))
+        return XS_CUDA_ERROR;
+    const uint32_t tiles = (ls.lines + kTileLines - 1) / kTileLines;
+    const unsigned blocks = std::min<uint32_t>(tiles, 148u);
+    line_transform_wide_kernel<kScale, Tin><<<blocks, kTransformThreads, smem, st>>>(in, out, ls, m, sc);
+    return check_launch();
+}
+
 template <bool kScale, class Tin>
 XsStatus transform(cudaStream_t st, const Tin* in, float* out, const LineSet& ls, const float* m, const LineScale& sc) {
     if (ls.n <= 32) return launch_transform<32, kScale, Tin>(st, in, out, ls, m, sc);
     if (ls.n <= 64) return launch_transform<64, kScale, Tin>(st, in, out, ls, m, sc);
-    return launch_transform<128, kScale, Tin>(st, in, out, ls, m, sc);
+    if (ls.n <= 128) return launch_transform<128, kScale, Tin>(st, in, out, ls, m, sc);
+    return launch_wide_transform<kScale, Tin>(st, in, out, ls, m, sc);
 }
 
 }  // namespace

@@ -255,7 +255,7 @@ XsStatus xs_pressure_solve_static(cudaStream_t stream, XsGrid grid, const XsPres
  * operators the operator separates into.  XS_INVALID_ARGUMENT for other
  * grids.  scratch: xs_separable_solve_scratch_bytes() bytes of device
  * memory. */
-#define XS_SEPARABLE_SOLVE_MAX 128u
+#define XS_SEPARABLE_SOLVE_MAX 256u
 size_t xs_separable_solve_scratch_bytes(void);
 XsStatus xs_separable_solve(cudaStream_t stream, XsGrid grid, XsScalarBoundary pressure_boundary, uint32_t pressure_anchor,
                             const double* rhs, float* x, void* scratch);

@@ -30,6 +30,9 @@ CASES = [
     ((48, 32, 40), (P, P, Z, F, P, P)),   # periodic x and z
     ((64, 8, 12), (F, F, F, F, Z, F)),
     ((128, 128, 128), (Z, Z, Z, F, Z, Z)),  # the coarse grid of the 256^3 plume
+    ((200, 24, 16), (Z, F, Z, Z, F, Z)),    # a mixed axis of 129-256 cells: the basis in two halves
+    ((256, 72, 12), (P, P, F, F, Z, F)),    # a periodic axis of 256 cells
+    ((256, 256, 128), (Z, Z, Z, F, Z, Z)),  # the coarse grid of the 512x512x256 plume
 ]
 
 
@@ -73,7 +76,7 @@ def test_separable_solve_rejects_other_grids(cuda):
     b = torch.zeros(1, dtype=torch.float64, device="cuda")
     x = torch.zeros(1, dtype=torch.float32, device="cuda")
     # an anchored (all zero-gradient) box and an axis longer than the basis
-    for res, modes in (((16, 16, 16), (Z,) * 6), ((160, 16, 16), (Z, Z, Z, F, Z, Z))):
+    for res, modes in (((16, 16, 16), (Z,) * 6), ((264, 16, 16), (Z, Z, Z, F, Z, Z))):
         ctx = Model(configuration(res, modes)).allocate_context(ExecutionMode.forward)
         status = L.xs_separable_solve(None, ctx.native.grid, ctx.native.pressure_boundary, ctx.native.pressure_anchor,
                                       C.c_void_p(b.data_ptr()), C.c_void_p(x.data_ptr()), C.c_void_p(scratch.data_ptr()))
