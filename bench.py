@@ -34,7 +34,8 @@ and per-stage times are in ``arms``.  Further records of the same run:
                       with the reverse step's algorithmic bytes
   reference_kernels   the reference's own kernels (oracle/_ref) timed per kernel
                       on the same box and state, next to this library's
-  large_grid          512x512x256: plain and headline arms, per-stage GB/s
+  large_grid          512x512x256 (steps 89-98 of its 100-step plume): plain,
+                      two-round classical and headline arms, per-stage GB/s
   cpu_baseline        full FP64 oracle steps from the spun-up state on the
                       host's cores
 
@@ -642,7 +643,10 @@ def reference_kernels_record(args, ro, shape, repeats=5):
     return rec
 
 
-def large_grid_record(args, network_large, shape=LARGE_GRID, spinup=40, warmup=3, steps=5, headline_steps=10):
+LARGE_SPINUP = 85  # every timed step of the large grid lies within its 100-step plume
+
+
+def large_grid_record(args, network_large, shape=LARGE_GRID, spinup=LARGE_SPINUP, warmup=3, steps=5, headline_steps=10):
     import torch
     saved, spin = spin_up(shape, network_large, spinup)
     initial = saved[spinup]
@@ -650,7 +654,8 @@ def large_grid_record(args, network_large, shape=LARGE_GRID, spinup=40, warmup=3
     torch.cuda.empty_cache()
     sub = argparse.Namespace(steps=steps, warmup=warmup)
     results = {}
-    for name, history, net, coarsening, k in (("plain", 0, None, 0, steps), (HEADLINE, HISTORY, network_large, COARSENING, headline_steps)):
+    for name, history, net, coarsening, k in (("plain", 0, None, 0, steps), ("history+coarse", HISTORY, None, COARSENING, headline_steps),
+                                              (HEADLINE, HISTORY, network_large, COARSENING, headline_steps)):
         ro = Rollout(shape, history, net, coarsening)
         sub.steps = k
         results[name] = timed_arm(sub, 1, ro, initial)
@@ -844,7 +849,7 @@ def main():
     if "large_grid" in extra:
         lg = extra.pop("large_grid")
         sub = argparse.Namespace(steps=1)
-        rec = {"grid": list(LARGE_GRID), "spinup_steps": 40, "arms": {}}
+        rec = {"grid": list(LARGE_GRID), "spinup_steps": LARGE_SPINUP, "arms": {}}
         for name, r in lg.items():
             sub.steps = r.pop("_steps")
             a_, pr = summarize({name: r}, sub, LARGE_GRID, 1, name)
