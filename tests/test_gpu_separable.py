@@ -36,7 +36,7 @@ CASES = [
 ]
 
 
-@pytest.mark.parametrize("res,modes", CASES)
+@pytest.mark.parametrize("res,modes", CASES, ids=["x".join(map(str, r)) for r, _ in CASES])
 def test_separable_solve_matches_the_oracle(cuda, res, modes):
     import torch
     from diff_solver_b200 import _native as N
