@@ -284,6 +284,27 @@ def test_coarse_grid_correction(cuda):
     assert late_coarse < 0.7 * late_hist, (late_coarse, late_hist)
 
 
+def test_coarse_grid_correction_on_axes_past_128(cuda):
+    """A coarse axis of 129-256 cells (the case of the 512x512x256 plume,
+    here 320 x 96 x 64 coarsened x2 to 160 x 48 x 32) is solved exactly as
+    well, by the transforms that take the basis in two halves: converged
+    steps, the history start's steps within the tolerance, no coarse CG
+    iterations, fewer fine iterations."""
+    from diff_solver_b200.data import plume_configuration
+    cfg = plume_configuration((320, 96, 64), inflow_center=(0.5, 0.05, 0.1), inflow_radius=0.04)
+    cfg.warm_start_history = 5
+    hist, hist_stats, _ = _rollout(cfg, 30)
+    cfg.warm_start_coarsening = 2
+    coarse, coarse_stats, _ = _rollout(cfg, 30)
+    assert all(s["status"] == 0 and s["final_residual"] <= 1e-6 for s in coarse_stats)
+    assert rel(coarse, hist) < 1e-4
+    assert all(s["coarse_iterations"] == 0 for s in coarse_stats)
+    late_hist = np.mean([s["iterations"] for s in hist_stats[15:]])
+    late_coarse = np.mean([s["iterations"] for s in coarse_stats[15:]])
+    print(late_hist, late_coarse)
+    assert late_coarse < 0.7 * late_hist, (late_coarse, late_hist)
+
+
 def test_coarse_grid_correction_by_coarse_cg(cuda):
     """A closed box (zero-gradient pressure on every face: an anchor cell) does
     not separate: its coarse grid is solved by Jacobi-PCG from the
