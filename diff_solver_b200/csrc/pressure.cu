@@ -1982,8 +1982,8 @@ __global__ void jacobi_sweep_kernel(Operator op, const T* __restrict__ rhs, cons
 }
 
 XsStatus jacobi_sweeps(cudaStream_t st, const Grid& g, uint32_t anchor, const uint32_t* mask, const XsScalarBoundary& pb, const float* rhs,
-                       const double* rhs_d, const float* x, float* tmp, float* x_out) {
-    if (!x || !tmp || !x_out || x_out == x || x_out == tmp || (!rhs && !rhs_d)) return XS_INVALID_ARGUMENT;
+                       const double* rhs_d, const float* x, float* tmp, float* x_out, int sweeps) {
+    if (!x || !tmp || !x_out || x_out == x || x_out == tmp || (!rhs && !rhs_d) || sweeps < 0) return XS_INVALID_ARGUMENT;
     const Operator op{g, mask, anchor, pb, rhs_d == nullptr};
     const uint64_t n = cell_count(g);
     const unsigned blocks = static_cast<unsigned>(std::min<uint64_t>((n + 255) / 256, 148 * 16));
@@ -1992,8 +1992,8 @@ XsStatus jacobi_sweeps(cudaStream_t st, const Grid& g, uint32_t anchor, const ui
     const bool fast = fast_pass_ok(g, mask, anchor, pb, rhs_d == nullptr);
     const FastGeom f = fast ? fast_geom(g, anchor, pb) : FastGeom{};
     const float* src = x;
-    for (int k = 0; k < kCoarsePreSweeps; ++k) {
-        float* dst = ((kCoarsePreSweeps - 1 - k) % 2 == 0) ? x_out : tmp;
+    for (int k = 0; k < sweeps; ++k) {
+        float* dst = ((sweeps - 1 - k) % 2 == 0) ? x_out : tmp;
         if (fast && rhs_d)
             fast_pass_kernel<kPassJacobi, double><<<fast_pass_blocks(g), 256, 0, st>>>(f, src, rhs_d, dst, omega);
         else if (fast)
@@ -2006,7 +2006,7 @@ XsStatus jacobi_sweeps(cudaStream_t st, const Grid& g, uint32_t anchor, const ui
         if (s != XS_OK) return s;
         src = dst;
     }
-    if (kCoarsePreSweeps == 0) return check_cuda(cudaMemcpyAsync(x_out, x, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
+    if (sweeps == 0) return check_cuda(cudaMemcpyAsync(x_out, x, sizeof(float) * n, cudaMemcpyDeviceToDevice, st));
     return XS_OK;
 }
 
@@ -2105,7 +2105,9 @@ XsStatus coarse_cycles(cudaStream_t st, const Grid& g, uint32_t anchor, const Xs
     for (int c = 0; c < cycles; ++c) {
         float* dst = (c % 2 == 0) ? h.start : h.ring_start;  // never x
         XsStatus s;
-        if ((s = jacobi_sweeps(st, g, anchor, nullptr, pb, rhs, rhs_d, x, h.extra_product, dst)) != XS_OK) return s;
+        if ((s = jacobi_sweeps(st, g, anchor, nullptr, pb, rhs, rhs_d, x, h.extra_product, dst, rhs_d ? kAdjointPreSweeps : kCoarsePreSweeps)) !=
+            XS_OK)
+            return s;
         if ((s = start_residual(st, g, anchor, nullptr, pb, rhs, dst, h.residual, rhs_d)) != XS_OK) return s;
         if ((s = coarse_correction(st, g, anchor, pb, h, h.residual, c == 0 ? kCoarseMaxIterations : kLaterCoarseIterations)) != XS_OK) return s;
         if ((s = line_step(st, g, anchor, nullptr, pb, h, h.correction, dst, h.residual, dst)) != XS_OK) return s;

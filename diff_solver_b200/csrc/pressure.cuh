@@ -124,8 +124,13 @@ constexpr double kCoarseTolerance = 1e-2;
 constexpr uint32_t kCoarseMaxIterations = 1000;
 // Damped Jacobi sweeps (weight 2/3) on the start before its residual is
 // restricted: they remove the high-frequency part of the error, which the
-// coarse grid cannot represent and CG would otherwise meet first.
+// coarse grid cannot represent and CG would otherwise meet first.  The
+// adjoint starts take nine per round: their ring predicts far less, and at
+// 256^3 nine sweeps in each of three rounds leave 3-5 adjoint iterations
+// per solve instead of 5-16 (3.7 % less time per reverse step; the forward
+// starts measured fastest with six).
 constexpr int kCoarsePreSweeps = 6;
+constexpr int kAdjointPreSweeps = 9;
 // The coarse grid's own coarsening for the start of its solve: 4 when its
 // extents allow (divisible, at least 8 cells after), else 2, else none.
 uint32_t second_coarsening(const Grid& coarse);
@@ -148,11 +153,11 @@ XsStatus galerkin_combine(cudaStream_t st, const Grid& g, uint32_t anchor, const
 // centres, clamped at the domain edges.  Grids without colliders only.
 XsStatus coarse_correction(cudaStream_t st, const Grid& g, uint32_t anchor, const XsScalarBoundary& pb, const WarmHistory& h, const float* r,
                            uint32_t max_iterations = kCoarseMaxIterations);
-// kCoarsePreSweeps damped Jacobi sweeps from x (FP32 rhs with fixed values,
-// or the FP64 adjoint rhs_d without), result in x_out; tmp is scratch (N).
-// x_out may not alias x or tmp.
+// `sweeps` damped Jacobi sweeps from x (FP32 rhs with fixed values, or the
+// FP64 adjoint rhs_d without), result in x_out; tmp is scratch (N).  x_out
+// may not alias x or tmp.
 XsStatus jacobi_sweeps(cudaStream_t st, const Grid& g, uint32_t anchor, const uint32_t* mask, const XsScalarBoundary& pb, const float* rhs,
-                       const double* rhs_d, const float* x, float* tmp, float* x_out);
+                       const double* rhs_d, const float* x, float* tmp, float* x_out, int sweeps = kCoarsePreSweeps);
 // Copies the coarse solve's iteration count into the fine solve's statistics.
 XsStatus record_coarse_iterations(cudaStream_t st, const WarmHistory& h, void* fine_workspace, const Grid& g);
 // One energy-optimal step along a direction d from x (in place allowed):
@@ -179,7 +184,8 @@ constexpr uint32_t kMaxStartRounds = 8;
 // solve) in rounds after the first: their residuals are rougher, and a
 // solve to kCoarseTolerance took 60-260 iterations for little gain.
 constexpr uint32_t kLaterCoarseIterations = 16;
-// `cycles` rounds of: kCoarsePreSweeps Jacobi sweeps, the residual, the
+// `cycles` rounds of: kCoarsePreSweeps Jacobi sweeps (kAdjointPreSweeps
+// for an adjoint start, rhs_d given), the residual, the
 // coarse-grid correction of it, one line step along that correction; from x
 // (h.ring_start on entry), the rounds alternating between h.start and
 // h.ring_start.  *out = the final start, h.residual = its residual.  Grids
