@@ -2016,7 +2016,7 @@ __global__ void line_update_kernel(uint64_t n, const double* __restrict__ coef, 
     const float c = static_cast<float>(coef[0]);
     for (uint64_t i = static_cast<uint64_t>(blockIdx.x) * blockDim.x + threadIdx.x; i < n; i += static_cast<uint64_t>(gridDim.x) * blockDim.x) {
         x_out[i] = fmaf(c, d[i], x[i]);
-        r[i] = fmaf(-c, ad[i], r[i]);
+        if (r) r[i] = fmaf(-c, ad[i], r[i]);
     }
 }
 
@@ -2027,7 +2027,7 @@ __global__ void __launch_bounds__(256) line_update4_kernel(uint32_t groups, cons
     for (uint32_t t = blockIdx.x * blockDim.x + threadIdx.x; t < groups; t += gridDim.x * blockDim.x) {
         const uint32_t i = 4u * t;
         st4(x_out + i, axpy4(ld4(x + i), c, ld4(d + i)));
-        st4(r + i, axpy4(ld4(r + i), -c, ld4(ad + i)));
+        if (r) st4(r + i, axpy4(ld4(r + i), -c, ld4(ad + i)));
     }
 }
 
@@ -2057,7 +2057,7 @@ __global__ void __launch_bounds__(256) line_gram_fast_kernel(FastGeom f, const f
 }
 
 XsStatus line_step(cudaStream_t st, const Grid& g, uint32_t anchor, const uint32_t* mask, const XsScalarBoundary& pb, const WarmHistory& h,
-                   const float* d, const float* x, float* r, float* x_out) {
+                   const float* d, const float* x, float* r, float* x_out, bool update_residual) {
     if (!h.meta || !h.extra_product || !d || !x || !r || !x_out) return XS_INVALID_ARGUMENT;
     const Operator op{g, mask, anchor, pb, true};
     const uint64_t n = cell_count(g);
@@ -2071,7 +2071,7 @@ XsStatus line_step(cudaStream_t st, const Grid& g, uint32_t anchor, const uint32
         if ((s = check_launch()) != XS_OK) return s;
         basis_solve_kernel<1><<<1, 64, 0, st>>>(h.partials, blocks, h.coef);
         if ((s = check_launch()) != XS_OK) return s;
-        line_update4_kernel<<<fast_pass_blocks(g), 256, 0, st>>>(f.groups, h.coef, d, h.extra_product, x, r, x_out);
+        line_update4_kernel<<<fast_pass_blocks(g), 256, 0, st>>>(f.groups, h.coef, d, h.extra_product, x, update_residual ? r : nullptr, x_out);
         return check_launch();
     }
     apply_operator_kernel<<<grid, 256, 0, st>>>(op, d, h.extra_product);
@@ -2094,12 +2094,12 @@ XsStatus line_step(cudaStream_t st, const Grid& g, uint32_t anchor, const uint32
     if ((s = check_launch()) != XS_OK) return s;
     basis_solve_kernel<1><<<1, 64, 0, st>>>(h.partials, blocks, h.coef);
     if ((s = check_launch()) != XS_OK) return s;
-    line_update_kernel<<<grid, 256, 0, st>>>(n, h.coef, d, h.extra_product, x, r, x_out);
+    line_update_kernel<<<grid, 256, 0, st>>>(n, h.coef, d, h.extra_product, x, update_residual ? r : nullptr, x_out);
     return check_launch();
 }
 
 XsStatus coarse_cycles(cudaStream_t st, const Grid& g, uint32_t anchor, const XsScalarBoundary& pb, const WarmHistory& h, const float* rhs,
-                       const double* rhs_d, int cycles, const float** out) {
+                       const double* rhs_d, int cycles, const float** out, bool keep_residual) {
     if (cycles < 1 || !out) return XS_INVALID_ARGUMENT;
     const float* x = h.ring_start;
     for (int c = 0; c < cycles; ++c) {
@@ -2110,7 +2110,8 @@ XsStatus coarse_cycles(cudaStream_t st, const Grid& g, uint32_t anchor, const Xs
             return s;
         if ((s = start_residual(st, g, anchor, nullptr, pb, rhs, dst, h.residual, rhs_d)) != XS_OK) return s;
         if ((s = coarse_correction(st, g, anchor, pb, h, h.residual, c == 0 ? kCoarseMaxIterations : kLaterCoarseIterations)) != XS_OK) return s;
-        if ((s = line_step(st, g, anchor, nullptr, pb, h, h.correction, dst, h.residual, dst)) != XS_OK) return s;
+        if ((s = line_step(st, g, anchor, nullptr, pb, h, h.correction, dst, h.residual, dst, keep_residual && c == cycles - 1)) != XS_OK)
+            return s;
         x = dst;
     }
     *out = x;

@@ -163,9 +163,11 @@ XsStatus record_coarse_iterations(cudaStream_t st, const WarmHistory& h, void* f
 // One energy-optimal step along a direction d from x (in place allowed):
 // x_out = x + c d, r -= c A d with c = (d . r) / (d . A d) minimising the
 // A-norm of the error along d (0 when d . A d vanishes); r is the residual
-// of x on entry and of x_out on return.  A d goes to h.extra_product.
+// of x on entry and, with update_residual, of x_out on return (left as it
+// was otherwise: a step whose residual nothing reads moves 8 bytes per cell
+// less).  A d goes to h.extra_product.
 XsStatus line_step(cudaStream_t st, const Grid& g, uint32_t anchor, const uint32_t* mask, const XsScalarBoundary& pb, const WarmHistory& h,
-                   const float* d, const float* x, float* r, float* x_out);
+                   const float* d, const float* x, float* r, float* x_out, bool update_residual = true);
 // Rounds of the start pipeline (sweeps + coarse-grid correction) before the
 // forward and the adjoint fine solves.  Measured at 256^3 (plume, steps
 // 185-205, exact coarse solve): the forward start leaves a relative residual
@@ -188,10 +190,11 @@ constexpr uint32_t kLaterCoarseIterations = 16;
 // for an adjoint start, rhs_d given), the residual, the
 // coarse-grid correction of it, one line step along that correction; from x
 // (h.ring_start on entry), the rounds alternating between h.start and
-// h.ring_start.  *out = the final start, h.residual = its residual.  Grids
-// without colliders only.
+// h.ring_start.  *out = the final start; with keep_residual h.residual = its
+// residual (otherwise a scratch value: every round recomputes the residual
+// after its sweeps).  Grids without colliders only.
 XsStatus coarse_cycles(cudaStream_t st, const Grid& g, uint32_t anchor, const XsScalarBoundary& pb, const WarmHistory& h, const float* rhs,
-                       const double* rhs_d, int cycles, const float** out);
+                       const double* rhs_d, int cycles, const float** out, bool keep_residual = false);
 // Trilinear interpolation of a cell-centred field on the grid coarsened f
 // times (coarse) at the cell centres of `fine`, clamped at the edges.
 XsStatus prolong_cells(cudaStream_t st, const Grid& fine, const Grid& coarse, uint32_t f, const float* ec, float* out);

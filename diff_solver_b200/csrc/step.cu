@@ -52,14 +52,14 @@ XsStatus projection_forward(cudaStream_t st, const Grid& g, const XsPressureSolv
             if (coarse) {
                 const int cycles = h.forward_rounds ? static_cast<int>(h.forward_rounds)
                                                     : (warm_start ? kForwardStartCyclesLearned : kForwardStartCycles);
-                if ((s = coarse_cycles(st, g, anchor, pb, h, rhs, nullptr, cycles, &x)) != XS_OK) return s;
+                if ((s = coarse_cycles(st, g, anchor, pb, h, rhs, nullptr, cycles, &x, warm_start != nullptr)) != XS_OK) return s;
             } else if ((s = start_residual(st, g, anchor, mask, pb, rhs, x, h.residual)) != XS_OK) {
                 return s;
             }
             if (warm_start) {
                 float* out = x == h.start ? h.ring_start : h.start;
                 if ((s = warm_start_guess(warm_start, st, g, h.residual, &guess)) != XS_OK) return s;
-                if ((s = line_step(st, g, anchor, mask, pb, h, guess, x, h.residual, out)) != XS_OK) return s;
+                if ((s = line_step(st, g, anchor, mask, pb, h, guess, x, h.residual, out, false)) != XS_OK) return s;
                 x = out;
             }
             used.initial_guess = x;
