@@ -439,6 +439,71 @@ def load_network(args, shape):
     return network
 
 
+# The U-Net's twelve 3x3x3 convolutions as (C_in, C_out, level), level l on
+# the network grid coarsened 2^l per axis; channel counts as the tensor cores
+# run them (padded to 16: the first layer reads 2 real channels, the output
+# layer writes 1).
+UNET_CONVOLUTIONS = [(16, 16, 0), (16, 16, 0), (16, 32, 1), (32, 32, 1), (32, 64, 2), (64, 64, 2), (64, 64, 3), (64, 64, 3),
+                     (64, 32, 2), (32, 16, 1), (16, 16, 0), (16, 16, 0)]
+
+
+def unet_flops(voxels, padded=True):
+    """Multiply-add FLOPs (2 per MAC) of one network forward on `voxels` cells
+    of the network grid; padded=False counts only the real input channels of
+    the first layer (2) and the real output channel of the last (1)."""
+    total = 0.0
+    for i, (cin, cout, level) in enumerate(UNET_CONVOLUTIONS):
+        if not padded:
+            cin = 2 if i == 0 else cin
+            cout = 1 if i == len(UNET_CONVOLUTIONS) - 1 else cout
+        total += 2.0 * 27 * cin * cout * voxels / 8 ** level
+    return total
+
+
+def network_record(network, shape, repeats=10):
+    """The learned step's network alone, timed with CUDA events on the
+    launching stream after 3 warm-up calls: `predict` (the twelve tcgen05
+    convolutions, pooling and upsampling on the network grid) and `guess`
+    (restriction of a fine-grid right-hand side, normalisation, predict and
+    prolongation).  Achieved TFLOP/s counts the algorithmic convolution
+    FLOPs (real channels) against the measured burst bf16 peak (the network
+    is timed alone)."""
+    import torch
+
+    from diff_solver_b200 import _native as N
+    peaks = json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json"))) if os.path.exists(os.path.join(ROOT, "MEASURED_PEAKS.json")) else {}
+    peak, kind = (float(peaks["bf16_tflops"]), "measured burst") if "bf16_tflops" in peaks else (1590.0, "fallback burst")
+    cells = network.cells
+    gen = torch.Generator(device="cuda").manual_seed(3)
+    small = torch.randn(cells, device="cuda", generator=gen)
+    fine_shape = tuple(s * network.factor for s in network.shape)
+    fine = torch.randn(fine_shape[0] * fine_shape[1] * fine_shape[2], device="cuda", generator=gen)
+    grid = N.XsGrid(*fine_shape, 1.0 / fine_shape[0], 0.5 / fine_shape[0])
+    stream = network.stream
+    for _ in range(3):
+        network.predict(small)
+        network.guess(grid, fine)
+    torch.cuda.synchronize()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(3)]
+    ev[0].record(stream)
+    for _ in range(repeats):
+        network.predict(small)
+    ev[1].record(stream)
+    for _ in range(repeats):
+        network.guess(grid, fine)
+    ev[2].record(stream)
+    torch.cuda.synchronize()
+    network.check()
+    predict_ms = ev[0].elapsed_time(ev[1]) / repeats
+    guess_ms = ev[1].elapsed_time(ev[2]) / repeats
+    flops = unet_flops(cells, padded=False)
+    achieved = flops / (predict_ms / 1e3) / 1e12
+    return {"network_grid": list(network.shape), "fluid_grid": list(fine_shape), "predict_ms": predict_ms, "guess_ms": guess_ms,
+            "flops_per_predict": flops, "flops_per_predict_padded": unet_flops(cells, padded=True),
+            "roofline": {"bound": "tensor", "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": achieved / peak,
+                         "peak_kind": kind}}
+
+
 def spin_up(shape, network, steps, keep=()):
     """The plume from rest (seeded velocity noise) with the headline start;
     returns {step: state copy} for the steps in `keep` and the last."""
@@ -712,6 +777,11 @@ def product_run(args, world, rank, local):
         del ro
         torch.cuda.empty_cache()
     clocks = sampler.stop()
+    if network is not None and world == 1:
+        try:
+            extra["network"] = network_record(network, args.shape)
+        except Exception as e:  # a record beside the headline: report it, keep the line
+            extra["network"] = {"error": f"{type(e).__name__}: {e}"}
     if not args.no_adjoint and world == 1:
         extra["adjoint"] = adjoint_record(args, args.shape, network, saved[keep[0]], window=window)
         torch.cuda.empty_cache()
@@ -840,6 +910,8 @@ def main():
         a["reverse_step_gbs"] = b / (a["ms_per_reverse_step"] / 1e3) / 1e9
         a["reverse_step_frac"] = a["reverse_step_gbs"] / peak
         line["adjoint"] = a
+    if "network" in extra:
+        line["network"] = extra.pop("network")
     if "reference_kernels" in extra:
         rk = extra.pop("reference_kernels")
         if "unavailable" not in rk:
