@@ -36,6 +36,10 @@ and per-stage times are in ``arms``.  Further records of the same run:
                       on the same box and state, next to this library's
   large_grid          512x512x256 (steps 89-98 of its 100-step plume): plain,
                       two-round classical and headline arms, per-stage GB/s
+  network             the warm-start network alone on its grid (predict and
+                      guess), its convolution FLOPs against the bf16 peak
+  config0             the 64^3 plume's full 100 steps from rest: plain and
+                      headline arms on the GPU, the FP64 oracle on the host
   cpu_baseline        full FP64 oracle steps from the spun-up state on the
                       host's cores
 
@@ -504,6 +508,80 @@ def network_record(network, shape, repeats=10):
                          "peak_kind": kind}}
 
 
+def config0_record(args, shape=(64, 64, 64), steps=100, cpu=True, cpu_budget_s=120.0):
+    """The 64^3 plume rolled from rest for its full 100 steps: on the GPU by
+    the plain arm and the headline arm (network on the 64^3 grid itself),
+    each timed with CUDA events on its stream after a 3-step warm-up and a
+    reload of the start; and, with `cpu`, by the FP64 CPU oracle from the
+    same start (the plain solve: Jacobi-PCG to 1e-6 from zero, all host
+    cores) until all steps are done or `cpu_budget_s` is spent."""
+    import torch
+
+    from diff_solver_b200.model import tensors_of
+    from diff_solver_b200.warm_start import WarmStartNetwork
+    net = WarmStartNetwork(shape, factor=1)
+    net.load(args.weights)
+    rec = {"grid": list(shape), "steps": steps, "start": "rest; velocity noise U(-0.01, 0.01) on every face (CUDA generator, seed 0)",
+           "arms": {}}
+    initial = None
+    for name, history, network, coarsening in (("plain", 0, None, 0), (HEADLINE, HISTORY, net, COARSENING)):
+        ro = Rollout(shape, history, network, coarsening)
+        gen = torch.Generator(device="cuda").manual_seed(0)
+        for t in ro.cur.velocity.components():
+            t.uniform_(-0.01, 0.01, generator=gen)
+        start = ro.model.allocate_state(ro.ctx)
+        for d, s in zip(tensors_of(start), tensors_of(ro.cur)):
+            d.copy_(s)
+        if initial is None:
+            initial = [x.double().cpu().numpy() for x in tensors_of(start)]
+        with torch.cuda.stream(ro.ctx.stream):
+            for _ in range(3):
+                ro.step()
+        torch.cuda.synchronize()
+        ro.load(start)
+        torch.cuda.synchronize()
+        ev = make_events(2)
+        ev[0].record(ro.ctx.stream)
+        with torch.cuda.stream(ro.ctx.stream):
+            for _ in range(steps):
+                ro.step()
+        ev[1].record(ro.ctx.stream)
+        torch.cuda.synchronize()
+        ms = ev[0].elapsed_time(ev[1])
+        last = ro.ctx.read_solve_stats()
+        rec["arms"][name] = {"steps_per_s": steps / (ms / 1e3), "ms_per_step": ms / steps,
+                             "last_solve": {k: last[k] for k in ("iterations", "final_residual")}}
+        del ro, start
+    net.check()
+    del net
+    torch.cuda.empty_cache()
+    if cpu:
+        rec["cpu"] = cpu_rollout({"density": initial[0], "temperature": initial[1], "velocity": initial[2:5]}, shape, steps, cpu_budget_s)
+    return rec
+
+
+def cpu_rollout(state_arrays, shape, steps, budget_s):
+    """Consecutive FP64 CPU oracle steps of the workload from `state_arrays`
+    (pressure by Jacobi-PCG to 1e-6 from zero, all host cores) until `steps`
+    are done or `budget_s` is spent; returns the timing record."""
+    import numpy as np
+
+    from oracle import binding as ob
+    threads = ob.set_threads(os.cpu_count() or 1)
+    P = ob.Problem(workload_configuration(shape), "f64", solver="pcg", iterations=20000, tolerance=1e-6)
+    ctl = ob.zeros_control(P.res, np.float64)
+    st = state_arrays
+    done, iterations, t0 = 0, 0, time.perf_counter()
+    while done < steps and time.perf_counter() - t0 < budget_s:
+        st, _, stats, _ = P.forward_step(st, ctl, PARAMS)
+        done += 1
+        iterations += int(stats.iterations)
+    seconds = time.perf_counter() - t0
+    return {"steps_per_s": done / seconds, "steps": done, "seconds": seconds, "pcg_iterations": iterations, "cores": threads,
+            "kind": "port", "sample": f"{done} of the {steps} steps by the FP64 CPU oracle from the same start, pressure by "
+                                      f"Jacobi-PCG to 1e-6 from zero ({iterations} iterations in all), on {threads} host threads"}
+
+
 def spin_up(shape, network, steps, keep=()):
     """The plume from rest (seeded velocity noise) with the headline start;
     returns {step: state copy} for the steps in `keep` and the last."""
@@ -794,6 +872,12 @@ def product_run(args, world, rank, local):
         big.check()
         del big
         torch.cuda.empty_cache()
+    if not args.no_config0 and world == 1 and network is not None:
+        try:
+            extra["config0"] = config0_record(args, cpu=not args.no_cpu_baseline)
+        except Exception as e:  # a record beside the headline: report it, keep the line
+            extra["config0"] = {"error": f"{type(e).__name__}: {e}"}
+        torch.cuda.empty_cache()
     if network is not None:
         network.check()
     host_state = None
@@ -834,6 +918,7 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true", help="skip the 40-step VJP record")
     ap.add_argument("--no-large", action="store_true", help="skip the 512x512x256 record")
     ap.add_argument("--no-reference-kernels", action="store_true", help="skip the per-kernel timing of the reference's kernels")
+    ap.add_argument("--no-config0", action="store_true", help="skip the 100-step 64^3 rollout from rest (GPU arms and CPU oracle)")
     ap.add_argument("--adjoint-window", type=int, default=40)
     ap.add_argument("--cpu-steps", type=int, default=3, help="most full FP64 steps the CPU legs time")
     ap.add_argument("--cpu-budget", type=float, default=150.0, help="seconds after which the CPU legs stop adding steps")
@@ -912,6 +997,8 @@ def main():
         line["adjoint"] = a
     if "network" in extra:
         line["network"] = extra.pop("network")
+    if "config0" in extra:
+        line["config0"] = extra.pop("config0")
     if "reference_kernels" in extra:
         rk = extra.pop("reference_kernels")
         if "unavailable" not in rk:

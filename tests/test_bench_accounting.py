@@ -1,6 +1,7 @@
 """The benchmark's byte and FLOP accounting on CPU (no GPU): the per-step
-byte counts follow the stage table of the smoke step, and the U-Net FLOP
-table describes the network the library builds (its parameter count)."""
+byte counts follow the stage table of the smoke step, the U-Net FLOP table
+describes the network the library builds (its parameter count), and the CPU
+oracle leg of the 64^3 record produces its timing record."""
 import os
 import sys
 
@@ -58,3 +59,17 @@ def test_reverse_step_bytes():
     b0 = bench.reverse_step_bytes(n, f, 0, 0)
     assert b0 == 4.0 * (8 * n + 8 * f) + 352.0 * n + 224.0 * f
     assert bench.reverse_step_bytes(n, f, 2, 3) - b0 == 36.0 * n * 5
+
+
+def test_cpu_rollout_record():
+    # the CPU leg of the 64^3 record on a small grid: consecutive FP64
+    # oracle steps from a seeded start, stopped by the step count
+    import numpy as np
+    from oracle import binding as ob
+    shape = (16, 16, 16)
+    rng = np.random.default_rng(0)
+    st = ob.zeros_state(shape, np.float64)
+    st["velocity"] = [rng.uniform(-0.01, 0.01, v.shape) for v in st["velocity"]]
+    rec = bench.cpu_rollout(st, shape, steps=3, budget_s=60.0)
+    assert rec["steps"] == 3 and rec["steps_per_s"] > 0 and rec["pcg_iterations"] > 0
+    assert rec["kind"] == "port" and rec["cores"] >= 1
