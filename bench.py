@@ -508,7 +508,7 @@ def network_record(network, shape, repeats=10):
                          "peak_kind": kind}}
 
 
-def config0_record(args, shape=(64, 64, 64), steps=100, cpu=True, cpu_budget_s=120.0):
+def config0_record(args, shape=(64, 64, 64), steps=100, cpu=True, cpu_budget_s=90.0):
     """The 64^3 plume rolled from rest for its full 100 steps: on the GPU by
     the plain arm and the headline arm (network on the 64^3 grid itself),
     each timed with CUDA events on its stream after a 3-step warm-up and a
