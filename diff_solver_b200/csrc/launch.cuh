@@ -14,9 +14,16 @@ XsStatus check_launch();
 // Converts a CUDA runtime status into an XsStatus (without counting).
 XsStatus check_cuda(cudaError_t e);
 
+// Kernels index cells and faces with 32-bit integers: (nx + 1)(ny + 1)(nz + 1)
+// must stay below 2^32.  Each factor is widened before the + 1, and the
+// product is formed one factor at a time so that it cannot wrap.
 inline bool valid_grid(const XsGrid& g) {
-    return g.nx > 0 && g.ny > 0 && g.nz > 0 && g.cell_size > 0.0f && g.time_step > 0.0f &&
-           static_cast<unsigned long long>(g.nx + 1) * (g.ny + 1) * (g.nz + 1) < (1ull << 32);
+    if (!(g.nx > 0 && g.ny > 0 && g.nz > 0 && g.cell_size > 0.0f && g.time_step > 0.0f)) return false;
+    constexpr unsigned long long kLimit = 1ull << 32;
+    const unsigned long long a = g.nx + 1ull, b = g.ny + 1ull, c = g.nz + 1ull;
+    if (a >= kLimit || b >= kLimit || c >= kLimit) return false;
+    const unsigned long long ab = a * b;  // < 2^64: both factors < 2^32
+    return ab < kLimit && ab * c < kLimit;
 }
 inline bool valid(const XsVector& v) { return v.x && v.y && v.z; }
 inline bool valid(const XsAdjointVector& v) { return v.x && v.y && v.z; }

@@ -5,6 +5,8 @@ import glob
 import os
 import re
 
+import pytest
+
 from common import ROOT
 
 from diff_solver_b200 import _native
@@ -79,6 +81,24 @@ def test_workspace_queries_without_gpu():
     fwd = lib.xs_smoke_workspace_bytes(ctypes.byref(m), 0)
     diff = lib.xs_smoke_workspace_bytes(ctypes.byref(m), 1)
     assert diff > fwd > ws
+
+
+@pytest.mark.parametrize("extents", [(2**32 - 1, 4, 4), (4, 2**32 - 1, 4), (2**22, 2**22, 2**22), (2**16, 2**16, 2),
+                                     (1024, 1024, 4096)])
+def test_grids_past_32_bit_indexing_are_rejected(extents):
+    # kernels index with 32 bits: (nx + 1)(ny + 1)(nz + 1) must stay below
+    # 2^32, without the extent sum or the product wrapping around
+    lib = _native.lib()
+    g = _native.XsGrid(*extents, 1e-3, 5e-4)
+    assert lib.xs_projection_workspace_bytes(g) == 0
+    assert lib.xs_source_forward(None, g, None, None, None, None, 0, 0, None) == _native.XS_INVALID_ARGUMENT
+
+
+def test_largest_grids_within_32_bit_indexing_are_accepted():
+    lib = _native.lib()
+    # 1023 x 1023 x 4094: (nx + 1)(ny + 1)(nz + 1) = 2^32 - 2^20
+    assert lib.xs_projection_workspace_bytes(_native.XsGrid(1023, 1023, 4094, 1e-3, 5e-4)) > 0
+    assert lib.xs_projection_workspace_bytes(_native.XsGrid(512, 512, 256, 1 / 512, 1 / 1024)) > 0
 
 
 def test_warm_start_options_are_validated_without_gpu():
