@@ -125,7 +125,7 @@ def test_plume_vjp_matches_oracle_finite_differences(cuda):
            projected_relative_error=projected)
     # the gradient projected on the directions agrees to 1e-3 relative L2, and
     # so does each directional derivative of comparable size; a direction
-    # whose derivative is far smaller than the others' (the fourth: 8x) is
+    # whose derivative is far smaller than the largest (the fourth: 11x) is
     # held to the others' absolute error, the FP32 model's noise floor
     # (~5e-7 here against FP64 differences)
     assert projected < 1e-3, (projected, rels)
